@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark of the gtd:: force-and-step hot path on B200.
+
+Workload (one GPU, the configuration the headline metric is quoted on): mixed-precision direct
+summation, N = 262144 equal-mass Plummer sphere (a = 1 AU, M = 1e30 kg, G = 6.674e-11, seeded
+synthetic data), leapfrog KDK with dt = 3600 s.  One "step" = one KDK step (kick-drift, one
+force evaluation of N(N-1) ordered pair-interactions, kick).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: the north-star path runs on one GPU; N > 1 runs N independent replicas (one process
+per GPU, no data-path collective; "scaling": "weak").  The reference arm times the reference's
+own single-threaded CPU evolve (oracle/_ref, built from the reference headers; the C port under
+oracle/ where that library is absent) on all host cores, as independent copies.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "pair-interactions/s mixed vs FP64 GPU at |ΔE/E|≤1e-6; ensemble steps/s"
+UNIT = "pair-interactions/s"
+FLOPS_PER_INTERACTION = 20
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--n", type=int, default=262144)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--fp64-steps", type=int, default=3)
+    p.add_argument("--e2e-calls", type=int, default=2)
+    p.add_argument("--e2e-iterations", type=int, default=5)
+    p.add_argument("--cpu-sample-n", type=int, default=16384)
+    p.add_argument("--cpu-sample-steps", type=int, default=1)
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------
+# process group (replicas only; used for barriers and the max-over-ranks of the timed region)
+# ------------------------------------------------------------------------------------------------
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU baselines (the reference's own evolve, else the C port of it)
+# ------------------------------------------------------------------------------------------------
+def cpu_sample(n_sample, steps, seed, threads):
+    """Times `threads` independent copies of evolve(leapfrog_kdk) on an n_sample Plummer system for
+    `steps` steps.  Returns (interactions/s, kind, seconds)."""
+    from gregpackagescpp_b200.ics import UNITS_G6674, plummer
+    from oracle.oracle import Oracle, RefOracle, ensure_built
+    m, x, v = plummer(n_sample, seed)
+    evals = steps + 1  # evolve(leapfrog_kdk) computes the initial acceleration, then one per step
+    inter = float(threads) * evals * n_sample * (n_sample - 1)
+    if RefOracle.available():
+        secs = RefOracle().bench_kdk(m, x, v, 3600.0, steps, threads, UNITS_G6674)
+        return inter / secs, "reference", secs
+    ensure_built()
+    o = Oracle()
+    secs = o.bench_kdk(m, x, v, 3600.0, steps, o.G(UNITS_G6674), threads)
+    return inter / secs, "port", secs
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = host_threads()
+    n_s, st = args.cpu_sample_n, args.cpu_sample_steps
+    for _ in range(max(args.warmup, 0)):
+        cpu_sample(n_s, st, args.seed, threads)
+    vals, secs_tot, kind = [], 0.0, None
+    for _ in range(args.steps):
+        val, kind, secs = cpu_sample(n_s, st, args.seed, threads)
+        vals.append(val)
+        secs_tot += secs
+    value = float(np.mean(vals))
+    sample = (f"{threads} independent copies of evolve(leapfrog_kdk), N={n_s} Plummer (seed {args.seed}), "
+              f"{st} step(s) = {st + 1} force evaluations each, per bench step; single-threaded evolve per copy")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs_tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (long double intermediates)",
+        "data": "synthetic (seeded Plummer sphere)",
+        "config": {"workload": "direct summation leapfrog KDK on a Plummer sphere (CPU sample of the N=262144 "
+                               "mixed-precision workload)", "n_bodies_sample": n_s, "threads": threads},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------------
+def run_ours(args, rank, world, local):
+    import torch
+
+    from gregpackagescpp_b200 import _lib
+    from gregpackagescpp_b200.ics import plummer
+    from gregpackagescpp_b200._lib import check
+
+    torch.cuda.set_device(local)
+    L = _lib.load()
+    n, K, W = args.n, args.steps, args.warmup
+    G, dt = 6.674e-11, 3600.0
+    m, x, v = plummer(n, args.seed)
+    x3, v3 = np.ascontiguousarray(x.reshape(-1)), np.ascontiguousarray(v.reshape(-1))
+    pair = float(n) * (n - 1)
+
+    def make(prec):
+        h = C.c_void_p()
+        check(L.gtd_system_create(C.byref(h), local, prec))
+        check(L.gtd_system_set_params(h, G, dt, 1000, 0.0, 0.5))
+        check(L.gtd_system_upload(h, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
+        return h
+
+    def stream_of(h):
+        p = C.c_void_p()
+        check(L.gtd_system_stream(h, C.byref(p)))
+        return torch.cuda.ExternalStream(p.value, device=torch.device("cuda", local))
+
+    def energy(h):
+        ke, pe = C.c_double(), C.c_double()
+        check(L.gtd_system_energy(h, C.byref(ke), C.byref(pe), None, None))
+        return ke.value + pe.value
+
+    def launches(h):
+        c = C.c_uint64()
+        check(L.gtd_system_launch_count(h, C.byref(c)))
+        return c.value
+
+    # --- accuracy of the mixed force against the FP64 one at the initial state (untimed)
+    h64, hmx = make(_lib.PREC_F64), make(_lib.PREC_MIXED)
+    a64, amx = np.zeros(3 * n), np.zeros(3 * n)
+    check(L.gtd_system_accelerations(h64, 0, a64.ctypes.data))
+    check(L.gtd_system_accelerations(hmx, 0, amx.ctypes.data))
+    rel = np.linalg.norm((amx - a64).reshape(n, 3), axis=1) / np.linalg.norm(a64.reshape(n, 3), axis=1)
+
+    # --- FP64 GPU path throughput (same workload, fewer steps)
+    check(L.gtd_system_evolve_begin(h64, 16))
+    check(L.gtd_system_evolve_steps(h64, 1))
+    s64 = stream_of(h64)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s64)
+    check(L.gtd_system_evolve_steps(h64, args.fp64_steps))
+    e1.record(s64)
+    e1.synchronize()
+    fp64_value = args.fp64_steps * pair / (e0.elapsed_time(e1) * 1e-3)
+    check(L.gtd_system_destroy(h64))
+
+    # --- mixed path: the timed hot loop
+    E0 = energy(hmx)
+    check(L.gtd_system_evolve_begin(hmx, 16))
+    for _ in range(W):
+        check(L.gtd_system_evolve_steps(hmx, 1))
+    smx = stream_of(hmx)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")  # > 126 MB L2
+    check(L.gtd_system_time_force_kernels(hmx, 1))
+    check(L.gtd_system_force_timing(hmx, None, None, 1))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    clocks = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    clocks.start()
+    time.sleep(0.4)
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = launches(hmx)
+    for k in range(K):
+        with torch.cuda.stream(smx):
+            flush.zero_()  # L2 flush between timed steps, outside the timed events
+        ev[k][0].record(smx)
+        check(L.gtd_system_evolve_steps(hmx, 1))
+        ev[k][1].record(smx)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    gpu_launches = launches(hmx) - l0
+    t_local = sum(a.elapsed_time(b) for a, b in ev) * 1e-3
+    force_ms, force_n = C.c_double(), C.c_uint64()
+    check(L.gtd_system_force_timing(hmx, C.byref(force_ms), C.byref(force_n), 1))
+    check(L.gtd_system_time_force_kernels(hmx, 0))
+    t_max = max_over_ranks(t_local, world)
+    total_inter = sum_over_ranks(K * pair, world)
+    value = total_inter / t_max
+    E1 = energy(hmx)
+    drift = abs(E1 - E0) / abs(E0)
+    check(L.gtd_system_destroy(hmx))
+    del flush
+
+    # --- roofline: the force kernel (FP32 pipe); denominator measured on this GPU
+    peak = C.c_double()
+    check(L.gtd_measure_fma_peak(local, _lib.PREC_MIXED, C.byref(peak)))
+    peak64 = C.c_double()
+    check(L.gtd_measure_fma_peak(local, _lib.PREC_F64, C.byref(peak64)))
+    avg_force_s = force_ms.value * 1e-3 / max(force_n.value, 1)
+    achieved = FLOPS_PER_INTERACTION * pair / avg_force_s
+
+    # --- end to end through the public C ABI with host buffers (upload, evolve, download)
+    iters = args.e2e_iterations
+    he = C.c_void_p()
+    check(L.gtd_system_create(C.byref(he), local, _lib.PREC_MIXED))
+    check(L.gtd_system_set_params(he, G, dt, iters, 0.0, 0.5))
+    xo, vo, ao = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n)
+    ns = C.c_int64()
+    check(L.gtd_system_upload(he, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
+    check(L.gtd_system_evolve(he, 16, C.byref(ns)))  # warm-up call
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_calls):
+        check(L.gtd_system_upload(he, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
+        check(L.gtd_system_evolve(he, 16, C.byref(ns)))
+        check(L.gtd_system_download(he, None, None, None, None, xo.ctypes.data, vo.ctypes.data, ao.ctypes.data))
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+    check(L.gtd_system_destroy(he))
+    e2e_steps = args.e2e_calls * iters
+    e2e_value = sum_over_ranks(args.e2e_calls * (iters + 1) * pair, world) / t_e2e
+    h2d = (m.nbytes + x3.nbytes + v3.nbytes) * args.e2e_calls / e2e_steps
+    d2h = (xo.nbytes + vo.nbytes + ao.nbytes) * args.e2e_calls / e2e_steps
+
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = host_threads()
+        cval, kind, secs = cpu_sample(args.cpu_sample_n, args.cpu_sample_steps, args.seed, threads)
+        cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{threads} concurrent copies of the reference evolve(leapfrog_kdk) on an N="
+                         f"{args.cpu_sample_n} Plummer sphere, {args.cpu_sample_steps} step(s) "
+                         f"({args.cpu_sample_steps + 1} force evaluations each), {secs:.1f} s wall"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": 1e3 * t_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 pair forces + fp64 Kahan sums/state", "data": "synthetic (seeded Plummer sphere)",
+            "config": {"workload": "mixed-precision direct summation, leapfrog KDK, equal-mass Plummer sphere "
+                                   "a=1 AU M=1e30 kg, dt=3600 s", "n_bodies": n, "G": G,
+                       "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
+                       "l2": "flushed (512 MB write) between timed steps, outside the timed events"},
+            "fp64_gpu": {"value": fp64_value, "unit": UNIT, "steps": args.fp64_steps,
+                         "mixed_over_fp64": value / world / fp64_value},
+            "accuracy": {"acc_rel_err_rms": float(np.sqrt((rel ** 2).mean())),
+                         "acc_rel_err_median": float(np.median(rel)), "acc_rel_err_max": float(rel.max()),
+                         "energy_drift_rel": drift, "energy_drift_steps": W + K},
+            "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
+                         "unit": "TFLOP/s", "frac": achieved / peak.value, "traffic": None,
+                         "kernel": "force_mixed_kernel", "flops_per_interaction": FLOPS_PER_INTERACTION,
+                         "peak_source": "measured FFMA/FFMA2 microkernel on this GPU (gtd_measure_fma_peak)",
+                         "fp64_peak": peak64.value / 1e12},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "calls": args.e2e_calls, "iterations_per_call": iters},
+            "gpu_launches": gpu_launches,
+            "clocks": clk,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,519 @@
+// Direct-summation force kernels and the integrator epilogues of gtd::system::evolve.
+//
+// Replaces, on the device: cumulative_acc / calc_acc_and_e (gregsys.hpp:352-357, 439-476), the
+// kick/drift updates of loop_kdk / loop_dkd and the KDK/DKD drivers (gregsys.hpp:477-607,
+// 2946-3039), take_euler_step (:380-391), the modified-Euler and midpoint predictors and steps
+// (:392-419, 2714-2891), and calc_energy (:608-630).
+//
+// Layout in HBM: one double4 per body for position + mass (x, y, z, m), double4 velocity and
+// acceleration (w unused), all coalesced 32-byte loads.  The force kernels stream j-tiles of 256
+// bodies through shared memory; every CTA of a grid sized to fill all SMs exactly processes an
+// equal contiguous range of (i-block, j-tile) pairs (stream-K), writing per-row partial sums that
+// the integrate kernel combines in a fixed order, so results are bit-reproducible.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "gtd_internal.cuh"
+
+namespace gtd {
+
+struct ForceKArgs {
+    int64_t n, rows, tiles, total;
+    int grid, bi;
+    const double4 *src;
+    double G;
+    double *part;
+};
+
+__device__ __forceinline__ void cta_range(const ForceKArgs &a, int g, int64_t &s, int64_t &e) {
+    s = (int64_t)g * a.total / a.grid;
+    e = (int64_t)(g + 1) * a.total / a.grid;
+}
+
+// -------------------------------------------------------------------------------------------
+// FP64: a_i = sum_j G m_j (x_j - x_i) / |x_j - x_i|^3, no softening (the reference's direct path
+// ignores eps).  The i == j term has r2 == 0 and is dropped by the select on inv.
+// -------------------------------------------------------------------------------------------
+template <int I>
+__global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
+    __shared__ double4 tile[2][kThreads];
+    const int t = threadIdx.x;
+    int64_t s, e;
+    cta_range(a, blockIdx.x, s, e);
+    const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+    while (s < e) {
+        const int64_t r = s / a.tiles;
+        const int64_t jt0 = s - r * a.tiles;
+        const int64_t row_end = min(e, (r + 1) * a.tiles);
+        const int64_t jt1 = row_end - r * a.tiles;
+        double xi[I], yi[I], zi[I], ax[I], ay[I], az[I];
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            const int64_t i = r * a.bi + k * kThreads + t;
+            const double4 p = i < a.n ? a.src[i] : zero;
+            xi[k] = p.x; yi[k] = p.y; zi[k] = p.z;
+            ax[k] = 0.0; ay[k] = 0.0; az[k] = 0.0;
+        }
+        {
+            const int64_t j = jt0 * kThreads + t;
+            double4 q = j < a.n ? a.src[j] : zero;
+            q.w *= a.G;
+            tile[0][t] = q;
+        }
+        __syncthreads();
+        int cur = 0;
+        for (int64_t jt = jt0; jt < jt1; ++jt) {
+            const bool more = jt + 1 < jt1;
+            double4 qn = zero;
+            if (more) {
+                const int64_t j = (jt + 1) * kThreads + t;
+                if (j < a.n) qn = a.src[j];
+            }
+#pragma unroll 4
+            for (int jj = 0; jj < kThreads; ++jj) {
+                const double4 q = tile[cur][jj];
+#pragma unroll
+                for (int k = 0; k < I; ++k) {
+                    const double dx = q.x - xi[k], dy = q.y - yi[k], dz = q.z - zi[k];
+                    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+                    double inv = rsqrt(r2);
+                    inv = r2 > 0.0 ? inv : 0.0;
+                    const double sc = (q.w * inv) * (inv * inv);
+                    ax[k] = fma(sc, dx, ax[k]);
+                    ay[k] = fma(sc, dy, ay[k]);
+                    az[k] = fma(sc, dz, az[k]);
+                }
+            }
+            if (more) {
+                qn.w *= a.G;
+                tile[cur ^ 1][t] = qn;
+            }
+            __syncthreads();
+            cur ^= 1;
+        }
+        double *slot = a.part + (size_t)(blockIdx.x + r) * 3 * a.bi;
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            const int l = k * kThreads + t;
+            slot[l] = ax[k];
+            slot[a.bi + l] = ay[k];
+            slot[2 * a.bi + l] = az[k];
+        }
+        s = row_end;
+        __syncthreads();
+    }
+}
+
+// -------------------------------------------------------------------------------------------
+// Mixed precision.  Each j-tile is staged in shared memory as FP32 coordinates relative to the
+// row's centre c (taken in FP64 from the row's first body), with G m_j in FP32.  Pair arithmetic
+// runs two j-bodies per instruction on the packed FP32x2 pipe (add/mul/fma .f32x2) with one MUFU
+// rsqrt per pair; each i keeps FP32 partial sums for kFold j-bodies, then folds them into FP64
+// Kahan-compensated accumulators.  Tiles that overlap the row (where i == j occurs) take the
+// guarded path; all others run without a compare.
+// -------------------------------------------------------------------------------------------
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ void kahan_add(double &sum, double &comp, double v) {
+    const double y = v - comp;
+    const double t = sum + y;
+    comp = (t - sum) - y;
+    sum = t;
+}
+
+template <int I, bool kGuard>
+__device__ __forceinline__ void mixed_tile(const float *__restrict__ tx, const float *__restrict__ ty,
+                                           const float *__restrict__ tz, const float *__restrict__ tm,
+                                           const float2 (&nx)[I], const float2 (&ny)[I], const float2 (&nz)[I],
+                                           double (&sx)[I], double (&sy)[I], double (&sz)[I], double (&cx)[I],
+                                           double (&cy)[I], double (&cz)[I]) {
+    const float2 *X = reinterpret_cast<const float2 *>(tx);
+    const float2 *Y = reinterpret_cast<const float2 *>(ty);
+    const float2 *Z = reinterpret_cast<const float2 *>(tz);
+    const float2 *M = reinterpret_cast<const float2 *>(tm);
+#pragma unroll 1
+    for (int q0 = 0; q0 < kThreads / 2; q0 += kFold / 2) {
+        float2 fx[I], fy[I], fz[I];
+#pragma unroll
+        for (int k = 0; k < I; ++k) fx[k] = fy[k] = fz[k] = make_float2(0.f, 0.f);
+#pragma unroll 8
+        for (int u = 0; u < kFold / 2; ++u) {
+            const float2 xj = X[q0 + u], yj = Y[q0 + u], zj = Z[q0 + u], mj = M[q0 + u];
+#pragma unroll
+            for (int k = 0; k < I; ++k) {
+                const float2 dx = __fadd2_rn(xj, nx[k]);
+                const float2 dy = __fadd2_rn(yj, ny[k]);
+                const float2 dz = __fadd2_rn(zj, nz[k]);
+                float2 r2 = __fmul2_rn(dx, dx);
+                r2 = __ffma2_rn(dy, dy, r2);
+                r2 = __ffma2_rn(dz, dz, r2);
+                float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                if (kGuard) {
+                    inv.x = r2.x > 0.f ? inv.x : 0.f;
+                    inv.y = r2.y > 0.f ? inv.y : 0.f;
+                }
+                const float2 inv2 = __fmul2_rn(inv, inv);
+                float2 sc = __fmul2_rn(mj, inv);
+                sc = __fmul2_rn(sc, inv2);
+                fx[k] = __ffma2_rn(dx, sc, fx[k]);
+                fy[k] = __ffma2_rn(dy, sc, fy[k]);
+                fz[k] = __ffma2_rn(dz, sc, fz[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            kahan_add(sx[k], cx[k], (double)fx[k].x + (double)fx[k].y);
+            kahan_add(sy[k], cy[k], (double)fy[k].x + (double)fy[k].y);
+            kahan_add(sz[k], cz[k], (double)fz[k].x + (double)fz[k].y);
+        }
+    }
+}
+
+template <int I>
+__global__ void __launch_bounds__(kThreads, 2) force_mixed_kernel(ForceKArgs a) {
+    __shared__ __align__(16) float tx[2][kThreads];
+    __shared__ __align__(16) float ty[2][kThreads];
+    __shared__ __align__(16) float tz[2][kThreads];
+    __shared__ __align__(16) float tm[2][kThreads];
+    const int t = threadIdx.x;
+    int64_t s, e;
+    cta_range(a, blockIdx.x, s, e);
+    const float kFar = 1e30f;  // padding bodies: far away and massless, their terms are exactly 0
+    while (s < e) {
+        const int64_t r = s / a.tiles;
+        const int64_t jt0 = s - r * a.tiles;
+        const int64_t row_end = min(e, (r + 1) * a.tiles);
+        const int64_t jt1 = row_end - r * a.tiles;
+        const int64_t row0 = r * a.bi;
+        const double4 c = a.src[row0];
+        float2 nx[I], ny[I], nz[I];
+        double sx[I], sy[I], sz[I], cx[I], cy[I], cz[I];
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            const int64_t i = row0 + k * kThreads + t;
+            float fx = 0.f, fy = 0.f, fz = 0.f;
+            if (i < a.n) {
+                const double4 p = a.src[i];
+                fx = (float)(p.x - c.x);
+                fy = (float)(p.y - c.y);
+                fz = (float)(p.z - c.z);
+            }
+            nx[k] = make_float2(-fx, -fx);
+            ny[k] = make_float2(-fy, -fy);
+            nz[k] = make_float2(-fz, -fz);
+            sx[k] = sy[k] = sz[k] = 0.0;
+            cx[k] = cy[k] = cz[k] = 0.0;
+        }
+        auto stage = [&](int64_t jt, int buf) {
+            const int64_t j = jt * kThreads + t;
+            if (j < a.n) {
+                const double4 q = a.src[j];
+                tx[buf][t] = (float)(q.x - c.x);
+                ty[buf][t] = (float)(q.y - c.y);
+                tz[buf][t] = (float)(q.z - c.z);
+                tm[buf][t] = (float)(a.G * q.w);
+            } else {
+                tx[buf][t] = kFar;
+                ty[buf][t] = kFar;
+                tz[buf][t] = kFar;
+                tm[buf][t] = 0.f;
+            }
+        };
+        stage(jt0, 0);
+        __syncthreads();
+        int cur = 0;
+        for (int64_t jt = jt0; jt < jt1; ++jt) {
+            const bool more = jt + 1 < jt1;
+            double4 qn = make_double4(0.0, 0.0, 0.0, 0.0);
+            bool have = false;
+            if (more) {
+                const int64_t j = (jt + 1) * kThreads + t;
+                if (j < a.n) {
+                    qn = a.src[j];
+                    have = true;
+                }
+            }
+            const int64_t j0 = jt * kThreads;
+            const bool diag = j0 < row0 + a.bi && row0 < j0 + kThreads;
+            if (diag)
+                mixed_tile<I, true>(tx[cur], ty[cur], tz[cur], tm[cur], nx, ny, nz, sx, sy, sz, cx, cy, cz);
+            else
+                mixed_tile<I, false>(tx[cur], ty[cur], tz[cur], tm[cur], nx, ny, nz, sx, sy, sz, cx, cy, cz);
+            if (more) {
+                const int nb = cur ^ 1;
+                if (have) {
+                    tx[nb][t] = (float)(qn.x - c.x);
+                    ty[nb][t] = (float)(qn.y - c.y);
+                    tz[nb][t] = (float)(qn.z - c.z);
+                    tm[nb][t] = (float)(a.G * qn.w);
+                } else {
+                    tx[nb][t] = kFar;
+                    ty[nb][t] = kFar;
+                    tz[nb][t] = kFar;
+                    tm[nb][t] = 0.f;
+                }
+            }
+            __syncthreads();
+            cur ^= 1;
+        }
+        double *slot = a.part + (size_t)(blockIdx.x + r) * 3 * a.bi;
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            const int l = k * kThreads + t;
+            slot[l] = sx[k] - cx[k];
+            slot[a.bi + l] = sy[k] - cy[k];
+            slot[2 * a.bi + l] = sz[k] - cz[k];
+        }
+        s = row_end;
+        __syncthreads();
+    }
+}
+
+// -------------------------------------------------------------------------------------------
+// Plan and launch
+// -------------------------------------------------------------------------------------------
+ForcePlan make_plan(int64_t n, int precision, int device) {
+    ForcePlan p;
+    p.n = n;
+    p.bi = kThreads * (precision == GTD_PREC_MIXED ? kIMix : kI64);
+    p.bj = kThreads;
+    p.rows = (n + p.bi - 1) / p.bi;
+    p.tiles = (n + p.bj - 1) / p.bj;
+    p.total = p.rows * p.tiles;
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (precision == GTD_PREC_MIXED)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, force_mixed_kernel<kIMix>, kThreads, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, force_f64_kernel<kI64>, kThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)sms * per_sm;
+    if (grid > p.total) grid = p.total > 0 ? p.total : 1;
+    p.grid = (int)grid;
+    p.slots = p.grid + p.rows;
+    return p;
+}
+
+size_t partial_bytes(const ForcePlan &p) { return (size_t)p.slots * 3 * p.bi * sizeof(double); }
+
+int launch_force(int precision, const ForcePlan &p, const double4 *src, double G, double *partials,
+                 cudaStream_t s) {
+    if (p.n == 0) return GTD_OK;
+    ForceKArgs a{p.n, p.rows, p.tiles, p.total, p.grid, p.bi, src, G, partials};
+    if (precision == GTD_PREC_MIXED)
+        force_mixed_kernel<kIMix><<<p.grid, kThreads, 0, s>>>(a);
+    else
+        force_f64_kernel<kI64><<<p.grid, kThreads, 0, s>>>(a);
+    GTD_CHECK_LAUNCH();
+    return GTD_OK;
+}
+
+// -------------------------------------------------------------------------------------------
+// Integrate: sum the partials of body i (CTA order) and apply the method's update in FP64.
+// -------------------------------------------------------------------------------------------
+struct IntArgs {
+    int64_t n, tiles, total;
+    int grid, bi, epi;
+    const double *part;
+    StepArgs st;
+};
+
+__device__ __forceinline__ int64_t cta_of(int64_t pos, int grid, int64_t total) {
+    return ((pos + 1) * (int64_t)grid - 1) / total;
+}
+
+__global__ void integrate_kernel(IntArgs a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int64_t r = i / a.bi;
+    const int l = (int)(i - r * a.bi);
+    const int64_t g0 = cta_of(r * a.tiles, a.grid, a.total);
+    const int64_t g1 = cta_of((r + 1) * a.tiles - 1, a.grid, a.total);
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int64_t g = g0; g <= g1; ++g) {
+        const double *slot = a.part + (size_t)(g + r) * 3 * a.bi;
+        ax += slot[l];
+        ay += slot[a.bi + l];
+        az += slot[2 * a.bi + l];
+    }
+    const StepArgs &st = a.st;
+    const double h = st.h, h2 = 0.5 * st.h;
+    const double4 x = st.cur[i];
+    double4 v = st.vel[i];
+    switch (a.epi) {
+        case EPI_ACC:
+            st.acc[i] = make_double4(ax, ay, az, 0.0);
+            break;
+        case EPI_KDK: {
+            st.acc[i] = make_double4(ax, ay, az, 0.0);
+            v.x = fma(h2, ax, v.x); v.y = fma(h2, ay, v.y); v.z = fma(h2, az, v.z);
+            if (!st.last) {
+                v.x = fma(h2, ax, v.x); v.y = fma(h2, ay, v.y); v.z = fma(h2, az, v.z);
+                st.dst[i] = make_double4(fma(h, v.x, x.x), fma(h, v.y, x.y), fma(h, v.z, x.z), x.w);
+            }
+            st.vel[i] = v;
+            break;
+        }
+        case EPI_DKD: {
+            st.acc[i] = make_double4(ax, ay, az, 0.0);
+            v.x = fma(h, ax, v.x); v.y = fma(h, ay, v.y); v.z = fma(h, az, v.z);
+            double4 y = make_double4(fma(h2, v.x, x.x), fma(h2, v.y, x.y), fma(h2, v.z, x.z), x.w);
+            if (!st.last) y = make_double4(fma(h2, v.x, y.x), fma(h2, v.y, y.y), fma(h2, v.z, y.z), x.w);
+            st.dst[i] = y;
+            st.vel[i] = v;
+            break;
+        }
+        case EPI_EULER: {
+            st.acc[i] = make_double4(ax, ay, az, 0.0);
+            st.dst[i] = make_double4(fma(h, v.x, x.x), fma(h, v.y, x.y), fma(h, v.z, x.z), x.w);
+            v.x = fma(h, ax, v.x); v.y = fma(h, ay, v.y); v.z = fma(h, az, v.z);
+            st.vel[i] = v;
+            break;
+        }
+        case EPI_PREDICT: {
+            const double hp = st.hp;
+            st.acc[i] = make_double4(ax, ay, az, 0.0);
+            st.pred_pos[i] = make_double4(fma(hp, v.x, x.x), fma(hp, v.y, x.y), fma(hp, v.z, x.z), x.w);
+            st.pred_vel[i] = make_double4(fma(hp, ax, v.x), fma(hp, ay, v.y), fma(hp, az, v.z), 0.0);
+            break;
+        }
+        case EPI_CORR_MEULER: {
+            const double4 pv = st.pred_vel[i], a0 = st.acc[i];
+            st.dst[i] = make_double4(fma(h2, v.x + pv.x, x.x), fma(h2, v.y + pv.y, x.y), fma(h2, v.z + pv.z, x.z),
+                                     x.w);
+            v.x = fma(h2, a0.x + ax, v.x); v.y = fma(h2, a0.y + ay, v.y); v.z = fma(h2, a0.z + az, v.z);
+            st.vel[i] = v;
+            break;
+        }
+        case EPI_CORR_MIDPOINT: {
+            const double4 pv = st.pred_vel[i];
+            st.dst[i] = make_double4(fma(h, pv.x, x.x), fma(h, pv.y, x.y), fma(h, pv.z, x.z), x.w);
+            v.x = fma(h, ax, v.x); v.y = fma(h, ay, v.y); v.z = fma(h, az, v.z);
+            st.vel[i] = v;
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+int launch_integrate(const ForcePlan &p, const double *partials, int epi, const StepArgs &st, cudaStream_t s) {
+    if (p.n == 0) return GTD_OK;
+    IntArgs a{p.n, p.tiles, p.total, p.grid, p.bi, epi, partials, st};
+    const int threads = 256;
+    integrate_kernel<<<(unsigned)((p.n + threads - 1) / threads), threads, 0, s>>>(a);
+    GTD_CHECK_LAUNCH();
+    return GTD_OK;
+}
+
+__global__ void kick_drift_kernel(int64_t n, const double4 *cur, double4 *dst, double4 *vel, const double4 *acc,
+                                  double h) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double h2 = 0.5 * h;
+    const double4 x = cur[i], a = acc[i];
+    double4 v = vel[i];
+    v.x = fma(h2, a.x, v.x); v.y = fma(h2, a.y, v.y); v.z = fma(h2, a.z, v.z);
+    vel[i] = v;
+    dst[i] = make_double4(fma(h, v.x, x.x), fma(h, v.y, x.y), fma(h, v.z, x.z), x.w);
+}
+
+__global__ void half_drift_kernel(int64_t n, const double4 *cur, double4 *dst, const double4 *vel, double h) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double h2 = 0.5 * h;
+    const double4 x = cur[i], v = vel[i];
+    dst[i] = make_double4(fma(h2, v.x, x.x), fma(h2, v.y, x.y), fma(h2, v.z, x.z), x.w);
+}
+
+int launch_kick_drift(int64_t n, const double4 *cur, double4 *dst, double4 *vel, const double4 *acc, double h,
+                      cudaStream_t s) {
+    if (n == 0) return GTD_OK;
+    kick_drift_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, cur, dst, vel, acc, h);
+    GTD_CHECK_LAUNCH();
+    return GTD_OK;
+}
+
+int launch_half_drift(int64_t n, const double4 *cur, double4 *dst, const double4 *vel, double h, cudaStream_t s) {
+    if (n == 0) return GTD_OK;
+    half_drift_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, cur, dst, vel, h);
+    GTD_CHECK_LAUNCH();
+    return GTD_OK;
+}
+
+// -------------------------------------------------------------------------------------------
+// FP64 energy / momentum diagnostics.  One thread per i sums G m_j / r_ij over all j != i
+// (j-tiles through shared memory); each block reduces its 9 sums in a fixed tree order and the
+// host adds the block partials in block order, so the result is reproducible run to run.
+// -------------------------------------------------------------------------------------------
+constexpr int kEThreads = 256;
+
+__global__ void __launch_bounds__(kEThreads) energy_kernel(int64_t n, const double4 *pm, const double4 *vel,
+                                                           double G, double *out) {
+    __shared__ double4 tile[kEThreads];
+    __shared__ double red[9][kEThreads];
+    const int t = threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * kEThreads + t;
+    double4 p = make_double4(0.0, 0.0, 0.0, 0.0), v = p;
+    if (i < n) {
+        p = pm[i];
+        v = vel[i];
+    }
+    double phi = 0.0;
+    for (int64_t j0 = 0; j0 < n; j0 += kEThreads) {
+        const int64_t j = j0 + t;
+        tile[t] = j < n ? pm[j] : make_double4(0.0, 0.0, 0.0, 0.0);
+        __syncthreads();
+        const int lim = (int)min((int64_t)kEThreads, n - j0);
+        for (int jj = 0; jj < lim; ++jj) {
+            const double4 q = tile[jj];
+            const double dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+            const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+            if (r2 > 0.0) phi += q.w / sqrt(r2);
+        }
+        __syncthreads();
+    }
+    double val[9];
+    val[0] = 0.5 * p.w * (v.x * v.x + v.y * v.y + v.z * v.z);
+    val[1] = -0.5 * G * p.w * phi;
+    val[2] = p.w * v.x; val[3] = p.w * v.y; val[4] = p.w * v.z;
+    val[5] = p.w * p.x; val[6] = p.w * p.y; val[7] = p.w * p.z;
+    val[8] = p.w;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) red[k][t] = i < n ? val[k] : 0.0;
+    __syncthreads();
+    for (int w = kEThreads / 2; w > 0; w >>= 1) {
+        if (t < w)
+            for (int k = 0; k < 9; ++k) red[k][t] += red[k][t + w];
+        __syncthreads();
+    }
+    if (t < 9) out[(size_t)blockIdx.x * 9 + t] = red[t][0];
+}
+
+int64_t energy_scratch_doubles(int64_t n) { return ((n + kEThreads - 1) / kEThreads) * 9 + 9; }
+
+int launch_energy(int64_t n, const double4 *pm, const double4 *vel, double G, double *scratch, int64_t scratch_n,
+                  cudaStream_t s) {
+    if (n == 0) return GTD_OK;
+    const int64_t blocks = (n + kEThreads - 1) / kEThreads;
+    if (blocks * 9 > scratch_n) return fail(GTD_ERR_CAPACITY, "energy scratch too small");
+    energy_kernel<<<(unsigned)blocks, kEThreads, 0, s>>>(n, pm, vel, G, scratch);
+    GTD_CHECK_LAUNCH();
+    return GTD_OK;
+}
+
+int finish_energy(const double *h, int64_t n, double *out9) {
+    const int64_t blocks = (n + kEThreads - 1) / kEThreads;
+    long double acc[9] = {0};
+    for (int64_t b = 0; b < blocks; ++b)
+        for (int k = 0; k < 9; ++k) acc[k] += h[b * 9 + k];
+    for (int k = 0; k < 9; ++k) out9[k] = (double)acc[k];
+    return GTD_OK;
+}
+
+}  // namespace gtd

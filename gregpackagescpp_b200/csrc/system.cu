@@ -1,0 +1,584 @@
+// C ABI of the device-resident gtd::system (include/gtd_b200.h): handle lifetime, gather/scatter
+// of the AoS bodies, and the evolve() loop of gregsys.hpp:2593-3071 driven on one CUDA stream.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "gtd_internal.cuh"
+#include "gtd_system.cuh"
+
+namespace gtd {
+
+static thread_local char g_err[1024];
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+int fail(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+    set_error("CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), what, file, line);
+    return e == cudaErrorMemoryAllocation ? GTD_ERR_OUT_OF_MEMORY : GTD_ERR_CUDA;
+}
+
+const char *last_error() { return g_err; }
+
+}  // namespace gtd
+
+using namespace gtd;
+
+// ---------------------------------------------------------------------------------------------
+// buffers
+// ---------------------------------------------------------------------------------------------
+static int ensure_capacity(gtd_system *s, int64_t n) {
+    if (n <= s->cap) return GTD_OK;
+    release_bodies(s);
+    const size_t b4 = sizeof(double4) * (size_t)n;
+    GTD_CUDA(cudaMalloc(&s->pm[0], b4));
+    GTD_CUDA(cudaMalloc(&s->pm[1], b4));
+    GTD_CUDA(cudaMalloc(&s->vel, b4));
+    GTD_CUDA(cudaMalloc(&s->acc, b4));
+    GTD_CUDA(cudaMalloc(&s->rad, sizeof(double) * (size_t)n));
+    GTD_CUDA(cudaMalloc(&s->rest, sizeof(double) * (size_t)n));
+    GTD_CUDA(cudaMalloc(&s->ids, sizeof(int32_t) * (size_t)n));
+    GTD_CUDA(cudaMallocHost(&s->stage, 4 * b4));
+    s->cap = n;
+    return GTD_OK;
+}
+
+void release_bodies(gtd_system *s) {
+    cudaFree(s->pm[0]);
+    cudaFree(s->pm[1]);
+    cudaFree(s->vel);
+    cudaFree(s->acc);
+    cudaFree(s->pred_pos);
+    cudaFree(s->pred_vel);
+    cudaFree(s->rad);
+    cudaFree(s->rest);
+    cudaFree(s->ids);
+    cudaFree(s->partials);
+    cudaFree(s->escratch);
+    cudaFreeHost(s->stage);
+    s->pm[0] = s->pm[1] = s->vel = s->acc = s->pred_pos = s->pred_vel = nullptr;
+    s->rad = s->rest = nullptr;
+    s->ids = nullptr;
+    s->partials = nullptr;
+    s->escratch = nullptr;
+    s->stage = nullptr;
+    s->part_bytes = 0;
+    s->escratch_n = 0;
+    s->cap = 0;
+}
+
+int ensure_plan(gtd_system *s) {
+    if (s->plan.n == s->n && s->plan_prec == s->precision && s->partials) return GTD_OK;
+    s->plan = make_plan(s->n, s->precision, s->device);
+    s->plan_prec = s->precision;
+    const size_t need = partial_bytes(s->plan);
+    if (need > s->part_bytes) {
+        cudaFree(s->partials);
+        s->partials = nullptr;
+        GTD_CUDA(cudaMalloc(&s->partials, need));
+        s->part_bytes = need;
+    }
+    return GTD_OK;
+}
+
+static int ensure_pred(gtd_system *s) {
+    if (s->pred_pos) return GTD_OK;
+    GTD_CUDA(cudaMalloc(&s->pred_pos, sizeof(double4) * (size_t)s->cap));
+    GTD_CUDA(cudaMalloc(&s->pred_vel, sizeof(double4) * (size_t)s->cap));
+    return GTD_OK;
+}
+
+// Force at `src` into acc (and the integrator epilogue); counts launches.
+static int collect_force_timing(gtd_system *s) {
+    if (s->ev_used == 0) return GTD_OK;
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    for (size_t k = 0; k + 1 < s->ev_used; k += 2) {
+        float ms = 0.f;
+        GTD_CUDA(cudaEventElapsedTime(&ms, s->ev_pool[k], s->ev_pool[k + 1]));
+        s->force_ms += ms;
+        s->force_launches += 1;
+    }
+    s->ev_used = 0;
+    return GTD_OK;
+}
+
+static int timed_event(gtd_system *s) {
+    if (s->ev_used == s->ev_pool.size()) {
+        if (s->ev_pool.size() >= 4096) {
+            int rc = collect_force_timing(s);
+            if (rc) return rc;
+        } else {
+            cudaEvent_t e;
+            GTD_CUDA(cudaEventCreate(&e));
+            s->ev_pool.push_back(e);
+        }
+    }
+    GTD_CUDA(cudaEventRecord(s->ev_pool[s->ev_used++], s->stream));
+    return GTD_OK;
+}
+
+int force_and_integrate(gtd_system *s, const double4 *src, int epi, const StepArgs &st) {
+    int rc = ensure_plan(s);
+    if (rc) return rc;
+    if (s->time_force && (rc = timed_event(s))) return rc;
+    rc = launch_force(s->precision, s->plan, src, s->G, s->partials, s->stream);
+    if (rc) return rc;
+    if (s->time_force && (rc = timed_event(s))) return rc;
+    rc = launch_integrate(s->plan, s->partials, epi, st, s->stream);
+    if (rc) return rc;
+    s->launches += 2;
+    return GTD_OK;
+}
+
+static StepArgs step_args(gtd_system *s, const double4 *src, bool last) {
+    StepArgs a{};
+    a.n = s->n;
+    a.src = src;
+    a.cur = s->pm[s->cur];
+    a.dst = s->pm[s->cur ^ 1];
+    a.vel = s->vel;
+    a.acc = s->acc;
+    a.pred_pos = s->pred_pos;
+    a.pred_vel = s->pred_vel;
+    a.h = s->dt;
+    a.hp = s->dt;
+    a.last = last ? 1 : 0;
+    return a;
+}
+
+// One direct-summation step of `method` (the bodies of the evolve loops, gregsys.hpp:2666-3039).
+static int direct_step(gtd_system *s, int method, bool last) {
+    int rc = GTD_OK;
+    switch (method) {
+        case GTD_LEAPFROG_KDK: {
+            if (s->synced) {
+                rc = launch_kick_drift(s->n, s->pm[s->cur], s->pm[s->cur ^ 1], s->vel, s->acc, s->dt, s->stream);
+                if (rc) return rc;
+                s->launches += 1;
+                s->cur ^= 1;
+            }
+            StepArgs a = step_args(s, s->pm[s->cur], last);
+            rc = force_and_integrate(s, s->pm[s->cur], EPI_KDK, a);
+            if (rc) return rc;
+            if (!last) s->cur ^= 1;
+            s->synced = last;
+            return GTD_OK;
+        }
+        case GTD_LEAPFROG_DKD: {
+            if (s->synced) {
+                rc = launch_half_drift(s->n, s->pm[s->cur], s->pm[s->cur ^ 1], s->vel, s->dt, s->stream);
+                if (rc) return rc;
+                s->launches += 1;
+                s->cur ^= 1;
+            }
+            StepArgs a = step_args(s, s->pm[s->cur], last);
+            rc = force_and_integrate(s, s->pm[s->cur], EPI_DKD, a);
+            if (rc) return rc;
+            s->cur ^= 1;
+            s->synced = last;
+            return GTD_OK;
+        }
+        case GTD_EULER: {
+            StepArgs a = step_args(s, s->pm[s->cur], true);
+            rc = force_and_integrate(s, s->pm[s->cur], EPI_EULER, a);
+            if (rc) return rc;
+            s->cur ^= 1;
+            return GTD_OK;
+        }
+        case GTD_MODIFIED_EULER:
+        case GTD_MIDPOINT: {
+            rc = ensure_pred(s);
+            if (rc) return rc;
+            StepArgs a = step_args(s, s->pm[s->cur], true);
+            a.hp = method == GTD_MIDPOINT ? 0.5 * s->dt : s->dt;
+            rc = force_and_integrate(s, s->pm[s->cur], EPI_PREDICT, a);
+            if (rc) return rc;
+            StepArgs b = step_args(s, s->pred_pos, true);
+            rc = force_and_integrate(s, s->pred_pos, method == GTD_MIDPOINT ? EPI_CORR_MIDPOINT : EPI_CORR_MEULER, b);
+            if (rc) return rc;
+            s->cur ^= 1;
+            return GTD_OK;
+        }
+        default:
+            return fail(GTD_ERR_UNSUPPORTED, "method %d has no direct-summation step", method);
+    }
+}
+
+// gtd::system::check_option, gregsys.hpp:1406-1411 (accepts nearly every value, like the original).
+static bool check_option(int option) {
+    const uint16_t lo = (uint16_t)(option & 0x0000ffff);
+    const uint16_t hi = (uint16_t)((unsigned)option >> 16);
+    return !(lo & (lo - 1)) || !lo || lo > GTD_RK4 || !(hi & (hi - 1)) || hi > 2;
+}
+
+// The branch of evolve() a method value selects, in the reference's if/else order
+// (gregsys.hpp:2626-3059).  Returns 0 when no branch does any work.
+static int select_branch(int method) {
+    if ((method & GTD_TWO_BODY) == GTD_TWO_BODY) return GTD_TWO_BODY;
+    if ((method & GTD_EULER) == GTD_EULER) return GTD_EULER;
+    if ((method & GTD_MODIFIED_EULER) == GTD_MODIFIED_EULER) return GTD_MODIFIED_EULER;
+    if ((method & GTD_MIDPOINT) == GTD_MIDPOINT) return GTD_MIDPOINT;
+    if ((method & GTD_LEAPFROG_KDK) == GTD_LEAPFROG_KDK) return GTD_LEAPFROG_KDK;
+    if ((method & GTD_LEAPFROG_DKD) == GTD_LEAPFROG_DKD) return GTD_LEAPFROG_DKD;
+    if ((method & GTD_RK4) == GTD_RK4) return GTD_RK4;
+    if ((method & GTD_RK3_8) == GTD_RK3_8) return GTD_RK3_8;
+    return 0;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        cudaGetDevice(&now);
+        if (prev >= 0 && now != prev) cudaSetDevice(prev);
+    }
+};
+
+int run_collisions(gtd_system *s);  // collide.cu
+int bh_evolve_kdk(gtd_system *s, uint64_t steps);  // octree.cu
+int bh_accelerations(gtd_system *s, double *a3, uint32_t *n_inter);  // octree.cu
+
+static int evolve_begin(gtd_system *s, int method) {
+    s->method = method;
+    s->begun = true;
+    s->synced = true;
+    if (s->n == 0) return GTD_OK;
+    if (method == GTD_LEAPFROG_KDK) {
+        StepArgs a = step_args(s, s->pm[s->cur], true);
+        return force_and_integrate(s, s->pm[s->cur], EPI_ACC, a);
+    }
+    return GTD_OK;
+}
+
+static int evolve_steps(gtd_system *s, uint64_t k) {
+    if (!s->begun) return fail(GTD_ERR_INVALID_ARGUMENT, "gtd_system_evolve_steps before gtd_system_evolve_begin");
+    if (s->n == 0 || k == 0) return GTD_OK;
+    for (uint64_t i = 0; i < k; ++i) {
+        const bool last = (i + 1 == k) || s->coll != GTD_NO_COLL;
+        int rc = direct_step(s, s->method, last);
+        if (rc) return rc;
+        if (s->coll != GTD_NO_COLL) {
+            rc = run_collisions(s);
+            if (rc) return rc;
+        }
+    }
+    return GTD_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------------
+extern "C" {
+
+const char *gtd_last_error(void) { return gtd::last_error(); }
+
+int gtd_abi_version(void) { return GTD_ABI_VERSION; }
+
+int gtd_device_count(int *count) {
+    if (!count) return fail(GTD_ERR_INVALID_ARGUMENT, "count is NULL");
+    *count = 0;
+    cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *count = 0;
+        return fail(GTD_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+    }
+    return GTD_OK;
+}
+
+int gtd_system_create(gtd_system **out, int device, int precision) {
+    if (!out) return fail(GTD_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (precision != GTD_PREC_F64 && precision != GTD_PREC_MIXED)
+        return fail(GTD_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
+    int nd = 0;
+    if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0) {
+        cudaGetLastError();
+        return fail(GTD_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= nd) return fail(GTD_ERR_INVALID_ARGUMENT, "device %d out of range", device);
+    DeviceGuard g(device);
+    gtd_system *s = new (std::nothrow) gtd_system();
+    if (!s) return fail(GTD_ERR_OUT_OF_MEMORY, "host allocation failed");
+    s->device = device;
+    s->precision = precision;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev1);
+    if (e != cudaSuccess) {
+        int rc = cuda_fail(e, "stream/event creation", __FILE__, __LINE__);
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return GTD_OK;
+}
+
+int gtd_system_destroy(gtd_system *s) {
+    if (!s) return GTD_OK;
+    DeviceGuard g(s->device);
+    cudaStreamSynchronize(s->stream);
+    release_bodies(s);
+    release_tree(s);
+    release_collide(s);
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    cudaEventDestroy(s->ev0);
+    cudaEventDestroy(s->ev1);
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return GTD_OK;
+}
+
+int gtd_system_set_params(gtd_system *s, double G, double dt, uint64_t iterations, double softening,
+                          double bh_theta) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (!(dt > 0)) return fail(GTD_ERR_INVALID_ARGUMENT, "Time-step cannot be zero or negative.");
+    if (iterations == 0) return fail(GTD_ERR_INVALID_ARGUMENT, "iterations cannot be zero");
+    if (!(bh_theta >= 0) || bh_theta >= M_PI)
+        return fail(GTD_ERR_INVALID_ARGUMENT,
+                    "Error: opening angle cannot be negative or equal to or larger than PI radians.");
+    if (!(softening >= 0)) return fail(GTD_ERR_INVALID_ARGUMENT, "softening cannot be negative");
+    s->G = G;
+    s->dt = dt;
+    s->iterations = iterations;
+    s->eps = softening;
+    s->theta = bh_theta;
+    return GTD_OK;
+}
+
+int gtd_system_set_collisions(gtd_system *s, int mode) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (mode != GTD_NO_COLL && mode != GTD_OVERLAP_COLL && mode != GTD_MERGE_COLL)
+        return fail(GTD_ERR_INVALID_ARGUMENT, "unknown collision mode %d", mode);
+    s->coll = mode;
+    return GTD_OK;
+}
+
+int gtd_system_upload(gtd_system *s, int64_t n, const double *m, const double *r, const double *rest,
+                      const double *x3, const double *v3) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (n < 0 || n > (int64_t)INT32_MAX) return fail(GTD_ERR_CAPACITY, "body count %lld not supported", (long long)n);
+    if (n > 0 && (!m || !x3)) return fail(GTD_ERR_INVALID_ARGUMENT, "masses and positions are required");
+    DeviceGuard g(s->device);
+    int rc = ensure_capacity(s, n);
+    if (rc) return rc;
+    s->n = n;
+    s->cur = 0;
+    s->begun = false;
+    s->synced = true;
+    s->tree_valid = false;
+    if (n == 0) return GTD_OK;
+    for (int64_t i = 0; i < n; ++i) {
+        if (m[i] < 0) return fail(GTD_ERR_INVALID_ARGUMENT, "negative mass at body %lld", (long long)i);
+        if (r && r[i] < 0) return fail(GTD_ERR_INVALID_ARGUMENT, "negative radius at body %lld", (long long)i);
+    }
+    double4 *hp = s->stage, *hv = s->stage + n;
+    double *hr = reinterpret_cast<double *>(s->stage + 2 * n), *he = hr + n;
+    int32_t *hid = reinterpret_cast<int32_t *>(s->stage + 3 * n);
+    for (int64_t i = 0; i < n; ++i) {
+        hp[i] = make_double4(x3[3 * i], x3[3 * i + 1], x3[3 * i + 2], m[i]);
+        hv[i] = v3 ? make_double4(v3[3 * i], v3[3 * i + 1], v3[3 * i + 2], 0.0) : make_double4(0, 0, 0, 0);
+        hr[i] = r ? r[i] : 0.0;
+        he[i] = rest ? rest[i] : 1.0;
+        hid[i] = (int32_t)i;
+    }
+    const size_t b4 = sizeof(double4) * (size_t)n;
+    GTD_CUDA(cudaMemcpyAsync(s->pm[0], hp, b4, cudaMemcpyHostToDevice, s->stream));
+    GTD_CUDA(cudaMemcpyAsync(s->vel, hv, b4, cudaMemcpyHostToDevice, s->stream));
+    GTD_CUDA(cudaMemcpyAsync(s->rad, hr, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    GTD_CUDA(cudaMemcpyAsync(s->rest, he, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    GTD_CUDA(cudaMemcpyAsync(s->ids, hid, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    GTD_CUDA(cudaMemsetAsync(s->acc, 0, b4, s->stream));
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    return GTD_OK;
+}
+
+int gtd_system_num_bodies(const gtd_system *s, int64_t *n) {
+    if (!s || !n) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    *n = s->n;
+    return GTD_OK;
+}
+
+int gtd_system_download(gtd_system *s, int64_t *n_out, double *m, double *r, double *rest, double *x3, double *v3,
+                        double *a3) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    DeviceGuard g(s->device);
+    const int64_t n = s->n;
+    if (n_out) *n_out = n;
+    if (n == 0) return GTD_OK;
+    double4 *hp = s->stage, *hv = s->stage + n, *ha = s->stage + 2 * n;
+    double *hr = reinterpret_cast<double *>(s->stage + 3 * n), *he = hr + n;
+    const size_t b4 = sizeof(double4) * (size_t)n;
+    GTD_CUDA(cudaMemcpyAsync(hp, s->pm[s->cur], b4, cudaMemcpyDeviceToHost, s->stream));
+    if (v3) GTD_CUDA(cudaMemcpyAsync(hv, s->vel, b4, cudaMemcpyDeviceToHost, s->stream));
+    if (a3) GTD_CUDA(cudaMemcpyAsync(ha, s->acc, b4, cudaMemcpyDeviceToHost, s->stream));
+    if (r) GTD_CUDA(cudaMemcpyAsync(hr, s->rad, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+    if (rest) GTD_CUDA(cudaMemcpyAsync(he, s->rest, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    for (int64_t i = 0; i < n; ++i) {
+        if (m) m[i] = hp[i].w;
+        if (x3) { x3[3 * i] = hp[i].x; x3[3 * i + 1] = hp[i].y; x3[3 * i + 2] = hp[i].z; }
+        if (v3) { v3[3 * i] = hv[i].x; v3[3 * i + 1] = hv[i].y; v3[3 * i + 2] = hv[i].z; }
+        if (a3) { a3[3 * i] = ha[i].x; a3[3 * i + 1] = ha[i].y; a3[3 * i + 2] = ha[i].z; }
+        if (r) r[i] = hr[i];
+        if (rest) rest[i] = he[i];
+    }
+    return GTD_OK;
+}
+
+int gtd_system_evolve_begin(gtd_system *s, int method) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    DeviceGuard g(s->device);
+    return evolve_begin(s, method);
+}
+
+int gtd_system_evolve_steps(gtd_system *s, uint64_t k) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    DeviceGuard g(s->device);
+    int rc = evolve_steps(s, k);
+    if (rc) return rc;
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    return GTD_OK;
+}
+
+int gtd_system_evolve(gtd_system *s, int method, int64_t *elapsed_ns) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (elapsed_ns) *elapsed_ns = 0;
+    if (s->n == 0 || !check_option(method)) return GTD_OK;  // gregsys.hpp:2611-2612
+    DeviceGuard g(s->device);
+    const int branch = select_branch(method);
+    const bool bh = (method & GTD_BARNES_HUT) == GTD_BARNES_HUT;
+    if (branch == GTD_TWO_BODY) {
+        if (s->n != 2) return fail(GTD_ERR_TWO_BODY, "two-body integration requires exactly two bodies");
+        return GTD_OK;  // the reference performs no integration in this branch
+    }
+    if (branch == 0 || branch == GTD_RK4 || branch == GTD_RK3_8) return GTD_OK;  // empty branches
+    if (bh && branch == GTD_EULER)
+        return fail(GTD_ERR_UNSUPPORTED, "Barnes-Hut Euler never advances in the reference (steps is not "
+                                         "incremented, gregsys.hpp:2631-2665); refusing to loop forever");
+    if (bh && branch != GTD_LEAPFROG_KDK) return GTD_OK;  // empty Barnes-Hut branches
+    GTD_CUDA(cudaEventRecord(s->ev0, s->stream));
+    int rc;
+    if (bh) {
+        rc = bh_evolve_kdk(s, s->iterations);
+    } else {
+        rc = evolve_begin(s, branch);
+        if (!rc) rc = evolve_steps(s, s->iterations);
+    }
+    if (rc) return rc;
+    GTD_CUDA(cudaEventRecord(s->ev1, s->stream));
+    GTD_CUDA(cudaEventSynchronize(s->ev1));
+    float ms = 0.f;
+    GTD_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    if (elapsed_ns) *elapsed_ns = (int64_t)((double)ms * 1e6);
+    return GTD_OK;
+}
+
+int gtd_system_accelerations(gtd_system *s, int method, double *a3) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    DeviceGuard g(s->device);
+    if (s->n == 0) return GTD_OK;
+    if ((method & GTD_BARNES_HUT) == GTD_BARNES_HUT) return bh_accelerations(s, a3, nullptr);
+    StepArgs a = step_args(s, s->pm[s->cur], true);
+    int rc = force_and_integrate(s, s->pm[s->cur], EPI_ACC, a);
+    if (rc) return rc;
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    if (a3) {
+        std::vector<double4> h((size_t)s->n);
+        GTD_CUDA(cudaMemcpy(h.data(), s->acc, sizeof(double4) * (size_t)s->n, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < s->n; ++i) {
+            a3[3 * i] = h[i].x;
+            a3[3 * i + 1] = h[i].y;
+            a3[3 * i + 2] = h[i].z;
+        }
+    }
+    return GTD_OK;
+}
+
+int gtd_system_energy(gtd_system *s, double *ke, double *pe, double *p3, double *com3) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    DeviceGuard g(s->device);
+    double out[9] = {0};
+    if (s->n > 0) {
+        const int64_t need = energy_scratch_doubles(s->n);
+        if (need > s->escratch_n) {
+            cudaFree(s->escratch);
+            s->escratch = nullptr;
+            GTD_CUDA(cudaMalloc(&s->escratch, sizeof(double) * (size_t)need));
+            s->escratch_n = need;
+        }
+        int rc = launch_energy(s->n, s->pm[s->cur], s->vel, s->G, s->escratch, s->escratch_n, s->stream);
+        if (rc) return rc;
+        s->launches += 1;
+        std::vector<double> h((size_t)need);
+        GTD_CUDA(cudaMemcpyAsync(h.data(), s->escratch, sizeof(double) * (size_t)need, cudaMemcpyDeviceToHost,
+                                 s->stream));
+        GTD_CUDA(cudaStreamSynchronize(s->stream));
+        finish_energy(h.data(), s->n, out);
+    }
+    if (ke) *ke = out[0];
+    if (pe) *pe = out[1];
+    if (p3) { p3[0] = out[2]; p3[1] = out[3]; p3[2] = out[4]; }
+    if (com3) {
+        for (int k = 0; k < 3; ++k) com3[k] = out[8] > 0 ? out[5 + k] / out[8] : 0.0;
+    }
+    return GTD_OK;
+}
+
+int gtd_system_launch_count(const gtd_system *s, uint64_t *count) {
+    if (!s || !count) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    *count = s->launches;
+    return GTD_OK;
+}
+
+int gtd_system_stream(const gtd_system *s, void **stream) {
+    if (!s || !stream) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    *stream = (void *)s->stream;
+    return GTD_OK;
+}
+
+int gtd_system_time_force_kernels(gtd_system *s, int enable) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    DeviceGuard g(s->device);
+    int rc = collect_force_timing(s);
+    if (rc) return rc;
+    s->time_force = enable != 0;
+    return GTD_OK;
+}
+
+int gtd_system_force_timing(gtd_system *s, double *total_ms, uint64_t *launches, int reset) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    DeviceGuard g(s->device);
+    int rc = collect_force_timing(s);
+    if (rc) return rc;
+    if (total_ms) *total_ms = s->force_ms;
+    if (launches) *launches = s->force_launches;
+    if (reset) {
+        s->force_ms = 0.0;
+        s->force_launches = 0;
+    }
+    return GTD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,217 @@
+"""Python mirror of gtd::system / gtd::body (gregsys.hpp:135-3612, gregbod.hpp:891-1084) over the
+C ABI.  Same method flags, setters, units format and evolve() contract as the reference; the
+state lives in numpy arrays on the host (authoritative between calls, like the reference's
+std::vector<body>) and is uploaded to the device for each evolve() and read back after it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from dataclasses import dataclass, field
+from fractions import Fraction
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ptr
+
+PI = 3.14159265358979323846
+
+_UNITS_RE = re.compile(
+    r"^\s*(m|M)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(d|D)\s*(?=\d{1,18}\s*:)"
+    r"\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(t|T)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*"
+    r"(?=\d{1,18}\s*$)\d*[1-9]+\d*\s*$")
+
+
+def parse_units(units: str) -> float:
+    """G for a units format "Ma:b,Dc:d,Tx:y" (gregsys.hpp:245-282): a = mass denominator,
+    b = mass numerator, c/d = distance numerator/denominator, x/y = time denominator/numerator;
+    G = 66743e-15 * b c^3 y^2 / (a d^3 x^2).  Raises ValueError on a malformed string, as the
+    reference throws std::invalid_argument."""
+    if not _UNITS_RE.match(units):
+        raise ValueError(f'The units_format string passed, "{units}", does not match the format required:\n'
+                         '"Ma:b,Dc:x,Ty:z"')
+    s = units.strip("MmDdTt ").replace(" ", "")
+    nums = [int(x) for x in re.findall(r"\d+", s)]
+    m_den, m_num, d_num, d_den, t_den, t_num = nums
+    g = Fraction(66743) * m_num * d_num ** 3 * t_num ** 2 / (m_den * d_den ** 3 * t_den ** 2) / 10 ** 15
+    return float(g)
+
+
+@dataclass
+class Body:
+    """gtd::body<M,R,T,0> fields that the force-and-step path reads and writes."""
+    mass: float = 1.0
+    radius: float = 1.0
+    pos: tuple = (0.0, 0.0, 0.0)
+    vel: tuple = (0.0, 0.0, 0.0)
+    restitution: float = 1.0
+    acc: tuple = field(default=(0.0, 0.0, 0.0))
+
+
+class System:
+    """gtd::system on the B200.  ``precision`` is "f64" (the reference's arithmetic) or "mixed"
+    (FP32 pair forces, FP64 Kahan sums and state)."""
+
+    two_body = 1
+    euler = 2
+    modified_euler = 4
+    midpoint = 8
+    leapfrog_kdk = 16
+    leapfrog_dkd = 32
+    rk4 = 64
+    rk3_8 = 128
+    barnes_hut = 65536
+    fast_multipole = 131072
+    no_coll_check = 0
+    overlap_coll_check = 3
+    pred_coll_check = 7
+    G_SI = 6.6743e-11
+
+    def __init__(self, m=None, x=None, v=None, r=None, rest=None, timestep: float = 1.0,
+                 num_iterations: int = 1000, units_format: str = "M1:1,D1:1,T1:1",
+                 allow_overlapping_bodies: bool = True, precision: str = "f64", collisions: int = 0,
+                 merge_overlapping: bool = False, device: int = 0):
+        L = _lib.load()
+        if timestep <= 0:
+            raise ValueError("Time-step cannot be zero or negative.\n")  # check_dt, gregsys.hpp:1401-1405
+        self.dt = float(timestep)
+        self.iterations = int(num_iterations)
+        self.G = parse_units(units_format)
+        self.eps = 0.0
+        self.theta = PI / 3
+        self.collisions = collisions
+        self.merge = merge_overlapping
+        self.precision = {"f64": _lib.PREC_F64, "mixed": _lib.PREC_MIXED}[precision]
+        n = 0 if m is None else len(m)
+        self.m = np.ascontiguousarray(np.zeros(0) if m is None else np.asarray(m, np.float64))
+        self.x = np.ascontiguousarray(np.zeros((n, 3)) if x is None else np.asarray(x, np.float64).reshape(n, 3))
+        self.v = np.ascontiguousarray(np.zeros((n, 3)) if v is None else np.asarray(v, np.float64).reshape(n, 3))
+        self.r = np.ascontiguousarray(np.zeros(n) if r is None else np.asarray(r, np.float64))
+        self.rest = np.ascontiguousarray(np.ones(n) if rest is None else np.asarray(rest, np.float64))
+        self.a = np.zeros((n, 3))
+        if (self.m < 0).any():
+            raise _lib.NbodyError(_lib.ERR_INVALID_ARGUMENT, "negative mass")
+        h = C.c_void_p()
+        check(L.gtd_system_create(C.byref(h), device, self.precision))
+        self._h = h
+        self._L = L
+        self.time_elapsed = 0.0
+        self.allow_overlap = allow_overlapping_bodies
+
+    # ---- reference accessors / setters (gregsys.hpp:1627-1672) --------------------------------
+    def num_bodies(self) -> int:
+        return len(self.m)
+
+    def G_val(self) -> float:
+        return self.G
+
+    def elapsed_time(self) -> float:
+        return self.time_elapsed
+
+    def set_iterations(self, number: int) -> bool:
+        if not number:
+            return False
+        self.iterations = int(number)
+        return True
+
+    def set_timestep(self, delta_t: float) -> bool:
+        if delta_t <= 0:
+            return False
+        self.dt = float(delta_t)
+        return True
+
+    def set_G_units(self, units_format: str) -> None:
+        self.G = parse_units(units_format)
+
+    def set_softening(self, epsilon: float) -> bool:
+        # the reference rejects eps < sqrt(LDBL_MIN) (~1.8e-2466): for a double that is eps <= 0
+        if not epsilon > 0:
+            return False
+        self.eps = float(epsilon)
+        return True
+
+    def set_bh_opening_angle(self, theta: float) -> bool:
+        if theta < 0 or theta >= PI:
+            return False
+        self.theta = float(theta)
+        return True
+
+    # ---- device round trip ------------------------------------------------------------------
+    def _push(self) -> None:
+        L = self._L
+        check(L.gtd_system_set_params(self._h, self.G, self.dt, max(self.iterations, 1), self.eps, self.theta))
+        mode = _lib.MERGE_COLL if self.merge and self.collisions else self.collisions
+        check(L.gtd_system_set_collisions(self._h, mode))
+        check(L.gtd_system_upload(self._h, len(self.m), ptr(self.m), ptr(self.r), ptr(self.rest), ptr(self.x),
+                                  ptr(self.v)))
+
+    def _pull(self) -> None:
+        n = C.c_int64()
+        L = self._L
+        check(L.gtd_system_num_bodies(self._h, C.byref(n)))
+        k = n.value
+        m, r, rest = np.zeros(k), np.zeros(k), np.zeros(k)
+        x, v, a = np.zeros((k, 3)), np.zeros((k, 3)), np.zeros((k, 3))
+        check(L.gtd_system_download(self._h, C.byref(n), ptr(m), ptr(r), ptr(rest), ptr(x), ptr(v), ptr(a)))
+        self.m, self.r, self.rest, self.x, self.v, self.a = m, r, rest, x, v, a
+
+    def evolve(self, integration_method: int = 16, continue_ev_if=None, for_each_bod=None,
+               for_all_bods=None) -> int:
+        """gtd::system::evolve (gregsys.hpp:2593-3071).  Returns the elapsed device time in ns.
+        With callbacks, the state is brought back to the host every step for them (the
+        reference's contract), the stepping itself stays on the GPU."""
+        self._push()
+        ns = C.c_int64()
+        if continue_ev_if is None and for_each_bod is None and for_all_bods is None:
+            check(self._L.gtd_system_evolve(self._h, integration_method, C.byref(ns)))
+            self._pull()
+            self.time_elapsed = self.iterations * self.dt
+            return ns.value
+        check(self._L.gtd_system_evolve_begin(self._h, integration_method))
+        steps = 0
+        while (continue_ev_if() if continue_ev_if is not None else steps < self.iterations):
+            check(self._L.gtd_system_evolve_steps(self._h, 1))
+            steps += 1
+            if for_all_bods is not None or for_each_bod is not None:
+                self._pull()
+                if for_all_bods is not None:
+                    for_all_bods(self)
+                if for_each_bod is not None:
+                    for i in range(len(self.m)):
+                        for_each_bod(self, i)
+                self._push()
+                check(self._L.gtd_system_evolve_begin(self._h, integration_method))
+        self._pull()
+        self.time_elapsed = steps * self.dt
+        return 0
+
+    def accelerations(self, method: int = 0) -> np.ndarray:
+        self._push()
+        a = np.zeros((len(self.m), 3))
+        check(self._L.gtd_system_accelerations(self._h, method, ptr(a)))
+        return a
+
+    def energy(self):
+        """(KE, PE, momentum[3], com[3]) in FP64 on the device (calc_energy, gregsys.hpp:608-630)."""
+        self._push()
+        ke, pe = C.c_double(), C.c_double()
+        p, com = np.zeros(3), np.zeros(3)
+        check(self._L.gtd_system_energy(self._h, C.byref(ke), C.byref(pe), ptr(p), ptr(com)))
+        return ke.value, pe.value, p, com
+
+    def launch_count(self) -> int:
+        c = C.c_uint64()
+        check(self._L.gtd_system_launch_count(self._h, C.byref(c)))
+        return c.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.gtd_system_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

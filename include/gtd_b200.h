@@ -1,0 +1,154 @@
+/* gtd_b200.h - C ABI of the B200 force-and-step engine behind the gtd:: N-body API.
+ *
+ * This is the boundary the drop-in C++ headers (include/gtd/*.hpp) call.  It takes plain pointers
+ * and sizes only (no CUDA, torch or C++ types), returns an int status (0 = GTD_OK) and keeps a
+ * thread-local message for gtd_last_error().  Every call is re-entrant per handle: a handle owns
+ * its device buffers and one CUDA stream, and no call touches global mutable state.
+ *
+ * Each entry point names the reference interface it replaces (file:line in
+ * GregW10/GregPackagesCPP).  Host arrays of vectors are triples: x3[3*i+k].  long double in the
+ * reference API is carried as double across this ABI (there is no long double on the device).
+ */
+#ifndef GTD_B200_H
+#define GTD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GTD_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define GTD_API __attribute__((visibility("default")))
+#else
+#define GTD_API
+#endif
+
+/* ---- status codes; the C++ wrapper maps them onto the reference's exception types ---------- */
+#define GTD_OK 0
+#define GTD_ERR_INVALID_ARGUMENT 1        /* std::invalid_argument (gregsys.hpp:1403, 1649, ...) */
+#define GTD_ERR_CUDA 2                    /* a CUDA runtime call failed */
+#define GTD_ERR_OUT_OF_MEMORY 3
+#define GTD_ERR_OVERLAPPING_BODIES 4      /* gtd::overlapping_bodies_error (gregbod.hpp:24, gregsys.hpp:322) */
+#define GTD_ERR_INVALID_BODY_PLACEMENT 5  /* gtd::invalid_body_placement (greg8tree.hpp:17, 140, 206) */
+#define GTD_ERR_INDISTINGUISHABLE 6       /* gtd::indistinguishable_bodies (greg8tree.hpp:32, 171-172) */
+#define GTD_ERR_NONFINITE 7               /* a NaN/Inf appeared in the device state */
+#define GTD_ERR_TIMEOUT 8                 /* a bounded device-side wait expired */
+#define GTD_ERR_TWO_BODY 9                /* gtd::two_body_error (gregbod.hpp:62, gregsys.hpp:2627-2629) */
+#define GTD_ERR_NO_DEVICE 10
+#define GTD_ERR_CAPACITY 11               /* a size beyond what the entry point supports */
+#define GTD_ERR_UNSUPPORTED 12            /* a method the reference leaves empty (rk4, rk3_8, ...) */
+
+/* ---- integration-method flags, identical to gtd::system's (gregsys.hpp:156-165) ------------- */
+#define GTD_TWO_BODY 1
+#define GTD_EULER 2
+#define GTD_MODIFIED_EULER 4
+#define GTD_MIDPOINT 8
+#define GTD_LEAPFROG_KDK 16
+#define GTD_LEAPFROG_DKD 32
+#define GTD_RK4 64
+#define GTD_RK3_8 128
+#define GTD_BARNES_HUT 65536
+
+/* ---- collision modes (gtd::system template parameter `collisions`, gregsys.hpp:166-168) ----- */
+#define GTD_NO_COLL 0
+#define GTD_OVERLAP_COLL 3  /* s_coll restitution impulses, gregsys.hpp:690-914 */
+#define GTD_MERGE_COLL 4    /* overlap merges with momentum conservation (body::operator+=) */
+
+/* ---- arithmetic of the pairwise force ---------------------------------------------------- */
+#define GTD_PREC_F64 0   /* FP64 everywhere */
+#define GTD_PREC_MIXED 1 /* FP32 pair forces and per-tile sums, FP64 Kahan sums across tiles, FP64 state */
+
+typedef struct gtd_system gtd_system;
+
+GTD_API const char *gtd_last_error(void);
+GTD_API int gtd_abi_version(void);
+GTD_API int gtd_device_count(int *count);
+
+/* A device-resident N-body system.  Replaces the storage of gtd::system (std::vector<body>,
+ * gregsys.hpp:179) for the duration of evolve(): the host vector stays authoritative between
+ * calls, the handle holds its SoA copy on the device. */
+GTD_API int gtd_system_create(gtd_system **out, int device, int precision);
+GTD_API int gtd_system_destroy(gtd_system *sys);
+
+/* Scalars of gtd::system: G (gregsys.hpp:171, 245-282), dt/half_dt (:202-203, set_timestep
+ * :1642-1651), iterations (:205, set_iterations :1636-1641), softening (:200-201, set_softening
+ * :1660-1666; used by Barnes-Hut only, as in the reference), bh_theta (:212, :1667-1672). */
+GTD_API int gtd_system_set_params(gtd_system *sys, double G, double dt, uint64_t iterations, double softening,
+                          double bh_theta);
+/* Collision handling (the `collisions` / `mergeOverlappingBodies` template parameters,
+ * gregsys.hpp:135-137): GTD_NO_COLL, GTD_OVERLAP_COLL or GTD_MERGE_COLL. */
+GTD_API int gtd_system_set_collisions(gtd_system *sys, int mode);
+
+/* Gather: the AoS gtd::body fields (gregbod.hpp:906-916) as SoA.  r, rest, v3 may be NULL
+ * (zero radius, restitution 1, zero velocity).  n == 0 is an empty system. */
+GTD_API int gtd_system_upload(gtd_system *sys, int64_t n, const double *m, const double *r, const double *rest,
+                      const double *x3, const double *v3);
+/* Scatter back.  *n receives the body count (it shrinks after merges); any output may be NULL.
+ * Bodies keep their upload order; merged-away bodies are removed, survivors keep their order. */
+GTD_API int gtd_system_download(gtd_system *sys, int64_t *n, double *m, double *r, double *rest, double *x3, double *v3,
+                        double *a3);
+GTD_API int gtd_system_num_bodies(const gtd_system *sys, int64_t *n);
+
+/* gtd::system::evolve(method) with no callbacks (gregsys.hpp:2593-3071): `iterations` steps of
+ * the method on the device, one upload/download around it done by the caller.  *elapsed_ns is
+ * the device time of the call (CUDA events), like the reference's returned duration.  Returns
+ * GTD_ERR_UNSUPPORTED for the methods the reference leaves empty. */
+GTD_API int gtd_system_evolve(gtd_system *sys, int method, int64_t *elapsed_ns);
+
+/* The same loop split for evolve() with callbacks: begin computes what the method needs before
+ * its first step (the initial acceleration of leapfrog KDK, gregsys.hpp:2947), steps advances k
+ * steps and leaves the state synchronised (positions and velocities at the same time). */
+GTD_API int gtd_system_evolve_begin(gtd_system *sys, int method);
+GTD_API int gtd_system_evolve_steps(gtd_system *sys, uint64_t k);
+
+/* Accelerations at the current positions: direct summation (calc_acc_and_e, gregsys.hpp:439-476)
+ * or, with GTD_BARNES_HUT in `method`, the Barnes-Hut walk.  a3 may be NULL (kept on device). */
+GTD_API int gtd_system_accelerations(gtd_system *sys, int method, double *a3);
+
+/* FP64 diagnostics: kinetic and potential energy (calc_energy gregsys.hpp:608-630), total
+ * momentum (sum of body::momentum, gregbod.hpp:595-597) and centre of mass (gregbod.hpp:1096-1106).
+ * Any output may be NULL. */
+GTD_API int gtd_system_energy(gtd_system *sys, double *ke, double *pe, double *p3, double *com3);
+
+/* ---- instrumentation (no counterpart in the reference, which only returns evolve()'s wall time,
+ * gregsys.hpp:2608-2625, 3061-3070) ------------------------------------------------------------ */
+
+/* Number of kernels this handle has launched since creation. */
+GTD_API int gtd_system_launch_count(const gtd_system *sys, uint64_t *count);
+/* The cudaStream_t the handle launches on, so a caller can record its own events on it. */
+GTD_API int gtd_system_stream(const gtd_system *sys, void **stream);
+/* enable != 0: bracket every force-kernel launch with CUDA events on the handle's stream and
+ * accumulate their durations; gtd_system_force_timing reads (and with reset != 0 clears) the total
+ * milliseconds and launch count. */
+GTD_API int gtd_system_time_force_kernels(gtd_system *sys, int enable);
+GTD_API int gtd_system_force_timing(gtd_system *sys, double *total_ms, uint64_t *launches, int reset);
+/* Measured throughput of a dependent-FMA microkernel on `device` (all SMs): precision
+ * GTD_PREC_MIXED gives FP32 FFMA FLOP/s, GTD_PREC_F64 gives FP64 DFMA FLOP/s (2 flops per FMA). */
+GTD_API int gtd_measure_fma_peak(int device, int precision, double *flops_per_s);
+
+/* ---- Barnes-Hut octree (greg8tree.hpp) ----------------------------------------------------- */
+
+/* Rebuilds the octree from the current positions: root box as bh_tree::find_min_max
+ * (greg8tree.hpp:1012-1047), 63-bit Morton codes along the reference's octant splits
+ * (set_corners :81-131, dispatch :146-210; depth 21), radix sort, linear octree in DFS pre-order
+ * with skip links, FP64 centres of mass (calc_com :213-281).  tree_float = 1 builds in T=float
+ * (positions rounded to float), 0 in T=double.  Replaces bh_tree::add_bodies + calc_com. */
+GTD_API int gtd_bh_build(gtd_system *sys, int tree_float);
+GTD_API int gtd_bh_tree_size(gtd_system *sys, int64_t *n_nodes, int64_t *n_leaves, double *box6);
+/* Copies the tree out (any pointer may be NULL): sorted codes and slot->body permutation [n],
+ * then per node in pre-order: depth, leaf flag, first slot, body count, skip, mass, com, width.
+ * Replaces walking bh_tree with its iterators (greg8tree.hpp:502-614, 1080-1085). */
+GTD_API int gtd_bh_tree_download(gtd_system *sys, uint64_t *codes, int32_t *perm, int8_t *depth, int8_t *is_leaf,
+                         int32_t *first, int32_t *count, int32_t *skip, double *mass, double *com3, double *width);
+/* Barnes-Hut accelerations of every body with the reference walk (cell_iterator,
+ * greg8tree.hpp:702-833) and bh_acc's force (gregsys.hpp:371-375, accumulated), on the tree of the
+ * last gtd_bh_build.  n_inter (per body, optional) counts accepted cells and leaves. */
+GTD_API int gtd_bh_accelerations(gtd_system *sys, double *a3, uint32_t *n_inter);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GTD_B200_H */

@@ -1,0 +1,297 @@
+"""ctypes access to the two CPU checkers.  TEST INFRASTRUCTURE ONLY.
+
+* ``Oracle``    - oracle/liboracle.so, the plain-C restatement (nbody_oracle.c).  Builds on any box
+                  with gcc (``ensure_built`` runs make).
+* ``RefOracle`` - oracle/_ref/libgtdref.so, the unmodified reference headers behind ref_oracle.cpp.
+                  Present only where it was built from the reference tree (it travels as a built
+                  file; it cannot be rebuilt where the reference sources are absent).
+
+Only tests/, the golden-fixture generator, ``__graft_entry__.smoke()`` and the CPU legs of
+bench.py import this module.  The product package never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REFLIB = os.path.join(HERE, "_ref", "libgtdref.so")
+REF_TREE = "/root/reference"
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_up = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+
+EULER, MODIFIED_EULER, MIDPOINT, LEAPFROG_KDK, LEAPFROG_DKD = 2, 4, 8, 16, 32
+
+
+def ensure_built(ref: bool = False) -> None:
+    """Compile the C restatement (and, when asked and the reference tree is present, the
+    reference-backed driver) with oracle/Makefile."""
+    targets = [LIB]
+    need = not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
+        os.path.getmtime(os.path.join(HERE, f)) for f in ("nbody_oracle.c", "nbody_oracle.h"))
+    if need:
+        subprocess.run(["make", "-s", "-C", HERE, LIB], check=True)
+    if ref and os.path.isdir(REF_TREE):
+        if (not os.path.exists(REFLIB) or
+                os.path.getmtime(REFLIB) < os.path.getmtime(os.path.join(HERE, "ref_oracle.cpp"))):
+            subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
+    del targets
+
+
+def _c3(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+
+
+class _Tree(C.Structure):
+    _fields_ = [("n", C.c_int), ("n_nodes", C.c_int), ("n_leaves", C.c_int),
+                ("code", C.POINTER(C.c_uint64)), ("perm", C.POINTER(C.c_int32)),
+                ("depth", C.POINTER(C.c_int8)), ("is_leaf", C.POINTER(C.c_int8)),
+                ("first", C.POINTER(C.c_int32)), ("count", C.POINTER(C.c_int32)),
+                ("skip", C.POINTER(C.c_int32)), ("mass", C.POINTER(C.c_double)),
+                ("com3", C.POINTER(C.c_double)), ("width", C.POINTER(C.c_double)),
+                ("box6", C.c_double * 6)]
+
+
+class Oracle:
+    """The plain-C restatement of the reference arithmetic."""
+
+    def __init__(self):
+        ensure_built()
+        L = self.lib = C.CDLL(LIB)
+        L.orc_G_units.restype = C.c_longdouble
+        L.orc_G_units.argtypes = [C.c_uint64] * 6
+        L.orc_G_units_into.argtypes = [C.c_uint64] * 6 + [C.POINTER(C.c_longdouble)]
+        L.orc_direct_acc.argtypes = [C.c_int, _dp, _dp, C.POINTER(C.c_longdouble), _dp]
+        L.orc_evolve.restype = C.c_int
+        L.orc_evolve.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_longdouble,
+                                 C.c_uint64, C.POINTER(C.c_longdouble)]
+        L.orc_s_coll.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.orc_energy.argtypes = [C.c_int, _dp, _dp, _dp, C.POINTER(C.c_longdouble), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double)]
+        L.orc_merge_pair.argtypes = [_dp, _dp]
+        L.orc_merge_overlapping.restype = C.c_int
+        L.orc_merge_overlapping.argtypes = [C.c_int, _dp]
+        L.orc_bh_root_box.argtypes = [C.c_int, _dp, C.c_int, _dp]
+        L.orc_bh_build.restype = C.c_int
+        L.orc_bh_build.argtypes = [C.c_int, _dp, _dp, C.c_int, C.POINTER(_Tree)]
+        L.orc_bh_free.argtypes = [C.POINTER(_Tree)]
+        L.orc_bh_acc.argtypes = [C.POINTER(_Tree), _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _up]
+        L.orc_bench_kdk.restype = C.c_int
+        L.orc_bench_kdk.argtypes = [C.c_int, _dp, _dp, _dp, C.c_longdouble, C.c_uint64, C.POINTER(C.c_longdouble),
+                                    C.c_int, C.POINTER(C.c_longlong)]
+
+    def bench_kdk(self, m, x, v, dt, steps, G, threads):
+        """Wall seconds for `threads` concurrent copies of orc_evolve(leapfrog_kdk)."""
+        ns = C.c_longlong()
+        self.lib.orc_bench_kdk(len(m), _c3(m), _c3(x), _c3(v), dt, steps, C.byref(G), threads, C.byref(ns))
+        return ns.value * 1e-9
+
+    @staticmethod
+    def G_units(units: str):
+        """The reference's G for a units string, as a Python float of the long double."""
+        parts = units.replace(" ", "").split(",")
+        nums = []
+        for p in parts:
+            a, b = p[1:].split(":")
+            nums += [int(a), int(b)]
+        return nums
+
+    def G(self, units: str = "M66743:66740,D1:1,T1:1"):
+        """The reference's G as a ctypes long double (all 64 mantissa bits kept; a Python float
+        would round it to double)."""
+        g = C.c_longdouble()
+        self.lib.orc_G_units_into(*self.G_units(units), C.byref(g))
+        return g
+
+    def direct_acc(self, m, x, G):
+        n = len(m)
+        a = np.zeros(3 * n)
+        self.lib.orc_direct_acc(n, _c3(m), _c3(x), C.byref(G), a)
+        return a.reshape(n, 3)
+
+    def evolve(self, method, m, x, v, dt, steps, G, r=None, rest=None, coll=0):
+        n = len(m)
+        x3, v3, a3 = _c3(x).copy(), _c3(v).copy(), np.zeros(3 * n)
+        r = _c3(np.zeros(n) if r is None else r)
+        rest = _c3(np.ones(n) if rest is None else rest)
+        rc = self.lib.orc_evolve(method, coll, n, _c3(m), r, rest, x3, v3, a3, dt, steps, C.byref(G))
+        if rc:
+            raise RuntimeError(f"orc_evolve failed ({rc})")
+        return x3.reshape(n, 3), v3.reshape(n, 3), a3.reshape(n, 3)
+
+    def s_coll(self, m, r, rest, x, v):
+        n = len(m)
+        v3 = _c3(v).copy()
+        self.lib.orc_s_coll(n, _c3(m), _c3(r), _c3(rest), _c3(x), v3)
+        return v3.reshape(n, 3)
+
+    def energy(self, m, x, v, G):
+        ke, pe = C.c_double(), C.c_double()
+        self.lib.orc_energy(len(m), _c3(m), _c3(x), _c3(v), C.byref(G), C.byref(ke), C.byref(pe))
+        return ke.value, pe.value
+
+    def merge_pair(self, a12, b12):
+        a = _c3(a12).copy()
+        self.lib.orc_merge_pair(a, _c3(b12))
+        return a
+
+    def merge_overlapping(self, rows12):
+        rows = _c3(rows12).copy()
+        n = self.lib.orc_merge_overlapping(len(rows) // 12, rows)
+        return rows.reshape(-1, 12)[:n].copy()
+
+    def root_box(self, x, is_float):
+        box = np.zeros(6)
+        self.lib.orc_bh_root_box(len(x), _c3(x), int(is_float), box)
+        return box
+
+    def bh_tree(self, x, m, is_float):
+        """Host rebuild of the linear octree; returns a dict of numpy arrays."""
+        t = _Tree()
+        n = len(m)
+        rc = self.lib.orc_bh_build(n, _c3(x), _c3(m), int(is_float), C.byref(t))
+        if rc:
+            raise RuntimeError(f"orc_bh_build failed ({rc})")
+        nn = t.n_nodes
+
+        def arr(p, k, dt):
+            return np.ctypeslib.as_array(p, shape=(k,)).astype(dt).copy() if k else np.zeros(0, dt)
+
+        out = dict(n=n, n_nodes=nn, n_leaves=t.n_leaves, box=np.array(t.box6[:]),
+                   code=arr(t.code, n, np.uint64), perm=arr(t.perm, n, np.int32),
+                   depth=arr(t.depth, nn, np.int8), is_leaf=arr(t.is_leaf, nn, np.int8),
+                   first=arr(t.first, nn, np.int32), count=arr(t.count, nn, np.int32),
+                   skip=arr(t.skip, nn, np.int32), mass=arr(t.mass, nn, np.float64),
+                   com=arr(t.com3, 3 * nn, np.float64).reshape(nn, 3), width=arr(t.width, nn, np.float64))
+        out["_tree"] = t
+        return out
+
+    def bh_free(self, tree):
+        self.lib.orc_bh_free(C.byref(tree["_tree"]))
+
+    def bh_acc(self, tree, x, m, is_float, theta, eps, G):
+        n = tree["n"]
+        a = np.zeros(3 * n)
+        cnt = np.zeros(n, np.uint32)
+        self.lib.orc_bh_acc(C.byref(tree["_tree"]), _c3(x), _c3(m), int(is_float), theta, eps, G, a, cnt)
+        return a.reshape(n, 3), cnt
+
+
+class RefOracle:
+    """The unmodified reference headers behind ref_oracle.cpp (oracle/_ref/libgtdref.so)."""
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REFLIB)
+
+    def __init__(self):
+        if not os.path.exists(REFLIB):
+            raise FileNotFoundError(REFLIB)
+        L = self.lib = C.CDLL(REFLIB)
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_evolve.restype = C.c_int
+        L.ref_evolve.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_uint64,
+                                 C.c_char_p, _dp, _dp, _dp, C.POINTER(C.c_longlong)]
+        L.ref_G.restype = C.c_int
+        L.ref_G.argtypes = [C.c_char_p, C.POINTER(C.c_longdouble)]
+        L.ref_energy.restype = C.c_int
+        L.ref_energy.argtypes = [C.c_int, _dp, _dp, _dp, C.c_char_p, C.POINTER(C.c_longdouble),
+                                 C.POINTER(C.c_longdouble)]
+        L.ref_check_overlap_merge.restype = C.c_int
+        L.ref_check_overlap_merge.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_int), _dp, _dp, _dp,
+                                              _dp]
+        L.ref_merge_pair.restype = C.c_int
+        L.ref_merge_pair.argtypes = [_dp, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double), _dp, _dp, _dp,
+                                     C.POINTER(C.c_double)]
+        L.ref_bh_tree_dump.restype = C.c_long
+        L.ref_bh_tree_dump.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_long, _ip, _ip, _dp, _dp, _dp, _dp, _dp]
+        L.ref_bh_acc.restype = C.c_int
+        L.ref_bh_acc.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_char_p, _dp,
+                                 C.POINTER(C.c_uint64)]
+        L.ref_bench_kdk.restype = C.c_int
+        L.ref_bench_kdk.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, C.c_uint64, C.c_char_p, C.c_int,
+                                    C.POINTER(C.c_longlong)]
+        L.ref_bh_kdk.restype = C.c_int
+        L.ref_bh_kdk.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, C.c_uint64, C.c_double, C.c_double,
+                                 C.c_char_p, _dp, _dp, _dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+
+    def _chk(self, rc):
+        if rc < 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return rc
+
+    def G(self, units="M66743:66740,D1:1,T1:1"):
+        g = C.c_longdouble()
+        self._chk(self.lib.ref_G(units.encode(), C.byref(g)))
+        return g.value
+
+    def bench_kdk(self, m, x, v, dt, steps, threads, units="M66743:66740,D1:1,T1:1"):
+        """Wall seconds for `threads` concurrent reference evolve(leapfrog_kdk) calls."""
+        ns = C.c_longlong()
+        self._chk(self.lib.ref_bench_kdk(len(m), _c3(m), _c3(x), _c3(v), dt, steps, units.encode(), threads,
+                                         C.byref(ns)))
+        return ns.value * 1e-9
+
+    def evolve(self, method, m, x, v, dt, steps, units="M66743:66740,D1:1,T1:1", r=None, rest=None, coll=0):
+        n = len(m)
+        xo, vo, ao = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n)
+        r = _c3(np.zeros(n) if r is None else r)
+        rest = _c3(np.ones(n) if rest is None else rest)
+        ns = C.c_longlong()
+        self._chk(self.lib.ref_evolve(method, coll, n, _c3(m), r, rest, _c3(x), _c3(v), dt, steps, units.encode(),
+                                      xo, vo, ao, C.byref(ns)))
+        return xo.reshape(n, 3), vo.reshape(n, 3), ao.reshape(n, 3), ns.value
+
+    def energy(self, m, x, v, units="M66743:66740,D1:1,T1:1"):
+        ke, pe = C.c_longdouble(), C.c_longdouble()
+        self._chk(self.lib.ref_energy(len(m), _c3(m), _c3(x), _c3(v), units.encode(), C.byref(ke), C.byref(pe)))
+        return float(ke.value), float(pe.value)
+
+    def check_overlap_merge(self, m, r, rest, x, v):
+        n = len(m)
+        no = C.c_int()
+        mo, ro, xo, vo = np.zeros(n), np.zeros(n), np.zeros(3 * n), np.zeros(3 * n)
+        self._chk(self.lib.ref_check_overlap_merge(n, _c3(m), _c3(r), _c3(rest), _c3(x), _c3(v), C.byref(no), mo,
+                                                   ro, xo, vo))
+        k = no.value
+        return mo[:k], ro[:k], xo.reshape(n, 3)[:k], vo.reshape(n, 3)[:k]
+
+    def merge_pair(self, a12, b12):
+        m, r, rest = C.c_double(), C.c_double(), C.c_double()
+        x, v, a = np.zeros(3), np.zeros(3), np.zeros(3)
+        self._chk(self.lib.ref_merge_pair(_c3(a12), _c3(b12), C.byref(m), C.byref(r), x, v, a, C.byref(rest)))
+        return np.concatenate([[m.value, r.value, rest.value], x, v, a])
+
+    def bh_tree_dump(self, x, m, is_float, max_nodes=None):
+        n = len(m)
+        cap = max_nodes or 8 * n + 64
+        depth, body = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+        mass, com, btm, top = np.zeros(cap), np.zeros(3 * cap), np.zeros(3 * cap), np.zeros(3 * cap)
+        box = np.zeros(6)
+        k = self._chk(self.lib.ref_bh_tree_dump(int(is_float), n, _c3(x), _c3(m), cap, depth, body, mass, com, btm,
+                                                top, box))
+        if k > cap:
+            return self.bh_tree_dump(x, m, is_float, k)
+        return dict(n_nodes=k, depth=depth[:k], body=body[:k], mass=mass[:k], com=com.reshape(-1, 3)[:k],
+                    btm=btm.reshape(-1, 3)[:k], top=top.reshape(-1, 3)[:k], box=box)
+
+    def bh_acc(self, x, m, theta, eps=0.0, units="M66743:66740,D1:1,T1:1"):
+        n = len(m)
+        a = np.zeros(3 * n)
+        cnt = C.c_uint64()
+        self._chk(self.lib.ref_bh_acc(n, _c3(x), _c3(m), theta, eps, units.encode(), a, C.byref(cnt)))
+        return a.reshape(n, 3), cnt.value
+
+    def bh_kdk(self, m, x, v, dt, steps, theta, eps=0.0, units="M66743:66740,D1:1,T1:1"):
+        n = len(m)
+        xo, vo, ao = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n)
+        tb, tw = C.c_longlong(), C.c_longlong()
+        self._chk(self.lib.ref_bh_kdk(n, _c3(m), _c3(x), _c3(v), dt, steps, theta, eps, units.encode(), xo, vo, ao,
+                                      C.byref(tb), C.byref(tw)))
+        return xo.reshape(n, 3), vo.reshape(n, 3), ao.reshape(n, 3), tb.value, tw.value

@@ -1,0 +1,102 @@
+"""Generates the golden fixtures in tests/golden/ by running the UNMODIFIED reference headers
+(through oracle/_ref/libgtdref.so, built from the reference tree by oracle/Makefile).
+
+Run here, where the reference tree is mounted:  python tests/golden/make_golden.py
+The fixtures are small .npz files; the tests read them, never the reference tree.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from gregpackagescpp_b200.ics import AU, UNITS_G6674, plummer  # noqa: E402
+from oracle.oracle import RefOracle, ensure_built  # noqa: E402
+
+METHODS = {"euler": 2, "modified_euler": 4, "midpoint": 8, "leapfrog_kdk": 16, "leapfrog_dkd": 32}
+
+
+def main():
+    ensure_built(ref=True)
+    r = RefOracle()
+    out = {}
+    # direct summation, every method, 10 steps of one hour (the configuration of the 1e-12 bar)
+    m, x, v = plummer(64, 1)
+    out["direct_m"], out["direct_x"], out["direct_v"] = m, x, v
+    for name, meth in METHODS.items():
+        xo, vo, ao, _ = r.evolve(meth, m, x, v, 3600.0, 10, UNITS_G6674)
+        out[f"direct_{name}_x"], out[f"direct_{name}_v"], out[f"direct_{name}_a"] = xo, vo, ao
+    # odd N, other seed, KDK only
+    m2, x2, v2 = plummer(37, 2)
+    out["odd_m"], out["odd_x"], out["odd_v"] = m2, x2, v2
+    xo, vo, ao, _ = r.evolve(16, m2, x2, v2, 3600.0, 10, UNITS_G6674)
+    out["odd_kdk_x"], out["odd_kdk_v"], out["odd_kdk_a"] = xo, vo, ao
+    # overlap collisions with restitution (collisions = 3)
+    m3, x3, v3 = plummer(128, 3)
+    rad = np.full(128, 0.08 * AU)
+    rest = np.random.default_rng(0).uniform(0.2, 1.0, 128)
+    out["coll_m"], out["coll_x"], out["coll_v"], out["coll_r"], out["coll_rest"] = m3, x3, v3, rad, rest
+    for name, meth in METHODS.items():
+        xo, vo, ao, _ = r.evolve(meth, m3, x3, v3, 3600.0, 5, UNITS_G6674, r=rad, rest=rest, coll=3)
+        out[f"coll_{name}_x"], out[f"coll_{name}_v"] = xo, vo
+    # energy
+    ke, pe = r.energy(m, x, v, UNITS_G6674)
+    out["energy_ke"], out["energy_pe"] = np.array(ke), np.array(pe)
+    out["G_6674"] = np.array(r.G(UNITS_G6674))
+    out["G_SI"] = np.array(r.G("M1:1,D1:1,T1:1"))
+    out["G_odd"] = np.array(r.G("M3:7,D2:5,T11:13"))
+    # body::operator+= merges
+    rng = np.random.default_rng(5)
+    pairs_a, pairs_b, merged = [], [], []
+    for _ in range(16):
+        a = np.concatenate([[rng.uniform(1e24, 1e30), rng.uniform(1e5, 1e7), rng.uniform(0, 1)],
+                            rng.normal(0, AU, 3), rng.normal(0, 3e4, 3), rng.normal(0, 1e-3, 3)])
+        b = np.concatenate([[rng.uniform(1e24, 1e30), rng.uniform(1e5, 1e7), rng.uniform(0, 1)],
+                            rng.normal(0, AU, 3), rng.normal(0, 3e4, 3), rng.normal(0, 1e-3, 3)])
+        pairs_a.append(a)
+        pairs_b.append(b)
+        merged.append(r.merge_pair(a, b))
+    out["merge_a"], out["merge_b"], out["merge_out"] = np.array(pairs_a), np.array(pairs_b), np.array(merged)
+    # check_overlap with merging: the case the reference's scan handles (overlap of the last two bodies)
+    m4, x4, v4 = plummer(12, 4)
+    x4[-1] = x4[-2] + np.array([0.3, 0.2, 0.1]) * 1e9
+    rad4 = np.full(12, 1e9)
+    rest4 = np.linspace(0.3, 0.9, 12)
+    mo, ro, xo, vo = r.check_overlap_merge(m4, rad4, rest4, x4, v4)
+    out["ovl_m"], out["ovl_x"], out["ovl_v"], out["ovl_r"], out["ovl_rest"] = m4, x4, v4, rad4, rest4
+    out["ovl_out_m"], out["ovl_out_r"], out["ovl_out_x"], out["ovl_out_v"] = mo, ro, xo, vo
+    # Barnes-Hut: reference octree (T=double and T=float) and the corrected walk
+    m5, x5, v5 = plummer(2000, 7)
+    out["bh_m"], out["bh_x"], out["bh_v"] = m5, x5, v5
+    for isf in (0, 1):
+        d = r.bh_tree_dump(x5, m5, isf)
+        out[f"bh_tree{isf}_depth"] = d["depth"].astype(np.int8)
+        out[f"bh_tree{isf}_body"] = d["body"].astype(np.int32)
+        out[f"bh_tree{isf}_box"] = d["box"]
+        # cell width as the opening test forms it, top.x - btm.x in T (greg8tree.hpp:753-755)
+        if isf:
+            out[f"bh_tree{isf}_width"] = (d["top"][:, 0].astype(np.float32) -
+                                          d["btm"][:, 0].astype(np.float32)).astype(np.float64)
+        else:
+            out[f"bh_tree{isf}_width"] = d["top"][:, 0] - d["btm"][:, 0]
+        if isf == 0:
+            out["bh_tree0_com"] = d["com"]
+            out["bh_tree0_mass"] = d["mass"]
+    a, cnt = r.bh_acc(x5, m5, 0.5, 0.0, UNITS_G6674)
+    out["bh_acc"], out["bh_count"] = a, np.array(cnt)
+    m6, x6, v6 = plummer(300, 8)
+    out["bhk_m"], out["bhk_x"], out["bhk_v"] = m6, x6, v6
+    xo, vo, ao, _, _ = r.bh_kdk(m6, x6, v6, 3600.0, 5, 0.5, 0.0, UNITS_G6674)
+    out["bhk_xo"], out["bhk_vo"], out["bhk_ao"] = xo, vo, ao
+    path = os.path.join(HERE, "reference_golden.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes,", len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,89 @@
+"""Direct-summation evolve on the B200 through the C ABI against the CPU oracle (a restatement of
+the reference pinned bit for bit to it) and the reference's own golden vectors.
+
+Bar (FP64): positions and velocities within 1e-12 relative after 10 steps."""
+import numpy as np
+import pytest
+
+from gregpackagescpp_b200 import System
+from gregpackagescpp_b200.ics import UNITS_G6674, plummer
+
+pytestmark = pytest.mark.gpu
+
+METHODS = {"euler": 2, "modified_euler": 4, "midpoint": 8, "leapfrog_kdk": 16, "leapfrog_dkd": 32}
+RTOL = 1e-12
+
+
+def rel_err(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize("name", list(METHODS))
+def test_methods_vs_reference_golden(gpu, golden, name):
+    g = golden
+    s = System(g["direct_m"], g["direct_x"], g["direct_v"], timestep=3600.0, num_iterations=10,
+               units_format=UNITS_G6674)
+    s.evolve(METHODS[name])
+    assert rel_err(s.x, g[f"direct_{name}_x"]) < RTOL
+    assert rel_err(s.v, g[f"direct_{name}_v"]) < RTOL
+    assert rel_err(s.a, g[f"direct_{name}_a"]) < 1e-11
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 37, 255, 256, 257, 511, 512, 513, 1500])
+@pytest.mark.parametrize("name", ["leapfrog_kdk", "modified_euler"])
+def test_ragged_sizes_vs_oracle(gpu, oracle, n, name):
+    m, x, v = plummer(n, 100 + n)
+    s = System(m, x, v, timestep=3600.0, num_iterations=10, units_format=UNITS_G6674)
+    s.evolve(METHODS[name])
+    xo, vo, ao = oracle.evolve(METHODS[name], m, x, v, 3600.0, 10, oracle.G(UNITS_G6674))
+    assert rel_err(s.x, xo) < RTOL
+    assert rel_err(s.v, vo) < RTOL or n == 1
+
+
+def test_empty_system_is_noop(gpu):
+    s = System(np.zeros(0), np.zeros((0, 3)), np.zeros((0, 3)), timestep=1.0, num_iterations=5)
+    assert s.evolve(16) == 0
+    assert s.num_bodies() == 0
+
+
+def test_kdk_1024_thousand_steps_energy(gpu, oracle):
+    """The reference's CPU configuration: N=1024 Plummer, KDK, dt=3600 s; 100 steps here (the full
+    1000-step run is in the benchmark)."""
+    m, x, v = plummer(1024, 1)
+    s = System(m, x, v, timestep=3600.0, num_iterations=100, units_format=UNITS_G6674)
+    ke0, pe0, _, _ = s.energy()
+    s.evolve(16)
+    ke1, pe1, p1, _ = s.energy()
+    xo, vo, _ = oracle.evolve(16, m, x, v, 3600.0, 100, oracle.G(UNITS_G6674))
+    assert rel_err(s.x, xo) < 1e-10
+    assert abs((ke1 + pe1) - (ke0 + pe0)) / abs(ke0 + pe0) < 1e-6
+
+
+def test_energy_diagnostic_vs_oracle(gpu, oracle, golden):
+    g = golden
+    s = System(g["direct_m"], g["direct_x"], g["direct_v"], units_format=UNITS_G6674)
+    ke, pe, p, com = s.energy()
+    assert abs(ke - float(g["energy_ke"])) <= 1e-13 * abs(ke)
+    assert abs(pe - float(g["energy_pe"])) <= 1e-13 * abs(pe)
+
+
+def test_mixed_acceleration_error(gpu):
+    """Mixed path: relative acceleration error against the FP64 path (bar: 1e-6, RMS over bodies)."""
+    m, x, v = plummer(16384, 21)
+    s64 = System(m, x, v, units_format=UNITS_G6674)
+    a64 = s64.accelerations()
+    smx = System(m, x, v, units_format=UNITS_G6674, precision="mixed")
+    amx = smx.accelerations()
+    rel = np.linalg.norm(amx - a64, axis=1) / np.linalg.norm(a64, axis=1)
+    rms = float(np.sqrt((rel ** 2).mean()))
+    assert rms < 1e-6, (rms, float(np.median(rel)), float(rel.max()))
+
+
+def test_mixed_kdk_tracks_fp64(gpu):
+    m, x, v = plummer(4096, 22)
+    a = System(m, x, v, timestep=3600.0, num_iterations=20, units_format=UNITS_G6674)
+    b = System(m, x, v, timestep=3600.0, num_iterations=20, units_format=UNITS_G6674, precision="mixed")
+    a.evolve(16)
+    b.evolve(16)
+    assert rel_err(b.x, a.x) < 1e-9
+    assert rel_err(b.v, a.v) < 1e-6
