@@ -25,7 +25,11 @@ import sys
 import threading
 import time
 
+import faulthandler
+
 import numpy as np
+
+faulthandler.enable()
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -46,8 +50,8 @@ def parse_args():
     p.add_argument("--fp64-steps", type=int, default=3)
     p.add_argument("--e2e-calls", type=int, default=2)
     p.add_argument("--e2e-iterations", type=int, default=5)
-    p.add_argument("--cpu-sample-n", type=int, default=16384)
-    p.add_argument("--cpu-sample-steps", type=int, default=1)
+    p.add_argument("--cpu-sample-n", type=int, default=8192)
+    p.add_argument("--cpu-sample-steps", type=int, default=3)
     return p.parse_args()
 
 
@@ -156,21 +160,38 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------------
 # CPU baselines (the reference's own evolve, else the C port of it)
 # ------------------------------------------------------------------------------------------------
-def cpu_sample(n_sample, steps, seed, threads):
-    """Times `threads` independent copies of evolve(leapfrog_kdk) on an n_sample Plummer system for
-    `steps` steps.  Returns (interactions/s, kind, seconds)."""
+def _cpu_copy(job):
+    """One single-threaded evolve(leapfrog_kdk) of an n-body Plummer system in this (spawned)
+    process; returns (interactions, evolve seconds, kind).  Construction is excluded: the
+    reference gives every body a unique ID by scanning a process-wide set from 0
+    (gregbod.hpp:111-117), so building n bodies costs O(n^2) before evolve starts."""
+    n_sample, steps, seed = job
     from gregpackagescpp_b200.ics import UNITS_G6674, plummer
     from oracle.oracle import Oracle, RefOracle, ensure_built
     m, x, v = plummer(n_sample, seed)
-    evals = steps + 1  # evolve(leapfrog_kdk) computes the initial acceleration, then one per step
-    inter = float(threads) * evals * n_sample * (n_sample - 1)
+    inter = float(steps + 1) * n_sample * (n_sample - 1)  # initial acceleration + one evaluation per step
     if RefOracle.available():
-        secs = RefOracle().bench_kdk(m, x, v, 3600.0, steps, threads, UNITS_G6674)
-        return inter / secs, "reference", secs
+        return inter, RefOracle().bench_kdk(m, x, v, 3600.0, steps, 1, UNITS_G6674), "reference"
     ensure_built()
     o = Oracle()
-    secs = o.bench_kdk(m, x, v, 3600.0, steps, o.G(UNITS_G6674), threads)
-    return inter / secs, "port", secs
+    return inter, o.bench_kdk(m, x, v, 3600.0, steps, o.G(UNITS_G6674), 1), "port"
+
+
+def cpu_sample(n_sample, steps, seed, copies):
+    """Aggregate CPU throughput of `copies` concurrent single-threaded evolve() runs, one process
+    each (the reference's evolve is single-threaded; concurrent independent systems are how its
+    drivers use several cores, bdsim.cpp:82-113).  Returns (interactions/s, kind, max seconds)."""
+    if copies == 1:
+        inter, secs, kind = _cpu_copy((n_sample, steps, seed))
+        return inter / secs, kind, secs
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(copies) as pool:
+        res = pool.map(_cpu_copy, [(n_sample, steps, seed)] * copies)
+    return sum(i / s for i, s, _ in res), res[0][2], max(s for _, s, _ in res)
+
+
+def stage(msg: str) -> None:
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
 
 
 def host_threads() -> int:
@@ -248,6 +269,7 @@ def run_ours(args, rank, world, local):
         check(L.gtd_system_launch_count(h, C.byref(c)))
         return c.value
 
+    stage("accuracy")
     # --- accuracy of the mixed force against the FP64 one at the initial state (untimed)
     h64, hmx = make(_lib.PREC_F64), make(_lib.PREC_MIXED)
     a64, amx = np.zeros(3 * n), np.zeros(3 * n)
@@ -255,6 +277,7 @@ def run_ours(args, rank, world, local):
     check(L.gtd_system_accelerations(hmx, 0, amx.ctypes.data))
     rel = np.linalg.norm((amx - a64).reshape(n, 3), axis=1) / np.linalg.norm(a64.reshape(n, 3), axis=1)
 
+    stage("fp64 throughput")
     # --- FP64 GPU path throughput (same workload, fewer steps)
     check(L.gtd_system_evolve_begin(h64, 16))
     check(L.gtd_system_evolve_steps(h64, 1))
@@ -268,6 +291,7 @@ def run_ours(args, rank, world, local):
     fp64_value = args.fp64_steps * pair / (e0.elapsed_time(e1) * 1e-3)
     check(L.gtd_system_destroy(h64))
 
+    stage("mixed timed loop")
     # --- mixed path: the timed hot loop
     E0 = energy(hmx)
     check(L.gtd_system_evolve_begin(hmx, 16))
@@ -306,6 +330,7 @@ def run_ours(args, rank, world, local):
     check(L.gtd_system_destroy(hmx))
     del flush
 
+    stage("peaks")
     # --- roofline: the force kernel (FP32 pipe); denominator measured on this GPU
     peak = C.c_double()
     check(L.gtd_measure_fma_peak(local, _lib.PREC_MIXED, C.byref(peak)))
@@ -314,6 +339,7 @@ def run_ours(args, rank, world, local):
     avg_force_s = force_ms.value * 1e-3 / max(force_n.value, 1)
     achieved = FLOPS_PER_INTERACTION * pair / avg_force_s
 
+    stage("e2e")
     # --- end to end through the public C ABI with host buffers (upload, evolve, download)
     iters = args.e2e_iterations
     he = C.c_void_p()
@@ -337,13 +363,13 @@ def run_ours(args, rank, world, local):
     d2h = (xo.nbytes + vo.nbytes + ao.nbytes) * args.e2e_calls / e2e_steps
 
     cpu = None
-    if rank == 0 and world == 1:
-        threads = host_threads()
-        cval, kind, secs = cpu_sample(args.cpu_sample_n, args.cpu_sample_steps, args.seed, threads)
-        cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": kind,
-               "sample": f"{threads} concurrent copies of the reference evolve(leapfrog_kdk) on an N="
+    if rank == 0 and world == 1 and args.cpu_sample_n > 0:
+        stage("cpu baseline sample")
+        cval, kind, secs = cpu_sample(args.cpu_sample_n, args.cpu_sample_steps, args.seed, 1)
+        cpu = {"value": cval, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"the reference evolve(leapfrog_kdk) (single-threaded by design) on an N="
                          f"{args.cpu_sample_n} Plummer sphere, {args.cpu_sample_steps} step(s) "
-                         f"({args.cpu_sample_steps + 1} force evaluations each), {secs:.1f} s wall"}
+                         f"({args.cpu_sample_steps + 1} force evaluations), {secs:.1f} s of evolve time"}
 
     if rank == 0:
         line = {

@@ -180,6 +180,7 @@ __global__ void __launch_bounds__(kThreads, 2) force_mixed_kernel(ForceKArgs a) 
     __shared__ __align__(16) float ty[2][kThreads];
     __shared__ __align__(16) float tz[2][kThreads];
     __shared__ __align__(16) float tm[2][kThreads];
+    __shared__ double cred[3][kThreads];
     const int t = threadIdx.x;
     int64_t s, e;
     cta_range(a, blockIdx.x, s, e);
@@ -190,7 +191,34 @@ __global__ void __launch_bounds__(kThreads, 2) force_mixed_kernel(ForceKArgs a) 
         const int64_t row_end = min(e, (r + 1) * a.tiles);
         const int64_t jt1 = row_end - r * a.tiles;
         const int64_t row0 = r * a.bi;
-        const double4 c = a.src[row0];
+        // the row's FP32 frame is centred on the mean position of its bodies
+        double px[I], py[I], pz[I];
+        double msx = 0.0, msy = 0.0, msz = 0.0;
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            const int64_t i = row0 + k * kThreads + t;
+            px[k] = py[k] = pz[k] = 0.0;
+            if (i < a.n) {
+                const double4 p = a.src[i];
+                px[k] = p.x; py[k] = p.y; pz[k] = p.z;
+                msx += p.x; msy += p.y; msz += p.z;
+            }
+        }
+        cred[0][t] = msx;
+        cred[1][t] = msy;
+        cred[2][t] = msz;
+        __syncthreads();
+        for (int w = kThreads / 2; w > 0; w >>= 1) {
+            if (t < w) {
+                cred[0][t] += cred[0][t + w];
+                cred[1][t] += cred[1][t + w];
+                cred[2][t] += cred[2][t + w];
+            }
+            __syncthreads();
+        }
+        const double inv_rows = 1.0 / (double)min((int64_t)a.bi, a.n - row0);
+        const double3 c = make_double3(cred[0][0] * inv_rows, cred[1][0] * inv_rows, cred[2][0] * inv_rows);
+        __syncthreads();
         float2 nx[I], ny[I], nz[I];
         double sx[I], sy[I], sz[I], cx[I], cy[I], cz[I];
 #pragma unroll
@@ -198,10 +226,9 @@ __global__ void __launch_bounds__(kThreads, 2) force_mixed_kernel(ForceKArgs a) 
             const int64_t i = row0 + k * kThreads + t;
             float fx = 0.f, fy = 0.f, fz = 0.f;
             if (i < a.n) {
-                const double4 p = a.src[i];
-                fx = (float)(p.x - c.x);
-                fy = (float)(p.y - c.y);
-                fz = (float)(p.z - c.z);
+                fx = (float)(px[k] - c.x);
+                fy = (float)(py[k] - c.y);
+                fz = (float)(pz[k] - c.z);
             }
             nx[k] = make_float2(-fx, -fx);
             ny[k] = make_float2(-fy, -fy);

@@ -24,6 +24,7 @@ struct gtd_system {
 
     // bodies: position + mass double-buffered, velocity, acceleration, radius, restitution
     int64_t n = 0, cap = 0;
+    int64_t n_uploaded = 0;  // bodies at upload (n shrinks after merges)
     double4 *pm[2] = {nullptr, nullptr};
     int cur = 0;
     double4 *vel = nullptr, *acc = nullptr;
@@ -53,29 +54,46 @@ struct gtd_system {
     double force_ms = 0.0;
     uint64_t force_launches = 0;
 
-    // Barnes-Hut tree (octree.cu)
+    // Barnes-Hut linear octree (octree.cu); arrays indexed by sorted slot [n] or by node [cap]
     bool tree_valid = false;
     int tree_float = 1;
-    int64_t tree_cap_n = 0, tree_cap_nodes = 0;
+    int64_t tree_n = 0;                 // bodies the n-sized arrays were sized for
+    int64_t node_cap = 0;               // nodes the node-sized arrays hold
     int64_t n_nodes = 0, n_leaves = 0;
-    double box[6] = {0, 0, 0, 0, 0, 0};
-    void *tree_buf = nullptr;  // one allocation carved into the arrays below
-    size_t tree_bytes = 0;
+    void *tree_nbuf = nullptr, *tree_kbuf = nullptr;
     unsigned long long *codes = nullptr, *codes_alt = nullptr;
-    int32_t *perm = nullptr, *perm_alt = nullptr;
-    int32_t *lcp = nullptr, *node_start = nullptr;
+    int32_t *perm = nullptr, *perm_alt = nullptr;  // slot -> body index
+    int32_t *lcp = nullptr;
+    uint32_t *node_start = nullptr;     // [n+1] exclusive scan of nodes started per slot
+    int32_t *own_leaf = nullptr;
+    void *slot_pos = nullptr;           // float4 or double4 (x, y, z, G m) per slot
+    void *slot_acc = nullptr;           // float4 or double4 per slot
+    uint32_t *slot_cnt = nullptr;       // interactions per slot
+    uint32_t *scratch = nullptr;        // radix / scan scratch
+    size_t scratch_words = 0;
+    double *bbox_part = nullptr;        // per-block min/max partials
+    double *box_dev = nullptr;          // btm xyz, top xyz
+    int *status = nullptr;              // device error word
+    uint32_t *host_total = nullptr;     // pinned: node total, status
     int8_t *ndepth = nullptr, *nleaf = nullptr;
-    int32_t *nfirst = nullptr, *ncount = nullptr, *nskip = nullptr, *own_leaf = nullptr;
-    double4 *ncom = nullptr;      // com xyz + mass (FP64)
-    double *nwidth = nullptr;
-    float4 *nwalk = nullptr;      // walk record: com xyz (FP32) + G M
-    float *nwidth2 = nullptr;     // width^2 / theta^2 (FP32 criterion)
-    float4 *sorted_pos = nullptr; // bodies in slot order: x y z (FP32) + G m
-    uint32_t *scan_tmp = nullptr; // radix histograms / scan scratch
-    int32_t *depth_list = nullptr, *depth_off = nullptr;
-    int *status = nullptr;        // device error word (placement / indistinguishable)
-    int64_t *counters = nullptr;  // device scalars: node total, etc.
-    double *box_dev = nullptr;
+    int32_t *nfirst = nullptr, *ncount = nullptr, *nskip = nullptr;
+    double4 *ncom = nullptr;            // FP64 centre of mass xyz + mass
+    double *nwidth = nullptr;           // top.x - btm.x in T
+    void *nwalk_a = nullptr;            // walk record: com xyz + G M (float4 / double4)
+    int4 *nwalk_b = nullptr;            // walk record: skip, first, count | leaf<<31, width^2 bits
+    double *nwalk_w2 = nullptr;         // width^2 for the FP64 walk
+    int32_t *depth_list = nullptr;      // internal nodes grouped by depth
+    uint32_t *depth_off = nullptr;      // [22] offsets + [22] cursors
+    double box[6] = {0, 0, 0, 0, 0, 0};
+    uint32_t *bh_ninter = nullptr;      // interactions per body (body order)
+
+    // spatial reordering of the bodies for the mixed-precision direct sum
+    int reorder_interval = 16;
+    uint64_t steps_since_reorder = 0;
+    bool ordered = false;
+    double4 *sc4 = nullptr;
+    double *sc1 = nullptr;
+    int32_t *sci = nullptr;
 
     // collisions (collide.cu)
     void *coll_buf = nullptr;
@@ -84,6 +102,11 @@ struct gtd_system {
 
 void release_bodies(gtd_system *s);
 void release_tree(gtd_system *s);
+int reorder_bodies(gtd_system *s);
+// row[s] = host row of device slot s: ascending upload index among the live bodies
+int output_rows(gtd_system *s, std::vector<int64_t> &row);
+// device accelerations -> host triples in host row order (synchronises the stream)
+int copy_acc_out(gtd_system *s, double *a3);
 void release_collide(gtd_system *s);
 int ensure_plan(gtd_system *s);
 int force_and_integrate(gtd_system *s, const double4 *src, int epi, const gtd::StepArgs &st);

@@ -1,12 +1,896 @@
-// Barnes-Hut octree (placeholder until the linear-octree kernels land).
+// Barnes-Hut on the device: the greg8tree octree rebuilt as a linear octree, and the reference
+// walk, plus the Morton ordering the mixed-precision direct sum uses.
+//
+// Reference semantics (greg8tree.hpp) and how they map here:
+//  * root box: bh_tree::find_min_max (:1012-1047) - min/max, longest edge, pad = edge/20, a cube
+//    anchored at min - pad - computed in T (float or double) exactly as the reference rounds.
+//  * octant splits: set_corners (:81-131) splits at (btm + top)/2 with the sum rounded to T; a
+//    coordinate >= the split goes to the upper child (half-open cells, gregvec.hpp:2115-2120);
+//    octant index bit0 = x, bit1 = y, bit2 = z (:74-76).  The 63-bit Morton code of a body is that
+//    descent repeated 21 times, so the codes reproduce the reference's cell assignment bit for bit.
+//  * topology: the reference octree (one body per leaf, a cell for every shared prefix) is the set
+//    of octal prefixes shared by >= 2 bodies plus one leaf per body; emitted here in DFS pre-order
+//    (children in octant order = ascending code = the leaf order of bh_cube::iterator :502-614)
+//    with skip links.  Depth is capped at 21: bodies sharing a full code form one bucket leaf.
+//  * centres of mass: calc_com (:213-281) in FP64 moments (the float moments of the reference
+//    overflow in SI units), children summed in octant order, deepest level first.
+//  * walk: cell_iterator (:702-833) - DFS from the root's children, leaves always accepted
+//    except the body's own, cells accepted when width/|x - com| < theta, otherwise descended.
+//    A warp walks 32 consecutive (Morton-adjacent) bodies together: each lane keeps its own next
+//    node, the warp fetches the minimum of those (one broadcast load for all lanes at that node),
+//    so every lane visits exactly its reference sequence of cells.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "gtd_internal.cuh"
+#include "gtd_sort.cuh"
 #include "gtd_system.cuh"
-using namespace gtd;
-void release_tree(gtd_system *s) { cudaFree(s->tree_buf); s->tree_buf = nullptr; s->tree_bytes = 0; s->tree_valid = false; }
-int bh_evolve_kdk(gtd_system *, uint64_t) { return fail(GTD_ERR_UNSUPPORTED, "Barnes-Hut not built"); }
-int bh_accelerations(gtd_system *, double *, uint32_t *) { return fail(GTD_ERR_UNSUPPORTED, "Barnes-Hut not built"); }
-extern "C" {
-int gtd_bh_build(gtd_system *, int) { return fail(GTD_ERR_UNSUPPORTED, "Barnes-Hut not built"); }
-int gtd_bh_tree_size(gtd_system *, int64_t *, int64_t *, double *) { return fail(GTD_ERR_UNSUPPORTED, "Barnes-Hut not built"); }
-int gtd_bh_tree_download(gtd_system *, uint64_t *, int32_t *, int8_t *, int8_t *, int32_t *, int32_t *, int32_t *, double *, double *, double *) { return fail(GTD_ERR_UNSUPPORTED, "Barnes-Hut not built"); }
-int gtd_bh_accelerations(gtd_system *, double *, uint32_t *) { return fail(GTD_ERR_UNSUPPORTED, "Barnes-Hut not built"); }
+
+namespace gtd {
+
+constexpr int kMaxDepth = 21;
+constexpr int kBBoxBlocks = 296;
+constexpr int kTT = 256;
+
+template <bool F>
+struct TreeT;
+template <>
+struct TreeT<true> {
+    using T = float;
+    __device__ static float rnd(double v) { return __double2float_rn(v); }
+    __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+    __device__ static float sub(float a, float b) { return __fsub_rn(a, b); }
+    __device__ static float div(float a, float b) { return __fdiv_rn(a, b); }
+};
+template <>
+struct TreeT<false> {
+    using T = double;
+    __device__ static double rnd(double v) { return v; }
+    __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
+    __device__ static double sub(double a, double b) { return __dsub_rn(a, b); }
+    __device__ static double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+
+// ---- root box (find_min_max) ---------------------------------------------------------------
+template <bool F>
+__global__ void bbox_partial_kernel(const double4 *pm, int64_t n, double *part) {
+    using TT = TreeT<F>;
+    __shared__ double red[6][kTT];
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double4 p = pm[i];
+        const double c[3] = {(double)TT::rnd(p.x), (double)TT::rnd(p.y), (double)TT::rnd(p.z)};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fmin(mn[k], c[k]);
+            mx[k] = fmax(mx[k], c[k]);
+        }
+    }
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        red[k][t] = mn[k];
+        red[3 + k][t] = mx[k];
+    }
+    __syncthreads();
+    for (int w = kTT / 2; w > 0; w >>= 1) {
+        if (t < w) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                red[k][t] = fmin(red[k][t], red[k][t + w]);
+                red[3 + k][t] = fmax(red[3 + k][t], red[3 + k][t + w]);
+            }
+        }
+        __syncthreads();
+    }
+    if (t < 6) part[(size_t)blockIdx.x * 6 + t] = red[t][0];
 }
+
+// One thread: the reference's arithmetic for the cube, greg8tree.hpp:1037-1046, in T.
+template <bool F>
+__global__ void bbox_final_kernel(const double *part, int blocks, double *box, int *status) {
+    using TT = TreeT<F>;
+    using T = typename TT::T;
+    if (threadIdx.x != 0) return;
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int b = 0; b < blocks; ++b)
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fmin(mn[k], part[b * 6 + k]);
+            mx[k] = fmax(mx[k], part[b * 6 + 3 + k]);
+        }
+    const T xr = TT::sub((T)mx[0], (T)mn[0]), yr = TT::sub((T)mx[1], (T)mn[1]), zr = TT::sub((T)mx[2], (T)mn[2]);
+    T edge = xr > yr ? (xr > zr ? xr : zr) : (yr > zr ? yr : zr);
+    // pad = edge / 20.0l: the long-double quotient rounded to T equals the correctly rounded T
+    // quotient (a division by 20 never lands on a rounding tie at 64 -> 53 or 24 bits)
+    const T pad = TT::div(edge, (T)20);
+    T btm[3];
+    for (int k = 0; k < 3; ++k) btm[k] = TT::sub((T)mn[k], pad);
+    edge = TT::add(edge, (T)2 * pad);
+    for (int k = 0; k < 3; ++k) {
+        box[k] = (double)btm[k];
+        box[3 + k] = (double)TT::add(btm[k], edge);
+    }
+    if (!(edge > (T)0) || !isfinite((double)edge)) atomicExch(status, GTD_ERR_INVALID_BODY_PLACEMENT);
+}
+
+// ---- Morton codes: 21 levels of the reference's octant descent -------------------------------
+template <bool F>
+__device__ __forceinline__ bool morton_of(double x, double y, double z, const double *box, unsigned long long &code) {
+    using TT = TreeT<F>;
+    using T = typename TT::T;
+    const T p[3] = {TT::rnd(x), TT::rnd(y), TT::rnd(z)};
+    T lo[3], hi[3];
+    bool inside = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = (T)box[k];
+        hi[k] = (T)box[3 + k];
+        inside = inside && lo[k] <= p[k] && p[k] < hi[k];
+    }
+    unsigned long long c = 0;
+#pragma unroll 1
+    for (int l = 0; l < kMaxDepth; ++l) {
+        unsigned oct = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const T mid = TT::add(lo[k], hi[k]) * (T)0.5;
+            if (p[k] >= mid) {
+                oct |= 1u << k;
+                lo[k] = mid;
+            } else {
+                hi[k] = mid;
+            }
+        }
+        c = (c << 3) | oct;
+    }
+    code = c;
+    return inside;
+}
+
+template <bool F>
+__global__ void morton_kernel(const double4 *pm, int64_t n, const double *box_g, unsigned long long *keys,
+                              int32_t *vals, int *status) {
+    __shared__ double box[6];
+    if (threadIdx.x < 6) box[threadIdx.x] = box_g[threadIdx.x];
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 p = pm[i];
+    unsigned long long c;
+    if (!morton_of<F>(p.x, p.y, p.z, box, c)) atomicExch(status, GTD_ERR_INVALID_BODY_PLACEMENT);
+    keys[i] = c;
+    vals[i] = (int32_t)i;
+}
+
+// ---- topology ---------------------------------------------------------------------------------
+__device__ __forceinline__ int lcp_digits(unsigned long long a, unsigned long long b) {
+    const unsigned long long x = a ^ b;
+    if (!x) return kMaxDepth;
+    return (__clzll((long long)x) - 1) / 3;
+}
+
+// Per slot: common octal prefix with the next slot and the number of nodes the slot opens.
+template <bool F>
+__global__ void lcp_count_kernel(const unsigned long long *codes, const int32_t *perm, const double4 *pm, int64_t n,
+                                 int32_t *lcp, uint32_t *cnt, int *status) {
+    using TT = TreeT<F>;
+    const int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a > n) return;
+    if (a == n) {
+        cnt[n] = 0;
+        return;
+    }
+    int la = -1;
+    if (a + 1 < n) {
+        la = lcp_digits(codes[a], codes[a + 1]);
+        if (la == kMaxDepth) {
+            const double4 p = pm[perm[a]], q = pm[perm[a + 1]];
+            if (TT::rnd(p.x) == TT::rnd(q.x) && TT::rnd(p.y) == TT::rnd(q.y) && TT::rnd(p.z) == TT::rnd(q.z))
+                atomicExch(status, GTD_ERR_INDISTINGUISHABLE);
+        }
+        lcp[a] = la;
+    }
+    const int lm = a > 0 ? lcp_digits(codes[a - 1], codes[a]) : -1;
+    const int lim = la < kMaxDepth - 1 ? la : kMaxDepth - 1;
+    const int ni = lim - lm > 0 ? lim - lm : 0;
+    cnt[a] = (uint32_t)(ni + (lm < kMaxDepth ? 1 : 0));
+}
+
+// last slot sharing the first d octal digits with slot a (galloping then binary search)
+__device__ __forceinline__ int64_t range_end(const unsigned long long *code, int64_t n, int64_t a, int d) {
+    if (d == 0) return n - 1;
+    const int shift = 63 - 3 * d;
+    const unsigned long long pre = code[a] >> shift;
+    int64_t lo = a, step = 1;
+    while (true) {
+        const int64_t nx = lo + step;
+        if (nx >= n || (code[nx] >> shift) != pre) break;
+        lo = nx;
+        step <<= 1;
+    }
+    int64_t hi = min(lo + step, n) - 1;
+    while (lo < hi) {
+        const int64_t mid = lo + (hi - lo + 1) / 2;
+        if ((code[mid] >> shift) == pre) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct EmitArgs {
+    int64_t n;
+    const unsigned long long *codes;
+    const int32_t *perm, *lcp;
+    const uint32_t *node_start;
+    const double4 *pm;
+    const double *box;
+    int8_t *depth, *leaf;
+    int32_t *first, *count, *skip, *own;
+    double4 *com;
+    double *width;
+    uint32_t *depth_hist;  // [21] internal nodes per depth
+};
+
+template <bool F>
+__device__ double cell_width(unsigned long long code, int depth, const double *box) {
+    using TT = TreeT<F>;
+    using T = typename TT::T;
+    T lo = (T)box[0], hi = (T)box[3];
+    for (int l = 0; l < depth; ++l) {
+        const T mid = TT::add(lo, hi) * (T)0.5;
+        if ((code >> (3 * (kMaxDepth - 1 - l))) & 1ull) lo = mid;
+        else hi = mid;
+    }
+    return (double)TT::sub(hi, lo);
+}
+
+template <bool F>
+__global__ void emit_kernel(EmitArgs e) {
+    using TT = TreeT<F>;
+    const int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= e.n) return;
+    const int lm = a > 0 ? e.lcp[a - 1] : -1;
+    const int la = a + 1 < e.n ? e.lcp[a] : -1;
+    const int lim = la < kMaxDepth - 1 ? la : kMaxDepth - 1;
+    int64_t node = e.node_start[a];
+    const unsigned long long ca = e.codes[a];
+    for (int d = lm + 1; d <= lim; ++d, ++node) {
+        const int64_t last = range_end(e.codes, e.n, a, d);
+        e.depth[node] = (int8_t)d;
+        e.leaf[node] = 0;
+        e.first[node] = (int32_t)a;
+        e.count[node] = (int32_t)(last - a + 1);
+        e.skip[node] = (int32_t)e.node_start[last + 1];
+        e.width[node] = cell_width<F>(ca, d, e.box);
+        atomicAdd(&e.depth_hist[d], 1u);
+    }
+    if (lm < kMaxDepth) {
+        const int64_t last = la == kMaxDepth ? range_end(e.codes, e.n, a, kMaxDepth) : a;
+        const int lb = last + 1 < e.n ? e.lcp[last] : -1;
+        const int dl = last > a ? kMaxDepth : (lm > lb ? lm : lb) + 1;
+        e.depth[node] = (int8_t)dl;
+        e.leaf[node] = 1;
+        e.first[node] = (int32_t)a;
+        e.count[node] = (int32_t)(last - a + 1);
+        e.skip[node] = (int32_t)e.node_start[last + 1];
+        e.width[node] = cell_width<F>(ca, dl, e.box);
+        if (last == a) {
+            const double4 p = e.pm[e.perm[a]];
+            e.com[node] = make_double4((double)TT::rnd(p.x), (double)TT::rnd(p.y), (double)TT::rnd(p.z),
+                                       (double)TT::rnd(p.w));
+        } else {
+            double ms = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+            for (int64_t q = a; q <= last; ++q) {
+                const double4 p = e.pm[e.perm[q]];
+                const double mb = (double)TT::rnd(p.w);
+                ms = __dadd_rn(ms, mb);
+                mx = __dadd_rn(mx, __dmul_rn(mb, (double)TT::rnd(p.x)));
+                my = __dadd_rn(my, __dmul_rn(mb, (double)TT::rnd(p.y)));
+                mz = __dadd_rn(mz, __dmul_rn(mb, (double)TT::rnd(p.z)));
+            }
+            e.com[node] = make_double4(__ddiv_rn(mx, ms), __ddiv_rn(my, ms), __ddiv_rn(mz, ms), ms);
+        }
+        for (int64_t q = a; q <= last; ++q) e.own[q] = (int32_t)node;
+    }
+}
+
+__global__ void depth_offsets_kernel(uint32_t *depth_off) {
+    // depth_off[0..20]: counts in, exclusive offsets out; depth_off[22..42]: cursors
+    if (threadIdx.x != 0) return;
+    uint32_t run = 0;
+    for (int d = 0; d < kMaxDepth; ++d) {
+        const uint32_t c = depth_off[d];
+        depth_off[d] = run;
+        depth_off[22 + d] = run;
+        run += c;
+    }
+    depth_off[kMaxDepth] = run;
+}
+
+__global__ void depth_scatter_kernel(const int8_t *depth, const int8_t *leaf, int64_t n_nodes, uint32_t *depth_off,
+                                     int32_t *list) {
+    const int64_t nd = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (nd >= n_nodes || leaf[nd]) return;
+    const uint32_t pos = atomicAdd(&depth_off[22 + depth[nd]], 1u);
+    list[pos] = (int32_t)nd;
+}
+
+// Internal nodes of one depth: FP64 moments of the children in octant order.
+__global__ void com_level_kernel(const int32_t *list, const uint32_t *depth_off, int d, const int32_t *skip,
+                                 double4 *com) {
+    const uint32_t b = depth_off[d], e = depth_off[d + 1];
+    for (uint32_t k = b + blockIdx.x * blockDim.x + threadIdx.x; k < e; k += gridDim.x * blockDim.x) {
+        const int32_t nd = list[k];
+        const int32_t end = skip[nd];
+        double ms = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+        for (int32_t c = nd + 1; c < end; c = skip[c]) {
+            const double4 q = com[c];
+            ms = __dadd_rn(ms, q.w);
+            mx = __dadd_rn(mx, __dmul_rn(q.w, q.x));
+            my = __dadd_rn(my, __dmul_rn(q.w, q.y));
+            mz = __dadd_rn(mz, __dmul_rn(q.w, q.z));
+        }
+        com[nd] = make_double4(__ddiv_rn(mx, ms), __ddiv_rn(my, ms), __ddiv_rn(mz, ms), ms);
+    }
+}
+
+// Walk records (one 16-byte A + one 16-byte B load per visited node) and slot-ordered bodies.
+template <bool F>
+__global__ void walk_records_kernel(int64_t n_nodes, const double4 *com, const double *width, const int8_t *leaf,
+                                    const int32_t *first, const int32_t *count, const int32_t *skip, double G,
+                                    void *rec_a, int4 *rec_b, double *w2_64) {
+    const int64_t nd = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (nd >= n_nodes) return;
+    const double4 c = com[nd];
+    const double w = width[nd];
+    int4 b;
+    b.x = skip[nd];
+    b.y = first[nd];
+    b.z = count[nd] | (leaf[nd] ? (int)0x80000000u : 0);
+    if (F) {
+        reinterpret_cast<float4 *>(rec_a)[nd] =
+            make_float4(__double2float_rn(c.x), __double2float_rn(c.y), __double2float_rn(c.z), (float)(G * c.w));
+        const float wf = (float)w;
+        b.w = __float_as_int(__fmul_rn(wf, wf));
+    } else {
+        reinterpret_cast<double4 *>(rec_a)[nd] = make_double4(c.x, c.y, c.z, G * c.w);
+        b.w = 0;
+        w2_64[nd] = w * w;
+    }
+    rec_b[nd] = b;
+}
+
+template <bool F>
+__global__ void slot_bodies_kernel(const double4 *pm, const int32_t *perm, int64_t n, double G, void *slot_pos) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double4 p = pm[perm[s]];
+    if (F) {
+        reinterpret_cast<float4 *>(slot_pos)[s] = make_float4(__double2float_rn(p.x), __double2float_rn(p.y),
+                                                              __double2float_rn(p.z), (float)(G * (double)(float)p.w));
+    } else {
+        reinterpret_cast<double4 *>(slot_pos)[s] = make_double4(p.x, p.y, p.z, G * p.w);
+    }
+}
+
+// ---- warp-cooperative walk ---------------------------------------------------------------------
+template <typename T>
+struct V4;
+template <>
+struct V4<float> {
+    using type = float4;
+};
+template <>
+struct V4<double> {
+    using type = double4;
+};
+
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mul_t(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_t(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float sub_t(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_t(double a, double b) { return __dsub_rn(a, b); }
+
+template <typename T>
+__global__ void __launch_bounds__(kTT) walk_kernel(int64_t n, int64_t n_nodes, const void *rec_a_v, const int4 *rec_b,
+                                                   const double *w2_64, const void *slot_pos_v, const int32_t *own,
+                                                   T th2, T eps2, void *slot_acc_v, uint32_t *slot_cnt) {
+    using V = typename V4<T>::type;
+    const V *rec_a = reinterpret_cast<const V *>(rec_a_v);
+    const V *bodies = reinterpret_cast<const V *>(slot_pos_v);
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = s < n;
+    V p;
+    p.x = p.y = p.z = p.w = (T)0;
+    int32_t ol = -1;
+    uint32_t next = 0x7fffffffu;
+    if (active) {
+        p = bodies[s];
+        ol = own[s];
+        next = n_nodes > 1 ? 1u : (uint32_t)n_nodes;
+    }
+    T ax = 0, ay = 0, az = 0;
+    uint32_t cnt = 0;
+    const uint32_t nn = (uint32_t)n_nodes;
+    while (true) {
+        const uint32_t node = __reduce_min_sync(0xffffffffu, next);
+        if (node >= nn) break;
+        if (next != node) continue;
+        const V A = rec_a[node];
+        const int4 B = rec_b[node];
+        const bool leaf = B.z < 0;
+        const int count = B.z & 0x7fffffff;
+        if (leaf) {
+            if (count == 1) {
+                if ((int32_t)node != ol) {
+                    const T dx = A.x - p.x, dy = A.y - p.y, dz = A.z - p.z;
+                    const T r2 = dx * dx + dy * dy + dz * dz + eps2;
+                    const T inv = rsqrt_t(r2);
+                    const T sc = A.w * inv * inv * inv;
+                    ax += sc * dx;
+                    ay += sc * dy;
+                    az += sc * dz;
+                    ++cnt;
+                }
+            } else {
+                for (int q = B.y; q < B.y + count; ++q) {
+                    if (q == (int)s) continue;
+                    const V Q = bodies[q];
+                    const T dx = Q.x - p.x, dy = Q.y - p.y, dz = Q.z - p.z;
+                    const T r2 = dx * dx + dy * dy + dz * dz + eps2;
+                    const T inv = rsqrt_t(r2);
+                    const T sc = Q.w * inv * inv * inv;
+                    ax += sc * dx;
+                    ay += sc * dy;
+                    az += sc * dz;
+                    ++cnt;
+                }
+            }
+            next = (uint32_t)B.x;
+        } else {
+            const T dx = sub_t(A.x, p.x), dy = sub_t(A.y, p.y), dz = sub_t(A.z, p.z);
+            const T r2 = fma_t(dz, dz, fma_t(dy, dy, mul_t(dx, dx)));
+            const T w2 = sizeof(T) == 4 ? (T)__int_as_float(B.w) : (T)w2_64[node];
+            if (w2 < mul_t(th2, r2)) {
+                const T r2e = r2 + eps2;
+                const T inv = rsqrt_t(r2e);
+                const T sc = A.w * inv * inv * inv;
+                ax += sc * dx;
+                ay += sc * dy;
+                az += sc * dz;
+                ++cnt;
+                next = (uint32_t)B.x;
+            } else {
+                next = node + 1;
+            }
+        }
+    }
+    if (active) {
+        V o;
+        o.x = ax; o.y = ay; o.z = az; o.w = (T)0;
+        reinterpret_cast<V *>(slot_acc_v)[s] = o;
+        slot_cnt[s] = cnt;
+    }
+}
+
+// slot order -> body order, optionally kicking the velocities with the new acceleration
+template <typename T>
+__global__ void scatter_acc_kernel(int64_t n, const int32_t *perm, const void *slot_acc_v, const uint32_t *slot_cnt,
+                                   double4 *acc, uint32_t *ninter, double4 *vel, double kick) {
+    using V = typename V4<T>::type;
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const V a = reinterpret_cast<const V *>(slot_acc_v)[s];
+    const int32_t b = perm[s];
+    const double4 ad = make_double4((double)a.x, (double)a.y, (double)a.z, 0.0);
+    acc[b] = ad;
+    if (ninter) ninter[b] = slot_cnt[s];
+    if (vel) {
+        double4 v = vel[b];
+        v.x = fma(kick, ad.x, v.x);
+        v.y = fma(kick, ad.y, v.y);
+        v.z = fma(kick, ad.z, v.z);
+        vel[b] = v;
+    }
+}
+
+__global__ void drift_kernel(int64_t n, double4 *pm, const double4 *vel, double h) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = pm[i];
+    const double4 v = vel[i];
+    p.x = fma(h, v.x, p.x);
+    p.y = fma(h, v.y, p.y);
+    p.z = fma(h, v.z, p.z);
+    pm[i] = p;
+}
+
+// gather for the spatial reorder
+template <typename V>
+__global__ void gather_kernel(int64_t n, const int32_t *perm, const V *in, V *out) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) out[s] = in[perm[s]];
+}
+
+}  // namespace gtd
+
+using namespace gtd;
+
+static unsigned blocks_for(int64_t n, int t = kTT) { return (unsigned)((n + t - 1) / t); }
+
+void release_tree(gtd_system *s) {
+    cudaFree(s->tree_nbuf);
+    cudaFree(s->tree_kbuf);
+    cudaFreeHost(s->host_total);
+    cudaFree(s->sc4);
+    cudaFree(s->sc1);
+    cudaFree(s->sci);
+    cudaFree(s->bh_ninter);
+    s->tree_nbuf = s->tree_kbuf = nullptr;
+    s->host_total = nullptr;
+    s->sc4 = nullptr;
+    s->sc1 = nullptr;
+    s->sci = nullptr;
+    s->bh_ninter = nullptr;
+    s->tree_n = s->node_cap = 0;
+    s->tree_valid = false;
+}
+
+template <typename P>
+static P *carve(char *&cur, size_t count) {
+    const size_t bytes = ((sizeof(P) * count) + 255) & ~(size_t)255;
+    P *p = reinterpret_cast<P *>(cur);
+    cur += bytes;
+    return p;
+}
+
+static size_t carve_size(size_t bytes) { return (bytes + 255) & ~(size_t)255; }
+
+static int ensure_tree_n(gtd_system *s, int64_t n) {
+    if (n <= s->tree_n && s->tree_nbuf) return GTD_OK;
+    cudaFree(s->tree_nbuf);
+    s->tree_nbuf = nullptr;
+    const size_t nn = (size_t)n + 1;
+    s->scratch_words = radix_scratch_words(n) + scan_scratch_words((int64_t)nn) + 64;
+    size_t total = 0;
+    total += 2 * carve_size(8 * nn);            // codes, codes_alt
+    total += 2 * carve_size(4 * nn);            // perm, perm_alt
+    total += carve_size(4 * nn);                // lcp
+    total += carve_size(4 * nn);                // node_start
+    total += carve_size(4 * nn);                // own_leaf
+    total += 2 * carve_size(32 * nn);           // slot_pos, slot_acc (double4 worst case)
+    total += carve_size(4 * nn);                // slot_cnt
+    total += carve_size(4 * s->scratch_words);  // scratch
+    total += carve_size(8 * 6 * kBBoxBlocks);   // bbox partials
+    total += carve_size(8 * 6) + carve_size(64) + carve_size(4 * 64);
+    GTD_CUDA(cudaMalloc(&s->tree_nbuf, total));
+    char *c = reinterpret_cast<char *>(s->tree_nbuf);
+    s->codes = carve<unsigned long long>(c, nn);
+    s->codes_alt = carve<unsigned long long>(c, nn);
+    s->perm = carve<int32_t>(c, nn);
+    s->perm_alt = carve<int32_t>(c, nn);
+    s->lcp = carve<int32_t>(c, nn);
+    s->node_start = carve<uint32_t>(c, nn);
+    s->own_leaf = carve<int32_t>(c, nn);
+    s->slot_pos = carve<double4>(c, nn);
+    s->slot_acc = carve<double4>(c, nn);
+    s->slot_cnt = carve<uint32_t>(c, nn);
+    s->scratch = carve<uint32_t>(c, s->scratch_words);
+    s->bbox_part = carve<double>(c, 6 * kBBoxBlocks);
+    s->box_dev = carve<double>(c, 6);
+    s->status = carve<int>(c, 16);
+    s->depth_off = carve<uint32_t>(c, 64);
+    if (!s->host_total) GTD_CUDA(cudaMallocHost(&s->host_total, 16 * sizeof(uint32_t)));
+    s->tree_n = n;
+    return GTD_OK;
+}
+
+static int ensure_tree_nodes(gtd_system *s, int64_t nodes) {
+    if (nodes <= s->node_cap && s->tree_kbuf) return GTD_OK;
+    cudaFree(s->tree_kbuf);
+    s->tree_kbuf = nullptr;
+    const size_t k = (size_t)(nodes + nodes / 4 + 1024);
+    size_t total = 2 * carve_size(k) + 3 * carve_size(4 * k) + carve_size(32 * k) + carve_size(8 * k) +
+                   carve_size(32 * k) + carve_size(16 * k) + carve_size(8 * k) + carve_size(4 * k);
+    GTD_CUDA(cudaMalloc(&s->tree_kbuf, total));
+    char *c = reinterpret_cast<char *>(s->tree_kbuf);
+    s->ndepth = carve<int8_t>(c, k);
+    s->nleaf = carve<int8_t>(c, k);
+    s->nfirst = carve<int32_t>(c, k);
+    s->ncount = carve<int32_t>(c, k);
+    s->nskip = carve<int32_t>(c, k);
+    s->ncom = carve<double4>(c, k);
+    s->nwidth = carve<double>(c, k);
+    s->nwalk_a = carve<double4>(c, k);
+    s->nwalk_b = carve<int4>(c, k);
+    s->nwalk_w2 = carve<double>(c, k);
+    s->depth_list = carve<int32_t>(c, k);
+    s->node_cap = (int64_t)k;
+    return GTD_OK;
+}
+
+// Morton codes of the current positions, sorted (codes, perm).  Leaves the box in s->box_dev.
+static int morton_sort(gtd_system *s, bool tree_float) {
+    const int64_t n = s->n;
+    int rc = ensure_tree_n(s, n);
+    if (rc) return rc;
+    const double4 *pm = s->pm[s->cur];
+    cudaStream_t st = s->stream;
+    GTD_CUDA(cudaMemsetAsync(s->status, 0, sizeof(int), st));
+    const int bb = (int)std::min<int64_t>(kBBoxBlocks, std::max<int64_t>(1, (n + kTT - 1) / kTT));
+    if (tree_float) {
+        bbox_partial_kernel<true><<<bb, kTT, 0, st>>>(pm, n, s->bbox_part);
+        bbox_final_kernel<true><<<1, 32, 0, st>>>(s->bbox_part, bb, s->box_dev, s->status);
+        morton_kernel<true><<<blocks_for(n), kTT, 0, st>>>(pm, n, s->box_dev, s->codes, s->perm, s->status);
+    } else {
+        bbox_partial_kernel<false><<<bb, kTT, 0, st>>>(pm, n, s->bbox_part);
+        bbox_final_kernel<false><<<1, 32, 0, st>>>(s->bbox_part, bb, s->box_dev, s->status);
+        morton_kernel<false><<<blocks_for(n), kTT, 0, st>>>(pm, n, s->box_dev, s->codes, s->perm, s->status);
+    }
+    GTD_CHECK_LAUNCH();
+    s->launches += 3;
+    return radix_sort_u64(s->codes, s->perm, s->codes_alt, s->perm_alt, n, 63, s->scratch, st, &s->launches);
+}
+
+static int read_status(gtd_system *s) {
+    GTD_CUDA(cudaMemcpyAsync(s->host_total + 1, s->status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    const int st = (int)s->host_total[1];
+    if (st == GTD_ERR_INVALID_BODY_PLACEMENT)
+        return fail(st, "Error: a body does not lie within the Barnes-Hut root cube (non-finite position?).");
+    if (st == GTD_ERR_INDISTINGUISHABLE)
+        return fail(st, "Error: two bodies have positions that are either equal or so close together that they "
+                        "cannot be told apart.");
+    if (st) return fail(st, "device status %d", st);
+    return GTD_OK;
+}
+
+static int bh_build_impl(gtd_system *s, int tree_float) {
+    const int64_t n = s->n;
+    s->tree_valid = false;
+    if (n < 2) {
+        // the reference's root cube of a single body has zero size and rejects its own body
+        return fail(GTD_ERR_INVALID_BODY_PLACEMENT, "Error: body with ID = 0 is not contained within the current "
+                                                    "Barnes-Hut cube.");
+    }
+    s->tree_float = tree_float ? 1 : 0;
+    int rc = morton_sort(s, tree_float != 0);
+    if (rc) return rc;
+    cudaStream_t st = s->stream;
+    const double4 *pm = s->pm[s->cur];
+    if (tree_float)
+        lcp_count_kernel<true><<<blocks_for(n + 1), kTT, 0, st>>>(s->codes, s->perm, pm, n, s->lcp, s->node_start,
+                                                                  s->status);
+    else
+        lcp_count_kernel<false><<<blocks_for(n + 1), kTT, 0, st>>>(s->codes, s->perm, pm, n, s->lcp, s->node_start,
+                                                                   s->status);
+    GTD_CHECK_LAUNCH();
+    s->launches += 1;
+    rc = exclusive_scan_u32(s->node_start, s->node_start, n + 1, s->scratch, st, &s->launches);
+    if (rc) return rc;
+    GTD_CUDA(cudaMemcpyAsync(s->host_total, s->node_start + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GTD_CUDA(cudaMemcpyAsync(s->host_total + 1, s->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GTD_CUDA(cudaStreamSynchronize(st));
+    rc = read_status(s);
+    if (rc) return rc;
+    const int64_t nodes = s->host_total[0];
+    rc = ensure_tree_nodes(s, nodes);
+    if (rc) return rc;
+    GTD_CUDA(cudaMemsetAsync(s->depth_off, 0, 64 * sizeof(uint32_t), st));
+    EmitArgs e{n, s->codes, s->perm, s->lcp, s->node_start, pm, s->box_dev, s->ndepth, s->nleaf, s->nfirst,
+               s->ncount, s->nskip, s->own_leaf, s->ncom, s->nwidth, s->depth_off};
+    if (tree_float) emit_kernel<true><<<blocks_for(n), kTT, 0, st>>>(e);
+    else emit_kernel<false><<<blocks_for(n), kTT, 0, st>>>(e);
+    GTD_CHECK_LAUNCH();
+    depth_offsets_kernel<<<1, 32, 0, st>>>(s->depth_off);
+    depth_scatter_kernel<<<blocks_for(nodes), kTT, 0, st>>>(s->ndepth, s->nleaf, nodes, s->depth_off, s->depth_list);
+    GTD_CHECK_LAUNCH();
+    s->launches += 3;
+    for (int d = kMaxDepth - 1; d >= 0; --d) {
+        com_level_kernel<<<4 * 148, kTT, 0, st>>>(s->depth_list, s->depth_off, d, s->nskip, s->ncom);
+        s->launches += 1;
+    }
+    GTD_CHECK_LAUNCH();
+    if (tree_float)
+        walk_records_kernel<true><<<blocks_for(nodes), kTT, 0, st>>>(nodes, s->ncom, s->nwidth, s->nleaf, s->nfirst,
+                                                                      s->ncount, s->nskip, s->G, s->nwalk_a,
+                                                                      s->nwalk_b, s->nwalk_w2);
+    else
+        walk_records_kernel<false><<<blocks_for(nodes), kTT, 0, st>>>(nodes, s->ncom, s->nwidth, s->nleaf, s->nfirst,
+                                                                       s->ncount, s->nskip, s->G, s->nwalk_a,
+                                                                       s->nwalk_b, s->nwalk_w2);
+    GTD_CHECK_LAUNCH();
+    if (tree_float) slot_bodies_kernel<true><<<blocks_for(n), kTT, 0, st>>>(pm, s->perm, n, s->G, s->slot_pos);
+    else slot_bodies_kernel<false><<<blocks_for(n), kTT, 0, st>>>(pm, s->perm, n, s->G, s->slot_pos);
+    GTD_CHECK_LAUNCH();
+    s->launches += 2;
+    s->n_nodes = nodes;
+    s->tree_valid = true;
+    return GTD_OK;
+}
+
+// Walk for every body; accelerations in body order, optionally kicking v by kick * a.
+static int bh_walk_impl(gtd_system *s, double kick, bool do_kick) {
+    if (!s->tree_valid) return fail(GTD_ERR_INVALID_ARGUMENT, "no Barnes-Hut tree: call gtd_bh_build first");
+    const int64_t n = s->n;
+    cudaStream_t st = s->stream;
+    if (!s->bh_ninter) GTD_CUDA(cudaMalloc(&s->bh_ninter, sizeof(uint32_t) * (size_t)s->cap));
+    if (s->tree_float) {
+        const float th2 = (float)(s->theta * s->theta), e2 = (float)(s->eps * s->eps);
+        walk_kernel<float><<<blocks_for(n), kTT, 0, st>>>(n, s->n_nodes, s->nwalk_a, s->nwalk_b, s->nwalk_w2,
+                                                          s->slot_pos, s->own_leaf, th2, e2, s->slot_acc, s->slot_cnt);
+        GTD_CHECK_LAUNCH();
+        scatter_acc_kernel<float><<<blocks_for(n), kTT, 0, st>>>(n, s->perm, s->slot_acc, s->slot_cnt, s->acc,
+                                                                 s->bh_ninter, do_kick ? s->vel : nullptr, kick);
+    } else {
+        const double th2 = s->theta * s->theta, e2 = s->eps * s->eps;
+        walk_kernel<double><<<blocks_for(n), kTT, 0, st>>>(n, s->n_nodes, s->nwalk_a, s->nwalk_b, s->nwalk_w2,
+                                                           s->slot_pos, s->own_leaf, th2, e2, s->slot_acc,
+                                                           s->slot_cnt);
+        GTD_CHECK_LAUNCH();
+        scatter_acc_kernel<double><<<blocks_for(n), kTT, 0, st>>>(n, s->perm, s->slot_acc, s->slot_cnt, s->acc,
+                                                                  s->bh_ninter, do_kick ? s->vel : nullptr, kick);
+    }
+    GTD_CHECK_LAUNCH();
+    s->launches += 2;
+    return GTD_OK;
+}
+
+// Leapfrog KDK with Barnes-Hut forces in the reference's schedule (gregsys.hpp:2893-2945):
+// initial walk and half kick, then per step a full drift, a rebuild, a walk and a full kick
+// (the velocities end half a step ahead of the positions, as in the reference).
+int bh_evolve_kdk(gtd_system *s, uint64_t steps) {
+    if (s->n == 0) return GTD_OK;
+    const int tf = s->tree_float;
+    int rc = bh_build_impl(s, tf);
+    if (rc) return rc;
+    rc = bh_walk_impl(s, 0.5 * s->dt, true);
+    if (rc) return rc;
+    for (uint64_t k = 0; k < steps; ++k) {
+        drift_kernel<<<blocks_for(s->n), kTT, 0, s->stream>>>(s->n, s->pm[s->cur], s->vel, s->dt);
+        GTD_CHECK_LAUNCH();
+        s->launches += 1;
+        rc = bh_build_impl(s, tf);
+        if (rc) return rc;
+        rc = bh_walk_impl(s, s->dt, true);
+        if (rc) return rc;
+    }
+    return GTD_OK;
+}
+
+static int copy_bh_out(gtd_system *s, double *a3, uint32_t *n_inter) {
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    if (a3) {
+        int rc = copy_acc_out(s, a3);
+        if (rc) return rc;
+    }
+    if (n_inter) {
+        const int64_t n = s->n;
+        std::vector<uint32_t> h((size_t)n);
+        GTD_CUDA(cudaMemcpy(h.data(), s->bh_ninter, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost));
+        std::vector<int64_t> row;
+        int rc = output_rows(s, row);
+        if (rc) return rc;
+        for (int64_t i = 0; i < n; ++i) n_inter[row[(size_t)i]] = h[(size_t)i];
+    }
+    return GTD_OK;
+}
+
+int bh_accelerations(gtd_system *s, double *a3, uint32_t *n_inter) {
+    int rc = bh_build_impl(s, s->tree_float);
+    if (rc) return rc;
+    rc = bh_walk_impl(s, 0.0, false);
+    if (rc) return rc;
+    return copy_bh_out(s, a3, n_inter);
+}
+
+// Spatial (Morton) reordering of every per-body array, so that the direct-sum rows are compact
+// and the mixed kernel's per-row FP32 frame stays close to its bodies.
+int reorder_bodies(gtd_system *s) {
+    const int64_t n = s->n;
+    if (n < 2) return GTD_OK;
+    int rc = morton_sort(s, true);
+    if (rc) return rc;
+    cudaStream_t st = s->stream;
+    if (!s->sc4) {
+        GTD_CUDA(cudaMalloc(&s->sc4, sizeof(double4) * (size_t)s->cap));
+        GTD_CUDA(cudaMalloc(&s->sc1, sizeof(double) * (size_t)s->cap));
+        GTD_CUDA(cudaMalloc(&s->sci, sizeof(int32_t) * (size_t)s->cap));
+    }
+    const unsigned g = blocks_for(n);
+    gather_kernel<double4><<<g, kTT, 0, st>>>(n, s->perm, s->pm[s->cur], s->pm[s->cur ^ 1]);
+    s->cur ^= 1;
+    gather_kernel<double4><<<g, kTT, 0, st>>>(n, s->perm, s->vel, s->sc4);
+    std::swap(s->vel, s->sc4);
+    gather_kernel<double4><<<g, kTT, 0, st>>>(n, s->perm, s->acc, s->sc4);
+    std::swap(s->acc, s->sc4);
+    gather_kernel<double><<<g, kTT, 0, st>>>(n, s->perm, s->rad, s->sc1);
+    std::swap(s->rad, s->sc1);
+    gather_kernel<double><<<g, kTT, 0, st>>>(n, s->perm, s->rest, s->sc1);
+    std::swap(s->rest, s->sc1);
+    gather_kernel<int32_t><<<g, kTT, 0, st>>>(n, s->perm, s->ids, s->sci);
+    std::swap(s->ids, s->sci);
+    GTD_CHECK_LAUNCH();
+    s->launches += 6;
+    s->ordered = true;
+    s->tree_valid = false;
+    return GTD_OK;
+}
+
+extern "C" {
+
+int gtd_bh_build(gtd_system *s, int tree_float) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    int rc = bh_build_impl(s, tree_float);
+    if (rc) return rc;
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    return GTD_OK;
+}
+
+int gtd_bh_set_tree_float(gtd_system *s, int tree_float) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    s->tree_float = tree_float ? 1 : 0;
+    s->tree_valid = false;
+    return GTD_OK;
+}
+
+int gtd_bh_tree_size(gtd_system *s, int64_t *n_nodes, int64_t *n_leaves, double *box6) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (!s->tree_valid) return fail(GTD_ERR_INVALID_ARGUMENT, "no Barnes-Hut tree: call gtd_bh_build first");
+    if (n_nodes) *n_nodes = s->n_nodes;
+    if (n_leaves) {
+        std::vector<int8_t> lf((size_t)s->n_nodes);
+        GTD_CUDA(cudaMemcpy(lf.data(), s->nleaf, (size_t)s->n_nodes, cudaMemcpyDeviceToHost));
+        int64_t c = 0;
+        for (int8_t v : lf) c += v ? 1 : 0;
+        *n_leaves = c;
+    }
+    if (box6) GTD_CUDA(cudaMemcpy(box6, s->box_dev, 6 * sizeof(double), cudaMemcpyDeviceToHost));
+    return GTD_OK;
+}
+
+int gtd_bh_tree_download(gtd_system *s, uint64_t *codes, int32_t *perm, int8_t *depth, int8_t *is_leaf,
+                         int32_t *first, int32_t *count, int32_t *skip, double *mass, double *com3, double *width) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (!s->tree_valid) return fail(GTD_ERR_INVALID_ARGUMENT, "no Barnes-Hut tree: call gtd_bh_build first");
+    const size_t n = (size_t)s->n, k = (size_t)s->n_nodes;
+    if (codes) GTD_CUDA(cudaMemcpy(codes, s->codes, 8 * n, cudaMemcpyDeviceToHost));
+    if (perm) {
+        // slot -> upload index of the body
+        std::vector<int32_t> p(n), ids(n);
+        GTD_CUDA(cudaMemcpy(p.data(), s->perm, 4 * n, cudaMemcpyDeviceToHost));
+        GTD_CUDA(cudaMemcpy(ids.data(), s->ids, 4 * n, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; ++i) perm[i] = ids[(size_t)p[i]];
+    }
+    if (depth) GTD_CUDA(cudaMemcpy(depth, s->ndepth, k, cudaMemcpyDeviceToHost));
+    if (is_leaf) GTD_CUDA(cudaMemcpy(is_leaf, s->nleaf, k, cudaMemcpyDeviceToHost));
+    if (first) GTD_CUDA(cudaMemcpy(first, s->nfirst, 4 * k, cudaMemcpyDeviceToHost));
+    if (count) GTD_CUDA(cudaMemcpy(count, s->ncount, 4 * k, cudaMemcpyDeviceToHost));
+    if (skip) GTD_CUDA(cudaMemcpy(skip, s->nskip, 4 * k, cudaMemcpyDeviceToHost));
+    if (width) GTD_CUDA(cudaMemcpy(width, s->nwidth, 8 * k, cudaMemcpyDeviceToHost));
+    if (mass || com3) {
+        std::vector<double4> c(k);
+        GTD_CUDA(cudaMemcpy(c.data(), s->ncom, sizeof(double4) * k, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < k; ++i) {
+            if (mass) mass[i] = c[i].w;
+            if (com3) { com3[3 * i] = c[i].x; com3[3 * i + 1] = c[i].y; com3[3 * i + 2] = c[i].z; }
+        }
+    }
+    return GTD_OK;
+}
+
+int gtd_bh_accelerations(gtd_system *s, double *a3, uint32_t *n_inter) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (!s->tree_valid) return fail(GTD_ERR_INVALID_ARGUMENT, "no Barnes-Hut tree: call gtd_bh_build first");
+    int rc = bh_walk_impl(s, 0.0, false);
+    if (rc) return rc;
+    return copy_bh_out(s, a3, n_inter);
+}
+
+}  // extern "C"

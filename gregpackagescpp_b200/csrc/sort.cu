@@ -1,0 +1,194 @@
+// Device scan and a stable LSD radix sort of 64-bit keys with 32-bit values (8-bit digits).
+// Used for the Morton order of the octree build (greg8tree.hpp leaf order = ascending code) and
+// for the spatial reordering of the direct-sum bodies.
+#include <cuda_runtime.h>
+
+#include "gtd_internal.cuh"
+#include "gtd_sort.cuh"
+
+namespace gtd {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;                      // keys per thread per block chunk
+constexpr int kChunk = kSortThreads * kSortItems;   // keys per block
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// ---- exclusive scan of uint32 (arbitrary length, three phases) ---------------------------------
+__global__ void scan_tiles_kernel(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *tile_sums) {
+    __shared__ uint32_t warp_tot[kScanThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems], run = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + k;
+        v[k] = i < n ? in[i] : 0u;
+        const uint32_t t = v[k];
+        v[k] = run;
+        run += t;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kScanThreads / 32 ? warp_tot[lane] : 0u;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < kScanThreads / 32) warp_tot[lane] = wi - w;
+        if (lane == kScanThreads / 32 - 1 && tile_sums) tile_sums[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    const uint32_t off = warp_tot[warp] + incl - run;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + k;
+        if (i < n) out[i] = v[k] + off;
+    }
+}
+
+__global__ void scan_add_kernel(uint32_t *out, int64_t n, const uint32_t *tile_offsets) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += tile_offsets[i / kScanTile];
+}
+
+size_t scan_scratch_words(int64_t n) {
+    size_t words = 0;
+    int64_t m = n;
+    while (m > kScanTile) {
+        m = (m + kScanTile - 1) / kScanTile;
+        words += (size_t)m;
+    }
+    return words + 1;
+}
+
+// Exclusive scan in -> out (may alias).  scratch: scan_scratch_words(n) words.
+int exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *scratch, cudaStream_t s,
+                       uint64_t *launches) {
+    if (n <= 0) return GTD_OK;
+    const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles == 1) {
+        scan_tiles_kernel<<<1, kScanThreads, 0, s>>>(in, out, n, nullptr);
+        GTD_CHECK_LAUNCH();
+        if (launches) *launches += 1;
+        return GTD_OK;
+    }
+    uint32_t *sums = scratch;
+    scan_tiles_kernel<<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, n, sums);
+    GTD_CHECK_LAUNCH();
+    int rc = exclusive_scan_u32(sums, sums, tiles, scratch + tiles, s, launches);
+    if (rc) return rc;
+    scan_add_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, sums);
+    GTD_CHECK_LAUNCH();
+    if (launches) *launches += 2;
+    return GTD_OK;
+}
+
+// ---- radix sort ----------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const unsigned long long *keys, int64_t n,
+                                                                  int shift, uint32_t *hist, int blocks) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kChunk;
+    for (int k = 0; k < kSortItems; ++k) {
+        const int64_t i = base + (int64_t)k * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xffu], 1u);
+    }
+    __syncthreads();
+    hist[(size_t)threadIdx.x * blocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter: each block walks its chunk in rounds of 256 keys in order; within a round,
+// equal digits are ranked by lane (match_any) and by warp (per-warp digit counts).
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsigned long long *keys_in,
+                                                                     const int32_t *vals_in,
+                                                                     unsigned long long *keys_out,
+                                                                     int32_t *vals_out, int64_t n, int shift,
+                                                                     const uint32_t *offsets, int blocks) {
+    constexpr int kWarps = kSortThreads / 32;
+    __shared__ uint32_t wcnt[kWarps][256];
+    __shared__ uint32_t run[256];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    run[t] = offsets[(size_t)t * blocks + blockIdx.x];
+    const int64_t base = (int64_t)blockIdx.x * kChunk;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int k = 0; k < kSortItems; ++k) {
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) wcnt[w][t] = 0;
+        __syncthreads();
+        const int64_t i = base + (int64_t)k * kSortThreads + t;
+        const bool valid = i < n;
+        unsigned long long key = 0;
+        int32_t val = 0;
+        uint32_t d = 256;  // invalid lanes get a digit no key has
+        if (valid) {
+            key = keys_in[i];
+            val = vals_in[i];
+            d = (uint32_t)((key >> shift) & 0xffu);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned rank = __popc(peers & lt);
+        if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            uint32_t pos = run[d] + rank;
+            for (int w = 0; w < warp; ++w) pos += wcnt[w][d];
+            keys_out[pos] = key;
+            vals_out[pos] = val;
+        }
+        __syncthreads();
+        uint32_t tot = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) tot += wcnt[w][t];
+        run[t] += tot;
+        __syncthreads();
+    }
+}
+
+size_t radix_scratch_words(int64_t n) {
+    const int64_t blocks = (n + kChunk - 1) / kChunk;
+    const int64_t h = 256 * blocks;
+    return (size_t)h + scan_scratch_words(h);
+}
+
+// Sorts (keys, vals) by the bits [0, bits) of the keys, stably.  Uses (keys_alt, vals_alt) as the
+// ping-pong buffers; the result lands back in (keys, vals).
+int radix_sort_u64(unsigned long long *keys, int32_t *vals, unsigned long long *keys_alt, int32_t *vals_alt,
+                   int64_t n, int bits, uint32_t *scratch, cudaStream_t s, uint64_t *launches) {
+    if (n <= 1) return GTD_OK;
+    const int blocks = (int)((n + kChunk - 1) / kChunk);
+    uint32_t *hist = scratch;
+    uint32_t *scan_scratch = scratch + (size_t)256 * blocks;
+    unsigned long long *ka = keys, *kb = keys_alt;
+    int32_t *va = vals, *vb = vals_alt;
+    int passes = 0;
+    for (int shift = 0; shift < bits; shift += 8, ++passes) {
+        radix_hist_kernel<<<blocks, kSortThreads, 0, s>>>(ka, n, shift, hist, blocks);
+        GTD_CHECK_LAUNCH();
+        int rc = exclusive_scan_u32(hist, hist, (int64_t)256 * blocks, scan_scratch, s, launches);
+        if (rc) return rc;
+        radix_scatter_kernel<<<blocks, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist, blocks);
+        GTD_CHECK_LAUNCH();
+        if (launches) *launches += 2;
+        unsigned long long *tk = ka; ka = kb; kb = tk;
+        int32_t *tv = va; va = vb; vb = tv;
+    }
+    if (ka != keys) {
+        GTD_CUDA(cudaMemcpyAsync(keys, ka, sizeof(unsigned long long) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+        GTD_CUDA(cudaMemcpyAsync(vals, va, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    }
+    return GTD_OK;
+}
+
+}  // namespace gtd

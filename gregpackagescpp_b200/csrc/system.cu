@@ -2,6 +2,7 @@
 // of the AoS bodies, and the evolve() loop of gregsys.hpp:2593-3071 driven on one CUDA stream.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -72,6 +73,14 @@ void release_bodies(gtd_system *s) {
     cudaFree(s->ids);
     cudaFree(s->partials);
     cudaFree(s->escratch);
+    cudaFree(s->sc4);
+    cudaFree(s->sc1);
+    cudaFree(s->sci);
+    cudaFree(s->bh_ninter);
+    s->sc4 = nullptr;
+    s->sc1 = nullptr;
+    s->sci = nullptr;
+    s->bh_ninter = nullptr;
     cudaFreeHost(s->stage);
     s->pm[0] = s->pm[1] = s->vel = s->acc = s->pred_pos = s->pred_vel = nullptr;
     s->rad = s->rest = nullptr;
@@ -259,11 +268,43 @@ int run_collisions(gtd_system *s);  // collide.cu
 int bh_evolve_kdk(gtd_system *s, uint64_t steps);  // octree.cu
 int bh_accelerations(gtd_system *s, double *a3, uint32_t *n_inter);  // octree.cu
 
+int output_rows(gtd_system *s, std::vector<int64_t> &row) {
+    const int64_t n = s->n;
+    row.resize((size_t)n);
+    if (!s->ordered && n == s->n_uploaded) {
+        for (int64_t i = 0; i < n; ++i) row[(size_t)i] = i;
+        return GTD_OK;
+    }
+    std::vector<int32_t> ids((size_t)n);
+    GTD_CUDA(cudaMemcpyAsync(ids.data(), s->ids, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    if (n == s->n_uploaded) {
+        for (int64_t i = 0; i < n; ++i) row[(size_t)i] = ids[(size_t)i];
+        return GTD_OK;
+    }
+    std::vector<int64_t> idx((size_t)n);
+    for (int64_t i = 0; i < n; ++i) idx[(size_t)i] = i;
+    std::sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return ids[(size_t)a] < ids[(size_t)b]; });
+    for (int64_t k = 0; k < n; ++k) row[(size_t)idx[(size_t)k]] = k;
+    return GTD_OK;
+}
+
+// The mixed kernel centres each row's FP32 frame on the row; Morton-ordered bodies keep rows
+// compact, so the mixed path reorders at the start of an evolve and every reorder_interval steps.
+static int maybe_reorder(gtd_system *s, bool force) {
+    if (s->precision != GTD_PREC_MIXED || s->n < 2) return GTD_OK;
+    if (!force && s->steps_since_reorder < (uint64_t)s->reorder_interval) return GTD_OK;
+    s->steps_since_reorder = 0;
+    return reorder_bodies(s);
+}
+
 static int evolve_begin(gtd_system *s, int method) {
     s->method = method;
     s->begun = true;
     s->synced = true;
     if (s->n == 0) return GTD_OK;
+    int rc = maybe_reorder(s, true);
+    if (rc) return rc;
     if (method == GTD_LEAPFROG_KDK) {
         StepArgs a = step_args(s, s->pm[s->cur], true);
         return force_and_integrate(s, s->pm[s->cur], EPI_ACC, a);
@@ -276,8 +317,11 @@ static int evolve_steps(gtd_system *s, uint64_t k) {
     if (s->n == 0 || k == 0) return GTD_OK;
     for (uint64_t i = 0; i < k; ++i) {
         const bool last = (i + 1 == k) || s->coll != GTD_NO_COLL;
-        int rc = direct_step(s, s->method, last);
+        int rc = maybe_reorder(s, false);
         if (rc) return rc;
+        rc = direct_step(s, s->method, last);
+        if (rc) return rc;
+        s->steps_since_reorder += 1;
         if (s->coll != GTD_NO_COLL) {
             rc = run_collisions(s);
             if (rc) return rc;
@@ -384,10 +428,13 @@ int gtd_system_upload(gtd_system *s, int64_t n, const double *m, const double *r
     int rc = ensure_capacity(s, n);
     if (rc) return rc;
     s->n = n;
+    s->n_uploaded = n;
     s->cur = 0;
     s->begun = false;
     s->synced = true;
     s->tree_valid = false;
+    s->ordered = false;
+    s->steps_since_reorder = 0;
     if (n == 0) return GTD_OK;
     for (int64_t i = 0; i < n; ++i) {
         if (m[i] < 0) return fail(GTD_ERR_INVALID_ARGUMENT, "negative mass at body %lld", (long long)i);
@@ -436,16 +483,42 @@ int gtd_system_download(gtd_system *s, int64_t *n_out, double *m, double *r, dou
     if (r) GTD_CUDA(cudaMemcpyAsync(hr, s->rad, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
     if (rest) GTD_CUDA(cudaMemcpyAsync(he, s->rest, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
     GTD_CUDA(cudaStreamSynchronize(s->stream));
+    std::vector<int64_t> row;
+    int rc = output_rows(s, row);
+    if (rc) return rc;
     for (int64_t i = 0; i < n; ++i) {
-        if (m) m[i] = hp[i].w;
-        if (x3) { x3[3 * i] = hp[i].x; x3[3 * i + 1] = hp[i].y; x3[3 * i + 2] = hp[i].z; }
-        if (v3) { v3[3 * i] = hv[i].x; v3[3 * i + 1] = hv[i].y; v3[3 * i + 2] = hv[i].z; }
-        if (a3) { a3[3 * i] = ha[i].x; a3[3 * i + 1] = ha[i].y; a3[3 * i + 2] = ha[i].z; }
-        if (r) r[i] = hr[i];
-        if (rest) rest[i] = he[i];
+        const int64_t o = row[(size_t)i];
+        if (m) m[o] = hp[i].w;
+        if (x3) { x3[3 * o] = hp[i].x; x3[3 * o + 1] = hp[i].y; x3[3 * o + 2] = hp[i].z; }
+        if (v3) { v3[3 * o] = hv[i].x; v3[3 * o + 1] = hv[i].y; v3[3 * o + 2] = hv[i].z; }
+        if (a3) { a3[3 * o] = ha[i].x; a3[3 * o + 1] = ha[i].y; a3[3 * o + 2] = ha[i].z; }
+        if (r) r[o] = hr[i];
+        if (rest) rest[o] = he[i];
     }
     return GTD_OK;
 }
+
+}  // extern "C"
+
+// Device acceleration array -> host triples in host row order.
+int copy_acc_out(gtd_system *s, double *a3) {
+    const int64_t n = s->n;
+    std::vector<double4> h((size_t)n);
+    GTD_CUDA(cudaMemcpyAsync(h.data(), s->acc, sizeof(double4) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    std::vector<int64_t> row;
+    int rc = output_rows(s, row);
+    if (rc) return rc;
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t o = row[(size_t)i];
+        a3[3 * o] = h[i].x;
+        a3[3 * o + 1] = h[i].y;
+        a3[3 * o + 2] = h[i].z;
+    }
+    return GTD_OK;
+}
+
+extern "C" {
 
 int gtd_system_evolve_begin(gtd_system *s, int method) {
     if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
@@ -500,19 +573,13 @@ int gtd_system_accelerations(gtd_system *s, int method, double *a3) {
     DeviceGuard g(s->device);
     if (s->n == 0) return GTD_OK;
     if ((method & GTD_BARNES_HUT) == GTD_BARNES_HUT) return bh_accelerations(s, a3, nullptr);
+    int rc = maybe_reorder(s, true);
+    if (rc) return rc;
     StepArgs a = step_args(s, s->pm[s->cur], true);
-    int rc = force_and_integrate(s, s->pm[s->cur], EPI_ACC, a);
+    rc = force_and_integrate(s, s->pm[s->cur], EPI_ACC, a);
     if (rc) return rc;
     GTD_CUDA(cudaStreamSynchronize(s->stream));
-    if (a3) {
-        std::vector<double4> h((size_t)s->n);
-        GTD_CUDA(cudaMemcpy(h.data(), s->acc, sizeof(double4) * (size_t)s->n, cudaMemcpyDeviceToHost));
-        for (int64_t i = 0; i < s->n; ++i) {
-            a3[3 * i] = h[i].x;
-            a3[3 * i + 1] = h[i].y;
-            a3[3 * i + 2] = h[i].z;
-        }
-    }
+    if (a3) return copy_acc_out(s, a3);
     return GTD_OK;
 }
 

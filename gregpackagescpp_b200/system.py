@@ -143,6 +143,7 @@ class System:
         check(L.gtd_system_set_params(self._h, self.G, self.dt, max(self.iterations, 1), self.eps, self.theta))
         mode = _lib.MERGE_COLL if self.merge and self.collisions else self.collisions
         check(L.gtd_system_set_collisions(self._h, mode))
+        check(L.gtd_bh_set_tree_float(self._h, 1 if getattr(self, "_bh_float", True) else 0))
         check(L.gtd_system_upload(self._h, len(self.m), ptr(self.m), ptr(self.r), ptr(self.rest), ptr(self.x),
                                   ptr(self.v)))
 
@@ -199,6 +200,41 @@ class System:
         p, com = np.zeros(3), np.zeros(3)
         check(self._L.gtd_system_energy(self._h, C.byref(ke), C.byref(pe), ptr(p), ptr(com)))
         return ke.value, pe.value, p, com
+
+    # ---- Barnes-Hut (greg8tree.hpp) ---------------------------------------------------------
+    def bh_build(self, tree_float: bool = True) -> None:
+        """bh_tree::add_bodies + calc_com (greg8tree.hpp:1062-1078) on the device."""
+        self._push()
+        check(self._L.gtd_bh_build(self._h, 1 if tree_float else 0))
+
+    def bh_tree(self) -> dict:
+        """The last built octree: sorted Morton codes, slot -> body, and per node in DFS pre-order
+        depth, leaf flag, first slot, body count, skip link, mass, centre of mass, cell width."""
+        L = self._L
+        nn, nl = C.c_int64(), C.c_int64()
+        box = np.zeros(6)
+        check(L.gtd_bh_tree_size(self._h, C.byref(nn), C.byref(nl), ptr(box)))
+        n, k = len(self.m), nn.value
+        out = dict(n_nodes=k, n_leaves=nl.value, box=box, code=np.zeros(n, np.uint64), perm=np.zeros(n, np.int32),
+                   depth=np.zeros(k, np.int8), is_leaf=np.zeros(k, np.int8), first=np.zeros(k, np.int32),
+                   count=np.zeros(k, np.int32), skip=np.zeros(k, np.int32), mass=np.zeros(k),
+                   com=np.zeros((k, 3)), width=np.zeros(k))
+        check(L.gtd_bh_tree_download(self._h, *(ptr(out[f]) for f in ("code", "perm", "depth", "is_leaf", "first",
+                                                                      "count", "skip", "mass", "com", "width"))))
+        return out
+
+    def bh_accelerations(self, tree_float: bool = True):
+        """Barnes-Hut accelerations with the reference walk (greg8tree.hpp:702-833, bh_acc
+        gregsys.hpp:371-375 accumulated) and the interactions each body took."""
+        self.bh_build(tree_float)
+        a = np.zeros((len(self.m), 3))
+        cnt = np.zeros(len(self.m), np.uint32)
+        check(self._L.gtd_bh_accelerations(self._h, ptr(a), ptr(cnt)))
+        return a, cnt
+
+    def bh_tree_float(self, tree_float: bool) -> None:
+        """Selects T=float (True, the default) or T=double geometry for the Barnes-Hut evolve."""
+        self._bh_float = bool(tree_float)
 
     def launch_count(self) -> int:
         c = C.c_uint64()

@@ -137,6 +137,8 @@ GTD_API int gtd_measure_fma_peak(int device, int precision, double *flops_per_s)
  * with skip links, FP64 centres of mass (calc_com :213-281).  tree_float = 1 builds in T=float
  * (positions rounded to float), 0 in T=double.  Replaces bh_tree::add_bodies + calc_com. */
 GTD_API int gtd_bh_build(gtd_system *sys, int tree_float);
+/* Tree geometry for evolve(leapfrog_kdk | barnes_hut): 1 = T=float (the default), 0 = T=double. */
+GTD_API int gtd_bh_set_tree_float(gtd_system *sys, int tree_float);
 GTD_API int gtd_bh_tree_size(gtd_system *sys, int64_t *n_nodes, int64_t *n_leaves, double *box6);
 /* Copies the tree out (any pointer may be NULL): sorted codes and slot->body permutation [n],
  * then per node in pre-order: depth, leaf flag, first slot, body count, skip, mass, com, width.

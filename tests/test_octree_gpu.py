@@ -1,0 +1,143 @@
+"""Barnes-Hut on the B200 through the C ABI.
+
+* Topology: Morton codes, slot order, every node's depth / leaf flag / range / skip link / cell
+  width and the FP64 centres of mass are bit-exact against the host rebuild (oracle/), which is
+  itself pinned to the reference's pointer octree (tests/test_oracle_pins.py).
+* Walk: per-body interaction counts equal the host rebuild's exactly; accelerations match the
+  reference's corrected walk (FP64 tree) to 1e-12 and the FP32 walk to 1e-5.
+"""
+import numpy as np
+import pytest
+
+from gregpackagescpp_b200 import IndistinguishableBodies, InvalidBodyPlacement, System
+from gregpackagescpp_b200.ics import AU, UNITS_G6674, plummer, two_plummer
+
+pytestmark = pytest.mark.gpu
+G = 6.674e-11
+
+
+def gpu_tree(m, x, tree_float):
+    s = System(m, x, np.zeros_like(x), units_format=UNITS_G6674)
+    s.bh_build(tree_float)
+    return s, s.bh_tree()
+
+
+def compare_tree(t, o):
+    assert t["n_nodes"] == o["n_nodes"]
+    assert t["n_leaves"] == o["n_leaves"]
+    assert np.array_equal(t["box"], o["box"])
+    assert np.array_equal(t["code"], o["code"])
+    assert np.array_equal(t["perm"], o["perm"])
+    for f in ("depth", "is_leaf", "first", "count", "skip", "width", "mass"):
+        assert np.array_equal(t[f], o[f]), f
+    assert np.array_equal(t["com"], o["com"])
+
+
+@pytest.mark.parametrize("tree_float", [0, 1])
+@pytest.mark.parametrize("n,seed", [(2, 1), (3, 2), (100, 3), (2000, 7), (20000, 9), (65537, 10)])
+def test_topology_bit_exact_vs_host_rebuild(gpu, oracle, tree_float, n, seed):
+    m, x, _ = plummer(n, seed)
+    s, t = gpu_tree(m, x, tree_float)
+    o = oracle.bh_tree(x, m, tree_float)
+    try:
+        compare_tree(t, o)
+    finally:
+        oracle.bh_free(o)
+
+
+def test_topology_two_spheres(gpu, oracle):
+    m, x, _ = two_plummer(50000, 4)
+    s, t = gpu_tree(m, x, 1)
+    o = oracle.bh_tree(x, m, 1)
+    try:
+        compare_tree(t, o)
+    finally:
+        oracle.bh_free(o)
+
+
+@pytest.mark.parametrize("isf", [0, 1])
+def test_topology_vs_reference_golden(gpu, golden, isf):
+    g = golden
+    s, t = gpu_tree(g["bh_m"], g["bh_x"], isf)
+    assert t["n_nodes"] == len(g[f"bh_tree{isf}_depth"])
+    assert np.array_equal(t["depth"], g[f"bh_tree{isf}_depth"])
+    leaf_body = np.where(t["is_leaf"] == 1, t["perm"][t["first"]], -1)
+    assert np.array_equal(leaf_body, g[f"bh_tree{isf}_body"])
+    assert np.array_equal(t["box"], g[f"bh_tree{isf}_box"])
+    assert np.array_equal(t["width"], g[f"bh_tree{isf}_width"])
+
+
+def test_fp64_walk_vs_reference_golden(gpu, golden, oracle):
+    g = golden
+    s = System(g["bh_m"], g["bh_x"], np.zeros_like(g["bh_x"]), units_format=UNITS_G6674)
+    s.set_bh_opening_angle(0.5)
+    a, cnt = s.bh_accelerations(tree_float=False)
+    assert int(cnt.sum()) == int(g["bh_count"])
+    rel = np.linalg.norm(a - g["bh_acc"], axis=1) / np.linalg.norm(g["bh_acc"], axis=1)
+    assert rel.max() < 1e-12
+    t = oracle.bh_tree(g["bh_x"], g["bh_m"], 0)
+    try:
+        _, ocnt = oracle.bh_acc(t, g["bh_x"], g["bh_m"], 0, 0.5, 0.0, G)
+    finally:
+        oracle.bh_free(t)
+    assert np.array_equal(cnt, ocnt)
+
+
+@pytest.mark.parametrize("n,theta", [(5000, 0.5), (30000, 0.5), (30000, 1.0), (3000, 0.0)])
+def test_fp32_walk_vs_host_rebuild(gpu, oracle, n, theta):
+    m, x, _ = plummer(n, 30 + n)
+    s = System(m, x, np.zeros_like(x), units_format=UNITS_G6674)
+    s.set_bh_opening_angle(theta)
+    a, cnt = s.bh_accelerations(tree_float=True)
+    t = oracle.bh_tree(x, m, 1)
+    try:
+        ao, ocnt = oracle.bh_acc(t, x, m, 1, theta, 0.0, G)
+    finally:
+        oracle.bh_free(t)
+    assert np.array_equal(cnt, ocnt)
+    rel = np.linalg.norm(a - ao, axis=1) / np.linalg.norm(ao, axis=1)
+    assert np.sqrt((rel ** 2).mean()) < 1e-5 and rel.max() < 1e-3
+
+
+def test_theta_zero_is_direct_sum(gpu, oracle):
+    """theta = 0 opens every cell: the walk degenerates to direct summation over leaves."""
+    m, x, _ = plummer(1500, 41)
+    s = System(m, x, np.zeros_like(x), units_format=UNITS_G6674)
+    s.set_bh_opening_angle(0.0)
+    a, cnt = s.bh_accelerations(tree_float=False)
+    assert np.all(cnt == len(m) - 1)
+    ad = oracle.direct_acc(m, x, oracle.G(UNITS_G6674))
+    rel = np.linalg.norm(a - ad, axis=1) / np.linalg.norm(ad, axis=1)
+    assert rel.max() < 1e-12
+
+
+def test_bh_kdk_vs_reference_golden(gpu, golden):
+    g = golden
+    s = System(g["bhk_m"], g["bhk_x"], g["bhk_v"], timestep=3600.0, num_iterations=5, units_format=UNITS_G6674)
+    s.set_bh_opening_angle(0.5)
+    s.bh_tree_float(False)
+    s.evolve(System.leapfrog_kdk | System.barnes_hut)
+    assert np.abs(s.x - g["bhk_xo"]).max() / np.abs(g["bhk_xo"]).max() < 1e-12
+    assert np.abs(s.v - g["bhk_vo"]).max() / np.abs(g["bhk_vo"]).max() < 1e-10
+
+
+def test_single_body_rejected_like_reference(gpu):
+    s = System(np.array([1e30]), np.zeros((1, 3)), np.zeros((1, 3)))
+    with pytest.raises(InvalidBodyPlacement):
+        s.bh_build(True)
+
+
+def test_coincident_bodies_rejected(gpu):
+    m, x, _ = plummer(100, 5)
+    x[17] = x[42]
+    s = System(m, x, np.zeros_like(x))
+    with pytest.raises(IndistinguishableBodies):
+        s.bh_build(False)
+
+
+def test_nonfinite_position_rejected(gpu):
+    m, x, _ = plummer(100, 6)
+    x[3, 1] = np.nan
+    s = System(m, x, np.zeros_like(x))
+    with pytest.raises(InvalidBodyPlacement):
+        s.bh_build(True)
