@@ -52,6 +52,10 @@ def parse_args():
     p.add_argument("--e2e-iterations", type=int, default=5)
     p.add_argument("--cpu-sample-n", type=int, default=8192)
     p.add_argument("--cpu-sample-steps", type=int, default=3)
+    p.add_argument("--drift-steps", type=int, default=0,
+                   help="instead of the benchmark: evolve the workload this many steps in both the mixed and the "
+                        "FP64 path and report |dE/E| and momentum drift every --drift-every steps")
+    p.add_argument("--drift-every", type=int, default=100)
     return p.parse_args()
 
 
@@ -269,9 +273,20 @@ def run_ours(args, rank, world, local):
         check(L.gtd_system_launch_count(h, C.byref(c)))
         return c.value
 
+    stage("autotune")
+    h64, hmx = make(_lib.PREC_F64), make(_lib.PREC_MIXED)
+    tuned = {}
+    for name, h in (("mixed", hmx), ("fp64", h64)):
+        best, best_ms = C.c_int(), C.c_double()
+        check(L.gtd_system_autotune_direct(h, 3, C.byref(best), C.byref(best_ms)))
+        ii, fold = C.c_int(), C.c_int()
+        check(L.gtd_direct_variant_info(_lib.PREC_MIXED if name == "mixed" else _lib.PREC_F64, best.value,
+                                        C.byref(ii), C.byref(fold)))
+        tuned[name] = {"variant": best.value, "i_per_thread": ii.value, "fold": fold.value,
+                       "force_ms": best_ms.value}
+
     stage("accuracy")
     # --- accuracy of the mixed force against the FP64 one at the initial state (untimed)
-    h64, hmx = make(_lib.PREC_F64), make(_lib.PREC_MIXED)
     a64, amx = np.zeros(3 * n), np.zeros(3 * n)
     check(L.gtd_system_accelerations(h64, 0, a64.ctypes.data))
     check(L.gtd_system_accelerations(hmx, 0, amx.ctypes.data))
@@ -393,11 +408,51 @@ def run_ours(args, rank, world, local):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "calls": args.e2e_calls, "iterations_per_call": iters},
             "gpu_launches": gpu_launches,
+            "autotuned": tuned,
             "clocks": clk,
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
+
+
+def run_drift(args, local):
+    """Energy and momentum conservation of the workload over a long run, mixed next to FP64."""
+    from gregpackagescpp_b200 import _lib
+    from gregpackagescpp_b200._lib import check
+    from gregpackagescpp_b200.ics import plummer
+
+    L = _lib.load()
+    n = args.n
+    m, x, v = plummer(n, args.seed)
+    x3, v3 = np.ascontiguousarray(x.reshape(-1)), np.ascontiguousarray(v.reshape(-1))
+    out = {"workload": f"N={n} Plummer, leapfrog KDK dt=3600 s", "steps": args.drift_steps, "series": {}}
+    for name, prec in (("mixed", _lib.PREC_MIXED), ("fp64", _lib.PREC_F64)):
+        h = C.c_void_p()
+        check(L.gtd_system_create(C.byref(h), local, prec))
+        check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, 1000, 0.0, 0.5))
+        check(L.gtd_system_upload(h, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
+        best = C.c_int()
+        check(L.gtd_system_autotune_direct(h, 2, C.byref(best), None))
+        ke, pe, p = C.c_double(), C.c_double(), np.zeros(3)
+        check(L.gtd_system_energy(h, C.byref(ke), C.byref(pe), p.ctypes.data, None))
+        E0, pscale = ke.value + pe.value, float((m[:, None] * np.abs(v)).sum())
+        rows = [(0, 0.0, float(np.linalg.norm(p)) / pscale)]
+        check(L.gtd_system_evolve_begin(h, 16))
+        t0 = time.perf_counter()
+        done = 0
+        while done < args.drift_steps:
+            k = min(args.drift_every, args.drift_steps - done)
+            check(L.gtd_system_evolve_steps(h, k))
+            done += k
+            check(L.gtd_system_energy(h, C.byref(ke), C.byref(pe), p.ctypes.data, None))
+            rows.append((done, (ke.value + pe.value - E0) / abs(E0), float(np.linalg.norm(p)) / pscale))
+        out["series"][name] = {"wall_s": time.perf_counter() - t0, "step_dE_over_E_dP": rows}
+        check(L.gtd_system_destroy(h))
+    mx, fx = out["series"]["mixed"]["step_dE_over_E_dP"], out["series"]["fp64"]["step_dE_over_E_dP"]
+    out["max_abs_dE_over_E"] = {"mixed": max(abs(r[1]) for r in mx), "fp64": max(abs(r[1]) for r in fx)}
+    out["max_abs_mixed_minus_fp64_dE_over_E"] = max(abs(a[1] - b[1]) for a, b in zip(mx, fx))
+    print(json.dumps(out), flush=True)
 
 
 def main():
@@ -406,6 +461,9 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.drift_steps > 0:
+            if rank == 0:
+                run_drift(args, local)
         else:
             run_ours(args, rank, world, local)
     finally:

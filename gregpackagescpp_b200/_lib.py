@@ -111,6 +111,10 @@ def load():
     L.gtd_system_time_force_kernels.argtypes = [vp, ip]
     L.gtd_system_force_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(u64), ip]
     L.gtd_measure_fma_peak.argtypes = [ip, ip, C.POINTER(C.c_double)]
+    L.gtd_direct_variant_count.argtypes = [ip, C.POINTER(C.c_int)]
+    L.gtd_direct_variant_info.argtypes = [ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.gtd_system_set_direct_variant.argtypes = [vp, ip]
+    L.gtd_system_autotune_direct.argtypes = [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.gtd_bh_build.argtypes = [vp, ip]
     L.gtd_bh_set_tree_float.argtypes = [vp, ip]
     L.gtd_bh_tree_size.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), dp]

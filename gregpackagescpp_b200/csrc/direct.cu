@@ -107,11 +107,11 @@ __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
 
 // -------------------------------------------------------------------------------------------
 // Mixed precision.  Each j-tile is staged in shared memory as FP32 coordinates relative to the
-// row's centre c (taken in FP64 from the row's first body), with G m_j in FP32.  Pair arithmetic
-// runs two j-bodies per instruction on the packed FP32x2 pipe (add/mul/fma .f32x2) with one MUFU
-// rsqrt per pair; each i keeps FP32 partial sums for kFold j-bodies, then folds them into FP64
-// Kahan-compensated accumulators.  Tiles that overlap the row (where i == j occurs) take the
-// guarded path; all others run without a compare.
+// row's centre c (the FP64 mean position of the row's bodies, which the Morton reordering keeps
+// compact), with G m_j in FP32.  Pair arithmetic runs two j-bodies per instruction on the packed
+// FP32x2 pipe (add/mul/fma .f32x2) with one MUFU rsqrt per pair; each i keeps FP32 partial sums
+// for FOLD j-bodies, then folds them into FP64 Kahan-compensated accumulators.  Tiles that
+// overlap the row (where i == j occurs) take the guarded path; all others run without a compare.
 // -------------------------------------------------------------------------------------------
 __device__ __forceinline__ float rsqrt_approx(float x) {
     float y;
@@ -126,7 +126,7 @@ __device__ __forceinline__ void kahan_add(double &sum, double &comp, double v) {
     sum = t;
 }
 
-template <int I, bool kGuard>
+template <int I, int FOLD, bool kGuard>
 __device__ __forceinline__ void mixed_tile(const float *__restrict__ tx, const float *__restrict__ ty,
                                            const float *__restrict__ tz, const float *__restrict__ tm,
                                            const float2 (&nx)[I], const float2 (&ny)[I], const float2 (&nz)[I],
@@ -137,12 +137,12 @@ __device__ __forceinline__ void mixed_tile(const float *__restrict__ tx, const f
     const float2 *Z = reinterpret_cast<const float2 *>(tz);
     const float2 *M = reinterpret_cast<const float2 *>(tm);
 #pragma unroll 1
-    for (int q0 = 0; q0 < kThreads / 2; q0 += kFold / 2) {
+    for (int q0 = 0; q0 < kThreads / 2; q0 += FOLD / 2) {
         float2 fx[I], fy[I], fz[I];
 #pragma unroll
         for (int k = 0; k < I; ++k) fx[k] = fy[k] = fz[k] = make_float2(0.f, 0.f);
 #pragma unroll 8
-        for (int u = 0; u < kFold / 2; ++u) {
+        for (int u = 0; u < FOLD / 2; ++u) {
             const float2 xj = X[q0 + u], yj = Y[q0 + u], zj = Z[q0 + u], mj = M[q0 + u];
 #pragma unroll
             for (int k = 0; k < I; ++k) {
@@ -174,8 +174,8 @@ __device__ __forceinline__ void mixed_tile(const float *__restrict__ tx, const f
     }
 }
 
-template <int I>
-__global__ void __launch_bounds__(kThreads, 2) force_mixed_kernel(ForceKArgs a) {
+template <int I, int FOLD, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs a) {
     __shared__ __align__(16) float tx[2][kThreads];
     __shared__ __align__(16) float ty[2][kThreads];
     __shared__ __align__(16) float tz[2][kThreads];
@@ -268,9 +268,9 @@ __global__ void __launch_bounds__(kThreads, 2) force_mixed_kernel(ForceKArgs a) 
             const int64_t j0 = jt * kThreads;
             const bool diag = j0 < row0 + a.bi && row0 < j0 + kThreads;
             if (diag)
-                mixed_tile<I, true>(tx[cur], ty[cur], tz[cur], tm[cur], nx, ny, nz, sx, sy, sz, cx, cy, cz);
+                mixed_tile<I, FOLD, true>(tx[cur], ty[cur], tz[cur], tm[cur], nx, ny, nz, sx, sy, sz, cx, cy, cz);
             else
-                mixed_tile<I, false>(tx[cur], ty[cur], tz[cur], tm[cur], nx, ny, nz, sx, sy, sz, cx, cy, cz);
+                mixed_tile<I, FOLD, false>(tx[cur], ty[cur], tz[cur], tm[cur], nx, ny, nz, sx, sy, sz, cx, cy, cz);
             if (more) {
                 const int nb = cur ^ 1;
                 if (have) {
@@ -304,10 +304,55 @@ __global__ void __launch_bounds__(kThreads, 2) force_mixed_kernel(ForceKArgs a) 
 // -------------------------------------------------------------------------------------------
 // Plan and launch
 // -------------------------------------------------------------------------------------------
-ForcePlan make_plan(int64_t n, int precision, int device) {
+// Kernel variants: i-bodies per thread (I) and, for the mixed kernel, the j-bodies summed in FP32
+// between FP64 folds (FOLD).  Index 0 of each table is the default; gtd_system_autotune_direct
+// times them all on the caller's bodies and keeps the fastest.
+struct VariantInfo {
+    int i, fold;
+};
+static const VariantInfo kMixedVariants[] = {{2, 64}, {1, 64}, {2, 32}, {2, 128}, {3, 64}, {4, 64}, {4, 128}};
+static const VariantInfo kF64Variants[] = {{2, 0}, {1, 0}, {4, 0}};
+constexpr int kNumMixed = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
+constexpr int kNumF64 = sizeof(kF64Variants) / sizeof(kF64Variants[0]);
+
+int variant_count(int precision) { return precision == GTD_PREC_MIXED ? kNumMixed : kNumF64; }
+
+int variant_info(int precision, int v, int *i, int *fold) {
+    if (v < 0 || v >= variant_count(precision)) return fail(GTD_ERR_INVALID_ARGUMENT, "variant %d out of range", v);
+    const VariantInfo &vi = precision == GTD_PREC_MIXED ? kMixedVariants[v] : kF64Variants[v];
+    if (i) *i = vi.i;
+    if (fold) *fold = vi.fold;
+    return GTD_OK;
+}
+
+template <typename F>
+static void with_mixed(int v, F &&f) {
+    switch (v) {
+        case 1: f(force_mixed_kernel<1, 64, 2>); break;
+        case 2: f(force_mixed_kernel<2, 32, 2>); break;
+        case 3: f(force_mixed_kernel<2, 128, 2>); break;
+        case 4: f(force_mixed_kernel<3, 64, 1>); break;
+        case 5: f(force_mixed_kernel<4, 64, 1>); break;
+        case 6: f(force_mixed_kernel<4, 128, 1>); break;
+        default: f(force_mixed_kernel<2, 64, 2>); break;
+    }
+}
+
+template <typename F>
+static void with_f64(int v, F &&f) {
+    switch (v) {
+        case 1: f(force_f64_kernel<1>); break;
+        case 2: f(force_f64_kernel<4>); break;
+        default: f(force_f64_kernel<2>); break;
+    }
+}
+
+ForcePlan make_plan(int64_t n, int precision, int device, int variant) {
     ForcePlan p;
     p.n = n;
-    p.bi = kThreads * (precision == GTD_PREC_MIXED ? kIMix : kI64);
+    p.variant = (variant >= 0 && variant < variant_count(precision)) ? variant : 0;
+    const VariantInfo &vi = precision == GTD_PREC_MIXED ? kMixedVariants[p.variant] : kF64Variants[p.variant];
+    p.bi = kThreads * vi.i;
     p.bj = kThreads;
     p.rows = (n + p.bi - 1) / p.bi;
     p.tiles = (n + p.bj - 1) / p.bj;
@@ -315,9 +360,9 @@ ForcePlan make_plan(int64_t n, int precision, int device) {
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (precision == GTD_PREC_MIXED)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, force_mixed_kernel<kIMix>, kThreads, 0);
+        with_mixed(p.variant, [&](auto k) { cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, 0); });
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, force_f64_kernel<kI64>, kThreads, 0);
+        with_f64(p.variant, [&](auto k) { cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, 0); });
     if (per_sm < 1) per_sm = 1;
     int64_t grid = (int64_t)sms * per_sm;
     if (grid > p.total) grid = p.total > 0 ? p.total : 1;
@@ -333,9 +378,9 @@ int launch_force(int precision, const ForcePlan &p, const double4 *src, double G
     if (p.n == 0) return GTD_OK;
     ForceKArgs a{p.n, p.rows, p.tiles, p.total, p.grid, p.bi, src, G, partials};
     if (precision == GTD_PREC_MIXED)
-        force_mixed_kernel<kIMix><<<p.grid, kThreads, 0, s>>>(a);
+        with_mixed(p.variant, [&](auto k) { k<<<p.grid, kThreads, 0, s>>>(a); });
     else
-        force_f64_kernel<kI64><<<p.grid, kThreads, 0, s>>>(a);
+        with_f64(p.variant, [&](auto k) { k<<<p.grid, kThreads, 0, s>>>(a); });
     GTD_CHECK_LAUNCH();
     return GTD_OK;
 }

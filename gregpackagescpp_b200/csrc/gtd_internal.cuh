@@ -37,13 +37,11 @@ struct ForcePlan {
     int64_t rows = 0, tiles = 0, total = 0;
     int grid = 0;            // CTAs of the force kernel
     int64_t slots = 0;       // partial-sum slots (grid + rows)
+    int variant = 0;         // kernel variant (i-bodies per thread, fold length)
 };
 
 // Per-thread launch shape of the two force kernels.
 constexpr int kThreads = 256;
-constexpr int kI64 = 2;      // i-bodies per thread, FP64 kernel
-constexpr int kIMix = 2;     // i-bodies per thread, mixed kernel
-constexpr int kFold = 64;    // j-bodies summed in FP32 before each FP64 Kahan fold (mixed)
 
 enum Epilogue : int {
     EPI_ACC = 0,         // acc = a
@@ -68,7 +66,9 @@ struct StepArgs {
     int last;             // KDK/DKD: leave the state synchronised
 };
 
-ForcePlan make_plan(int64_t n, int precision, int device);
+ForcePlan make_plan(int64_t n, int precision, int device, int variant);
+int variant_count(int precision);
+int variant_info(int precision, int variant, int *i_per_thread, int *fold);
 size_t partial_bytes(const ForcePlan &p);
 // Force on every body of `src` (positions + G-free masses), written as partial sums.
 int launch_force(int precision, const ForcePlan &p, const double4 *src, double G, double *partials,

@@ -36,6 +36,7 @@ struct gtd_system {
     // direct summation
     gtd::ForcePlan plan;
     int plan_prec = -1;
+    int variant = 0;  // force-kernel variant (gtd_system_set_direct_variant / autotune)
     double *partials = nullptr;
     size_t part_bytes = 0;
     double *escratch = nullptr;

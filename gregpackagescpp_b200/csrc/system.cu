@@ -94,8 +94,9 @@ void release_bodies(gtd_system *s) {
 }
 
 int ensure_plan(gtd_system *s) {
-    if (s->plan.n == s->n && s->plan_prec == s->precision && s->partials) return GTD_OK;
-    s->plan = make_plan(s->n, s->precision, s->device);
+    if (s->plan.n == s->n && s->plan_prec == s->precision && s->plan.variant == s->variant && s->partials)
+        return GTD_OK;
+    s->plan = make_plan(s->n, s->precision, s->device, s->variant);
     s->plan_prec = s->precision;
     const size_t need = partial_bytes(s->plan);
     if (need > s->part_bytes) {
@@ -616,6 +617,66 @@ int gtd_system_energy(gtd_system *s, double *ke, double *pe, double *p3, double 
 int gtd_system_launch_count(const gtd_system *s, uint64_t *count) {
     if (!s || !count) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
     *count = s->launches;
+    return GTD_OK;
+}
+
+int gtd_direct_variant_count(int precision, int *count) {
+    if (!count) return fail(GTD_ERR_INVALID_ARGUMENT, "count is NULL");
+    *count = variant_count(precision);
+    return GTD_OK;
+}
+
+int gtd_direct_variant_info(int precision, int variant, int *i_per_thread, int *fold) {
+    return variant_info(precision, variant, i_per_thread, fold);
+}
+
+int gtd_system_set_direct_variant(gtd_system *s, int variant) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (variant < 0) variant = 0;
+    if (variant >= variant_count(s->precision)) return fail(GTD_ERR_INVALID_ARGUMENT, "variant %d out of range", variant);
+    s->variant = variant;
+    return GTD_OK;
+}
+
+int gtd_system_autotune_direct(gtd_system *s, int reps, int *best, double *best_ms) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (s->n == 0) return fail(GTD_ERR_INVALID_ARGUMENT, "autotune needs bodies");
+    DeviceGuard g(s->device);
+    if (reps < 1) reps = 1;
+    int rc = maybe_reorder(s, true);
+    if (rc) return rc;
+    const int prev = s->variant;
+    int arg = prev;
+    double bestv = 1e300;
+    for (int v = 0; v < variant_count(s->precision); ++v) {
+        s->variant = v;
+        rc = ensure_plan(s);
+        if (rc) return rc;
+        // warm-up launch, then the median of `reps` timed force launches
+        rc = launch_force(s->precision, s->plan, s->pm[s->cur], s->G, s->partials, s->stream);
+        if (rc) return rc;
+        std::vector<float> t(reps);
+        for (int k = 0; k < reps; ++k) {
+            GTD_CUDA(cudaEventRecord(s->ev0, s->stream));
+            rc = launch_force(s->precision, s->plan, s->pm[s->cur], s->G, s->partials, s->stream);
+            if (rc) return rc;
+            GTD_CUDA(cudaEventRecord(s->ev1, s->stream));
+            GTD_CUDA(cudaEventSynchronize(s->ev1));
+            GTD_CUDA(cudaEventElapsedTime(&t[k], s->ev0, s->ev1));
+        }
+        s->launches += (uint64_t)reps + 1;
+        std::sort(t.begin(), t.end());
+        const double med = t[reps / 2];
+        if (med < bestv) {
+            bestv = med;
+            arg = v;
+        }
+    }
+    s->variant = arg;
+    rc = ensure_plan(s);
+    if (rc) return rc;
+    if (best) *best = arg;
+    if (best_ms) *best_ms = bestv;
     return GTD_OK;
 }
 

@@ -125,6 +125,14 @@ GTD_API int gtd_system_stream(const gtd_system *sys, void **stream);
  * milliseconds and launch count. */
 GTD_API int gtd_system_time_force_kernels(gtd_system *sys, int enable);
 GTD_API int gtd_system_force_timing(gtd_system *sys, double *total_ms, uint64_t *launches, int reset);
+/* Force-kernel variants (i-bodies per thread; for GTD_PREC_MIXED also the j-bodies summed in FP32
+ * between FP64 folds).  Variant 0 is the default.  gtd_system_autotune_direct times every variant
+ * on the handle's current bodies (a warm-up and `reps` timed force launches each, median) and keeps
+ * the fastest for the handle; it leaves the bodies untouched apart from their order on the device. */
+GTD_API int gtd_direct_variant_count(int precision, int *count);
+GTD_API int gtd_direct_variant_info(int precision, int variant, int *i_per_thread, int *fold);
+GTD_API int gtd_system_set_direct_variant(gtd_system *sys, int variant);
+GTD_API int gtd_system_autotune_direct(gtd_system *sys, int reps, int *best, double *best_ms);
 /* Measured throughput of a dependent-FMA microkernel on `device` (all SMs): precision
  * GTD_PREC_MIXED gives FP32 FFMA FLOP/s, GTD_PREC_F64 gives FP64 DFMA FLOP/s (2 flops per FMA). */
 GTD_API int gtd_measure_fma_peak(int device, int precision, double *flops_per_s);
