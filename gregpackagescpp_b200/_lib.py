@@ -99,6 +99,7 @@ def load():
     L.gtd_system_set_params.argtypes = [vp, C.c_double, C.c_double, u64, C.c_double, C.c_double]
     L.gtd_system_set_collisions.argtypes = [vp, ip]
     L.gtd_system_upload.argtypes = [vp, i64, dp, dp, dp, dp, dp]
+    L.gtd_system_check_overlap.argtypes = [vp, ip, dp]
     L.gtd_system_download.argtypes = [vp, C.POINTER(i64), dp, dp, dp, dp, dp, dp]
     L.gtd_system_num_bodies.argtypes = [vp, C.POINTER(i64)]
     L.gtd_system_evolve.argtypes = [vp, ip, C.POINTER(i64)]

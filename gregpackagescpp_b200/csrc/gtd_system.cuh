@@ -104,6 +104,7 @@ struct gtd_system {
 void release_bodies(gtd_system *s);
 void release_tree(gtd_system *s);
 int reorder_bodies(gtd_system *s);
+int restore_upload_order(gtd_system *s);
 // row[s] = host row of device slot s: ascending upload index among the live bodies
 int output_rows(gtd_system *s, std::vector<int64_t> &row);
 // device accelerations -> host triples in host row order (synchronises the stream)

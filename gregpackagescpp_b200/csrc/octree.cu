@@ -511,6 +511,13 @@ __global__ void drift_kernel(int64_t n, double4 *pm, const double4 *vel, double 
     pm[i] = p;
 }
 
+__global__ void ids_to_keys_kernel(int64_t n, const int32_t *ids, unsigned long long *keys, int32_t *vals) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    keys[s] = (unsigned long long)(uint32_t)ids[s];
+    vals[s] = (int32_t)s;
+}
+
 // gather for the spatial reorder
 template <typename V>
 __global__ void gather_kernel(int64_t n, const int32_t *perm, const V *in, V *out) {
@@ -819,6 +826,40 @@ int reorder_bodies(gtd_system *s) {
     GTD_CHECK_LAUNCH();
     s->launches += 6;
     s->ordered = true;
+    s->tree_valid = false;
+    return GTD_OK;
+}
+
+// Puts the bodies back in upload order (ascending ids), undoing reorder_bodies; the order-dependent
+// collision passes scan in this order, as the reference scans its std::vector.
+int restore_upload_order(gtd_system *s) {
+    if (!s->ordered) return GTD_OK;
+    const int64_t n = s->n;
+    s->ordered = false;
+    if (n < 2) return GTD_OK;
+    int rc = ensure_tree_n(s, n);
+    if (rc) return rc;
+    cudaStream_t st = s->stream;
+    const unsigned g = blocks_for(n);
+    ids_to_keys_kernel<<<g, kTT, 0, st>>>(n, s->ids, s->codes, s->perm);
+    GTD_CHECK_LAUNCH();
+    s->launches += 1;
+    rc = radix_sort_u64(s->codes, s->perm, s->codes_alt, s->perm_alt, n, 32, s->scratch, st, &s->launches);
+    if (rc) return rc;
+    gather_kernel<double4><<<g, kTT, 0, st>>>(n, s->perm, s->pm[s->cur], s->pm[s->cur ^ 1]);
+    s->cur ^= 1;
+    gather_kernel<double4><<<g, kTT, 0, st>>>(n, s->perm, s->vel, s->sc4);
+    std::swap(s->vel, s->sc4);
+    gather_kernel<double4><<<g, kTT, 0, st>>>(n, s->perm, s->acc, s->sc4);
+    std::swap(s->acc, s->sc4);
+    gather_kernel<double><<<g, kTT, 0, st>>>(n, s->perm, s->rad, s->sc1);
+    std::swap(s->rad, s->sc1);
+    gather_kernel<double><<<g, kTT, 0, st>>>(n, s->perm, s->rest, s->sc1);
+    std::swap(s->rest, s->sc1);
+    gather_kernel<int32_t><<<g, kTT, 0, st>>>(n, s->perm, s->ids, s->sci);
+    std::swap(s->ids, s->sci);
+    GTD_CHECK_LAUNCH();
+    s->launches += 6;
     s->tree_valid = false;
     return GTD_OK;
 }

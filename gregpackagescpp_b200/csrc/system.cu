@@ -293,7 +293,8 @@ int output_rows(gtd_system *s, std::vector<int64_t> &row) {
 // The mixed kernel centres each row's FP32 frame on the row; Morton-ordered bodies keep rows
 // compact, so the mixed path reorders at the start of an evolve and every reorder_interval steps.
 static int maybe_reorder(gtd_system *s, bool force) {
-    if (s->precision != GTD_PREC_MIXED || s->n < 2) return GTD_OK;
+    // collisions scan the bodies in upload order (as the reference scans its vector): no reordering
+    if (s->precision != GTD_PREC_MIXED || s->n < 2 || s->coll != GTD_NO_COLL) return GTD_OK;
     if (!force && s->steps_since_reorder < (uint64_t)s->reorder_interval) return GTD_OK;
     s->steps_since_reorder = 0;
     return reorder_bodies(s);

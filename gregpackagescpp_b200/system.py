@@ -98,6 +98,19 @@ class System:
         self._L = L
         self.time_elapsed = 0.0
         self.allow_overlap = allow_overlapping_bodies
+        if not allow_overlapping_bodies:
+            self.check_overlap()
+
+    def check_overlap(self) -> None:
+        """check_overlap (gregsys.hpp:307-342) on the device: raises OverlappingBodiesError for the
+        first overlapping pair, or with merge_overlapping=True merges them (body::operator+=)."""
+        if len(self.m) < 2:
+            return
+        self._push()
+        pair = np.zeros(2, np.int32)
+        check(self._L.gtd_system_check_overlap(self._h, 1 if self.merge else 0, ptr(pair)))
+        if self.merge:
+            self._pull()
 
     # ---- reference accessors / setters (gregsys.hpp:1627-1672) --------------------------------
     def num_bodies(self) -> int:

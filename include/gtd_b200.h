@@ -82,6 +82,15 @@ GTD_API int gtd_system_set_params(gtd_system *sys, double G, double dt, uint64_t
  * gregsys.hpp:135-137): GTD_NO_COLL, GTD_OVERLAP_COLL or GTD_MERGE_COLL. */
 GTD_API int gtd_system_set_collisions(gtd_system *sys, int mode);
 
+/* The add-time overlap check of the system constructors (check_overlap, gregsys.hpp:307-342),
+ * scanning in upload order.  merge == 0: returns GTD_ERR_OVERLAPPING_BODIES naming the first
+ * overlapping pair found (pair[0..1] = their upload indices, pair may be NULL), as the reference
+ * throws overlapping_bodies_error.  merge != 0: merges overlapping bodies with body::operator+=
+ * (gregbod.hpp:1066-1082), re-checking a merged body against every body from index 0 (the
+ * routine's stated intent: after its first merge the reference loop's counter and pointer fall
+ * out of step, gregsys.hpp:329-335, and it then deletes bodies it never merged). */
+GTD_API int gtd_system_check_overlap(gtd_system *sys, int merge, int32_t *pair);
+
 /* Gather: the AoS gtd::body fields (gregbod.hpp:906-916) as SoA.  r, rest, v3 may be NULL
  * (zero radius, restitution 1, zero velocity).  n == 0 is an empty system. */
 GTD_API int gtd_system_upload(gtd_system *sys, int64_t n, const double *m, const double *r, const double *rest,
