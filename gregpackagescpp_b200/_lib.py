@@ -112,6 +112,15 @@ def load():
     L.gtd_system_time_force_kernels.argtypes = [vp, ip]
     L.gtd_system_force_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(u64), ip]
     L.gtd_measure_fma_peak.argtypes = [ip, ip, C.POINTER(C.c_double)]
+    L.gtd_ensemble_create.argtypes = [C.POINTER(vp), ip]
+    L.gtd_ensemble_destroy.argtypes = [vp]
+    L.gtd_ensemble_set_params.argtypes = [vp, C.c_double, C.c_double, ip]
+    L.gtd_ensemble_upload.argtypes = [vp, i64, dp, dp, dp, dp, dp, dp]
+    L.gtd_ensemble_evolve.argtypes = [vp, u64, C.POINTER(i64)]
+    L.gtd_ensemble_counts.argtypes = [vp, dp, C.POINTER(u64), C.POINTER(u64)]
+    L.gtd_ensemble_download.argtypes = [vp, dp, dp, dp, dp, dp, dp]
+    L.gtd_ensemble_set_threads.argtypes = [vp, ip]
+    L.gtd_ensemble_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.gtd_direct_variant_count.argtypes = [ip, C.POINTER(C.c_int)]
     L.gtd_direct_variant_info.argtypes = [ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.gtd_system_set_direct_variant.argtypes = [vp, ip]

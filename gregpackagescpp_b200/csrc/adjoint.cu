@@ -1,0 +1,380 @@
+// Hand-written adjoint of the FP64 leapfrog KDK direct-summation evolve: gradients of a loss on
+// the final state with respect to the initial positions, velocities and masses.  There is no
+// counterpart in the reference; the forward it differentiates is gtd::system::evolve(leapfrog_kdk)
+// (gregsys.hpp:2946-2990, force gregsys.hpp:352-357).
+//
+// Forward, as a sequence of kicks K(c, x): v += c a(x) and drifts D: x += h v:
+//     K(h/2, x0) D K(h, x1) D ... D K(h, x_{T-1}) D K(h/2, xT)
+// (a step's closing half kick and the next step's opening half kick act at the same positions and
+// merge into one full kick).  Reverse sweep from (lx, lv) = (dL/dxT, dL/dvT), mu = 0:
+//     for k = T .. 0:   lx += c_k J(x_k)^T lv ;  mu += c_k (da/dm)^T lv ;  if k > 0: lv += h lx
+// with, for a_i = sum_j G m_j d_ij / r^3 (d_ij = x_j - x_i),
+//     (J^T w)_k = sum_j G [ u / r^3 - 3 d (d . u) / r^5 ],  u = m_k w_j - m_j w_k,  d = x_j - x_k
+//     (dL/dm)_k += sum_j G (w_j . (x_k - x_j)) / r^3.
+// Memory: sqrt(T)-step checkpointing.  The forward keeps (x, v_{k-1/2}, a) every C steps; the
+// reverse sweep recomputes one segment of positions at a time from its checkpoint, then runs the
+// segment's VJPs backwards.  Both the force and the VJP use the stream-K FP64 decomposition of
+// direct.cu (every SM gets the same number of pair tiles whatever N is).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "gtd_internal.cuh"
+
+namespace gtd {
+
+struct VjpArgs {
+    int64_t n, rows, tiles, total;
+    int grid, bi;
+    const double4 *x;   // positions + mass
+    const double4 *w;   // c_k * lambda_v (xyz)
+    double G;
+    double *part;       // 4 doubles per body per slot
+};
+
+constexpr int kVT = 256;
+
+// Partial VJP sums over j-tiles; same (row, tile) stream-K split as the force kernel, I = 1.
+__global__ void __launch_bounds__(kVT) vjp_kernel(VjpArgs a) {
+    __shared__ double4 tx[kVT];
+    __shared__ double4 tw[kVT];
+    const int t = threadIdx.x;
+    int64_t s = (int64_t)blockIdx.x * a.total / a.grid;
+    const int64_t e = (int64_t)(blockIdx.x + 1) * a.total / a.grid;
+    while (s < e) {
+        const int64_t r = s / a.tiles;
+        const int64_t jt0 = s - r * a.tiles;
+        const int64_t row_end = min(e, (r + 1) * a.tiles);
+        const int64_t jt1 = row_end - r * a.tiles;
+        const int64_t k = r * a.bi + t;
+        double4 xk = make_double4(0, 0, 0, 0), wk = xk;
+        if (k < a.n) {
+            xk = a.x[k];
+            wk = a.w[k];
+        }
+        double jx = 0, jy = 0, jz = 0, mu = 0;
+        for (int64_t jt = jt0; jt < jt1; ++jt) {
+            const int64_t j = jt * kVT + t;
+            __syncthreads();
+            tx[t] = j < a.n ? a.x[j] : make_double4(0, 0, 0, 0);
+            tw[t] = j < a.n ? a.w[j] : make_double4(0, 0, 0, 0);
+            __syncthreads();
+#pragma unroll 2
+            for (int jj = 0; jj < kVT; ++jj) {
+                const double4 xj = tx[jj], wj = tw[jj];
+                const double dx = xj.x - xk.x, dy = xj.y - xk.y, dz = xj.z - xk.z;
+                const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+                double inv = rsqrt(r2);
+                inv = r2 > 0.0 ? inv : 0.0;  // j == k and padding contribute nothing
+                const double inv2 = inv * inv, inv3 = inv2 * inv;
+                const double ux = xk.w * wj.x - xj.w * wk.x;
+                const double uy = xk.w * wj.y - xj.w * wk.y;
+                const double uz = xk.w * wj.z - xj.w * wk.z;
+                const double du = fma(dz, uz, fma(dy, uy, dx * ux));
+                const double c5 = 3.0 * du * inv3 * inv2;
+                jx = fma(inv3, ux, fma(-c5, dx, jx));
+                jy = fma(inv3, uy, fma(-c5, dy, jy));
+                jz = fma(inv3, uz, fma(-c5, dz, jz));
+                const double wd = fma(wj.z, dz, fma(wj.y, dy, wj.x * dx));
+                mu = fma(-wd, inv3, mu);
+            }
+        }
+        double *slot = a.part + (size_t)(blockIdx.x + r) * 4 * a.bi;
+        slot[t] = jx;
+        slot[a.bi + t] = jy;
+        slot[2 * a.bi + t] = jz;
+        slot[3 * a.bi + t] = mu;
+        s = row_end;
+    }
+}
+
+// lx += G J^T w ; mu += G (..) ; then (if drift) lv += h lx ; and w for the next VJP
+__global__ void vjp_combine_kernel(int64_t n, int64_t tiles, int64_t total, int grid, int bi, const double *part,
+                                   double G, double4 *lx, double4 *lv, double *mu, double h, int drift) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t r = i / bi;
+    const int l = (int)(i - r * bi);
+    const int64_t g0 = ((r * tiles + 1) * (int64_t)grid - 1) / total;
+    const int64_t g1 = (((r + 1) * tiles) * (int64_t)grid - 1) / total;
+    double jx = 0, jy = 0, jz = 0, m = 0;
+    for (int64_t g = g0; g <= g1; ++g) {
+        const double *slot = part + (size_t)(g + r) * 4 * bi;
+        jx += slot[l];
+        jy += slot[bi + l];
+        jz += slot[2 * bi + l];
+        m += slot[3 * bi + l];
+    }
+    double4 x = lx[i];
+    x.x = fma(G, jx, x.x);
+    x.y = fma(G, jy, x.y);
+    x.z = fma(G, jz, x.z);
+    lx[i] = x;
+    mu[i] = fma(G, m, mu[i]);
+    if (drift) {
+        double4 v = lv[i];
+        v.x = fma(h, x.x, v.x);
+        v.y = fma(h, x.y, v.y);
+        v.z = fma(h, x.z, v.z);
+        lv[i] = v;
+    }
+}
+
+__global__ void scale_kernel(int64_t n, const double4 *lv, double c, double4 *w) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 v = lv[i];
+    w[i] = make_double4(c * v.x, c * v.y, c * v.z, 0.0);
+}
+
+// v += c a ; x += h v   (a kick followed by a drift)
+__global__ void kick_then_drift_kernel(int64_t n, double4 *x, double4 *v, const double4 *a, double c, double h) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 vv = v[i];
+    const double4 aa = a[i];
+    vv.x = fma(c, aa.x, vv.x); vv.y = fma(c, aa.y, vv.y); vv.z = fma(c, aa.z, vv.z);
+    v[i] = vv;
+    double4 xx = x[i];
+    xx.x = fma(h, vv.x, xx.x); xx.y = fma(h, vv.y, xx.y); xx.z = fma(h, vv.z, xx.z);
+    x[i] = xx;
+}
+
+__global__ void kick_kernel(int64_t n, double4 *v, const double4 *a, double c) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 vv = v[i];
+    const double4 aa = a[i];
+    vv.x = fma(c, aa.x, vv.x); vv.y = fma(c, aa.y, vv.y); vv.z = fma(c, aa.z, vv.z);
+    v[i] = vv;
+}
+
+__global__ void pack_kernel(int64_t n, const double *x3, const double *m, const double *v3, double4 *x, double4 *v) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] = make_double4(x3[3 * i], x3[3 * i + 1], x3[3 * i + 2], m[i]);
+    if (v) v[i] = make_double4(v3[3 * i], v3[3 * i + 1], v3[3 * i + 2], 0.0);
+}
+
+__global__ void unpack_kernel(int64_t n, const double4 *a, double *a3) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 q = a[i];
+    a3[3 * i] = q.x;
+    a3[3 * i + 1] = q.y;
+    a3[3 * i + 2] = q.z;
+}
+
+__global__ void copy_triples_kernel(int64_t n, const double *in3, double4 *out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = in3 ? make_double4(in3[3 * i], in3[3 * i + 1], in3[3 * i + 2], 0.0) : make_double4(0, 0, 0, 0);
+}
+
+}  // namespace gtd
+
+using namespace gtd;
+
+struct gtd_adjoint {
+    int device = 0;
+    int64_t n = 0;
+    uint64_t steps = 0, every = 1;
+    double G = 0, h = 0;
+    ForcePlan fplan, vplan;
+    double *fpart = nullptr, *vpart = nullptr;
+    double4 *x = nullptr, *v = nullptr, *a = nullptr;     // working state
+    double4 *ck = nullptr;                                 // checkpoints: (x, v_{k-1/2}, a) * ncheck
+    int64_t ncheck = 0;
+    double4 *seg = nullptr;                                // positions of one segment [(every+1) * n]
+    double4 *lx = nullptr, *lv = nullptr, *w = nullptr;
+    double *mu = nullptr;
+    bool have_forward = false;
+    uint64_t launches = 0;
+};
+
+static unsigned g1(int64_t n) { return (unsigned)((n + 255) / 256); }
+
+static int adj_force(gtd_adjoint *A, const double4 *x, cudaStream_t st) {
+    int rc = launch_force(GTD_PREC_F64, A->fplan, x, A->G, A->fpart, st);
+    if (rc) return rc;
+    StepArgs sa{};
+    sa.n = A->n;
+    sa.src = x;
+    sa.cur = x;
+    sa.acc = A->a;
+    rc = launch_integrate(A->fplan, A->fpart, EPI_ACC, sa, st);
+    A->launches += 2;
+    return rc;
+}
+
+static int adj_vjp(gtd_adjoint *A, const double4 *x, bool drift, cudaStream_t st) {
+    const ForcePlan &p = A->vplan;
+    VjpArgs va{p.n, p.rows, p.tiles, p.total, p.grid, p.bi, x, A->w, A->G, A->vpart};
+    vjp_kernel<<<p.grid, kVT, 0, st>>>(va);
+    GTD_CHECK_LAUNCH();
+    vjp_combine_kernel<<<g1(A->n), 256, 0, st>>>(A->n, p.tiles, p.total, p.grid, p.bi, A->vpart, A->G, A->lx, A->lv,
+                                                 A->mu, A->h, drift ? 1 : 0);
+    GTD_CHECK_LAUNCH();
+    A->launches += 2;
+    return GTD_OK;
+}
+
+extern "C" {
+
+int gtd_adjoint_create(gtd_adjoint **out, int device, int64_t n, uint64_t steps, uint64_t checkpoint_every,
+                       double G, double dt) {
+    if (!out) return fail(GTD_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (n < 2 || steps < 1 || !(dt > 0)) return fail(GTD_ERR_INVALID_ARGUMENT, "need n >= 2, steps >= 1, dt > 0");
+    if (checkpoint_every < 1) checkpoint_every = 1;
+    GTD_CUDA(cudaSetDevice(device));
+    gtd_adjoint *A = new (std::nothrow) gtd_adjoint();
+    if (!A) return fail(GTD_ERR_OUT_OF_MEMORY, "host allocation failed");
+    A->device = device;
+    A->n = n;
+    A->steps = steps;
+    A->every = std::min<uint64_t>(checkpoint_every, steps);
+    A->G = G;
+    A->h = dt;
+    A->fplan = make_plan(n, GTD_PREC_F64, device, 0);
+    // the VJP kernel runs one i-body per thread: a plan with 256-body rows
+    A->vplan = A->fplan;
+    A->vplan.bi = kVT;
+    A->vplan.rows = (n + kVT - 1) / kVT;
+    A->vplan.total = A->vplan.rows * A->vplan.tiles;
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vjp_kernel, kVT, 0);
+    A->vplan.grid = (int)std::min<int64_t>((int64_t)sms * std::max(per_sm, 1), A->vplan.total);
+    A->vplan.slots = A->vplan.grid + A->vplan.rows;
+    A->ncheck = (int64_t)((steps + A->every - 1) / A->every) + 1;
+    const size_t b4 = sizeof(double4) * (size_t)n;
+    cudaError_t e = cudaSuccess;
+    auto M = [&](void **p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
+    M((void **)&A->fpart, partial_bytes(A->fplan));
+    M((void **)&A->vpart, (size_t)A->vplan.slots * 4 * A->vplan.bi * sizeof(double));
+    M((void **)&A->x, b4);
+    M((void **)&A->v, b4);
+    M((void **)&A->a, b4);
+    M((void **)&A->ck, 3 * b4 * (size_t)A->ncheck);
+    M((void **)&A->seg, b4 * (size_t)(A->every + 1));
+    M((void **)&A->lx, b4);
+    M((void **)&A->lv, b4);
+    M((void **)&A->w, b4);
+    M((void **)&A->mu, sizeof(double) * (size_t)n);
+    if (e != cudaSuccess) {
+        int rc = cuda_fail(e, "adjoint buffers", __FILE__, __LINE__);
+        gtd_adjoint_destroy(A);
+        return rc;
+    }
+    *out = A;
+    return GTD_OK;
+}
+
+int gtd_adjoint_destroy(gtd_adjoint *A) {
+    if (!A) return GTD_OK;
+    cudaSetDevice(A->device);
+    cudaFree(A->fpart); cudaFree(A->vpart); cudaFree(A->x); cudaFree(A->v); cudaFree(A->a); cudaFree(A->ck);
+    cudaFree(A->seg); cudaFree(A->lx); cudaFree(A->lv); cudaFree(A->w); cudaFree(A->mu);
+    delete A;
+    return GTD_OK;
+}
+
+// Forward KDK over all steps from device arrays x0/v0 (n x 3) and m (n); writes xT/vT (device, may
+// be NULL) and keeps the checkpoints for gtd_adjoint_backward.  stream: a cudaStream_t or NULL.
+int gtd_adjoint_forward(gtd_adjoint *A, const double *x0, const double *v0, const double *m, double *xT,
+                        double *vT, void *stream) {
+    if (!A || !x0 || !v0 || !m) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaSetDevice(A->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t n = A->n;
+    const size_t b4 = sizeof(double4) * (size_t)n;
+    pack_kernel<<<g1(n), 256, 0, st>>>(n, x0, m, v0, A->x, A->v);
+    GTD_CHECK_LAUNCH();
+    int rc = adj_force(A, A->x, st);
+    if (rc) return rc;
+    const double h = A->h;
+    for (uint64_t k = 0; k < A->steps; ++k) {
+        if (k % A->every == 0) {
+            double4 *c = A->ck + 3 * (size_t)n * (k / A->every);
+            GTD_CUDA(cudaMemcpyAsync(c, A->x, b4, cudaMemcpyDeviceToDevice, st));
+            GTD_CUDA(cudaMemcpyAsync(c + n, A->v, b4, cudaMemcpyDeviceToDevice, st));
+            GTD_CUDA(cudaMemcpyAsync(c + 2 * n, A->a, b4, cudaMemcpyDeviceToDevice, st));
+        }
+        kick_then_drift_kernel<<<g1(n), 256, 0, st>>>(n, A->x, A->v, A->a, k == 0 ? 0.5 * h : h, h);
+        GTD_CHECK_LAUNCH();
+        A->launches += 1;
+        rc = adj_force(A, A->x, st);
+        if (rc) return rc;
+    }
+    kick_kernel<<<g1(n), 256, 0, st>>>(n, A->v, A->a, 0.5 * h);
+    GTD_CHECK_LAUNCH();
+    A->launches += 1;
+    if (xT) unpack_kernel<<<g1(n), 256, 0, st>>>(n, A->x, xT);
+    if (vT) unpack_kernel<<<g1(n), 256, 0, st>>>(n, A->v, vT);
+    GTD_CHECK_LAUNCH();
+    A->have_forward = true;
+    return GTD_OK;
+}
+
+// Reverse sweep: gxT, gvT (device, n x 3, gvT may be NULL) -> gx0, gv0 (n x 3), gm (n).
+int gtd_adjoint_backward(gtd_adjoint *A, const double *gxT, const double *gvT, double *gx0, double *gv0, double *gm,
+                         void *stream) {
+    if (!A || !gxT) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!A->have_forward) return fail(GTD_ERR_INVALID_ARGUMENT, "gtd_adjoint_forward must run first");
+    cudaSetDevice(A->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t n = A->n;
+    const size_t b4 = sizeof(double4) * (size_t)n;
+    const double h = A->h;
+    const uint64_t T = A->steps, C = A->every;
+    copy_triples_kernel<<<g1(n), 256, 0, st>>>(n, gxT, A->lx);
+    copy_triples_kernel<<<g1(n), 256, 0, st>>>(n, gvT, A->lv);
+    GTD_CHECK_LAUNCH();
+    GTD_CUDA(cudaMemsetAsync(A->mu, 0, sizeof(double) * (size_t)n, st));
+    const int64_t nseg = (int64_t)((T + C - 1) / C);
+    for (int64_t sgi = nseg - 1; sgi >= 0; --sgi) {
+        const uint64_t k0 = (uint64_t)sgi * C, k1 = std::min<uint64_t>(k0 + C, T);
+        // recompute positions x_{k0..k1} of this segment from its checkpoint
+        const double4 *c = A->ck + 3 * (size_t)n * (size_t)sgi;
+        GTD_CUDA(cudaMemcpyAsync(A->x, c, b4, cudaMemcpyDeviceToDevice, st));
+        GTD_CUDA(cudaMemcpyAsync(A->v, c + n, b4, cudaMemcpyDeviceToDevice, st));
+        GTD_CUDA(cudaMemcpyAsync(A->a, c + 2 * n, b4, cudaMemcpyDeviceToDevice, st));
+        GTD_CUDA(cudaMemcpyAsync(A->seg, A->x, b4, cudaMemcpyDeviceToDevice, st));
+        for (uint64_t k = k0; k < k1; ++k) {
+            kick_then_drift_kernel<<<g1(n), 256, 0, st>>>(n, A->x, A->v, A->a, k == 0 ? 0.5 * h : h, h);
+            GTD_CHECK_LAUNCH();
+            A->launches += 1;
+            GTD_CUDA(cudaMemcpyAsync(A->seg + (size_t)(k + 1 - k0) * n, A->x, b4, cudaMemcpyDeviceToDevice, st));
+            if (k + 1 < k1) {
+                int rc = adj_force(A, A->x, st);
+                if (rc) return rc;
+            }
+        }
+        // VJPs at x_k, k = k1 .. k0 (k0 only for the first segment's x0 handled when sgi == 0)
+        const uint64_t kstop = sgi == 0 ? k0 : k0 + 1;
+        for (uint64_t k = k1 + 1; k-- > kstop;) {
+            const double ck = (k == 0 || k == T) ? 0.5 * h : h;
+            scale_kernel<<<g1(n), 256, 0, st>>>(n, A->lv, ck, A->w);
+            GTD_CHECK_LAUNCH();
+            A->launches += 1;
+            int rc = adj_vjp(A, A->seg + (size_t)(k - k0) * n, k > 0, st);
+            if (rc) return rc;
+        }
+    }
+    if (gx0) unpack_kernel<<<g1(n), 256, 0, st>>>(n, A->lx, gx0);
+    if (gv0) unpack_kernel<<<g1(n), 256, 0, st>>>(n, A->lv, gv0);
+    if (gm) GTD_CUDA(cudaMemcpyAsync(gm, A->mu, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    GTD_CHECK_LAUNCH();
+    return GTD_OK;
+}
+
+int gtd_adjoint_launch_count(const gtd_adjoint *A, uint64_t *count) {
+    if (!A || !count) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    *count = A->launches;
+    return GTD_OK;
+}
+
+}  // extern "C"

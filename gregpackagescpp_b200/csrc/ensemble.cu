@@ -1,0 +1,624 @@
+// Batched ensemble of independent few-body systems: one persistent launch advances every system
+// by one leapfrog KDK step (gregsys.hpp:2946-2990 per system), the step loop is captured in a CUDA
+// graph, and overlap merges (body::operator+=, the check_overlap scan) run inside the same launch.
+//
+// This is the device form of the reference drivers' ensemble pattern - one gtd::system per
+// std::thread (bdsim.cpp:82-113) - with FP64 state and FP32 pair forces.
+//
+// Work decomposition: one CTA owns one system at a time.  Systems are handed out largest first
+// from an atomic work counter (longest-processing-time order), so the 680x spread in per-system
+// work (N = 3 .. 2048) balances across the persistent grid.  A system's bodies are staged once per
+// step in shared memory as FP32 coordinates relative to the system's mean position, with G m and
+// the radius; each thread owns bodies i = t, t + T, ... and sums its forces two j-bodies per
+// packed FP32x2 instruction, folding every 64 j-bodies into FP64.  Alongside the force it keeps the
+// smallest separation to any other body (integer min on the ALU pipe); a body closer to another
+// than its radius plus the system's largest radius flags the system, and only flagged systems run
+// the exact FP64 merge scan.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "gtd_internal.cuh"
+
+struct gtd_ensemble {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double G = 6.6743e-11, dt = 1.0;
+    int merge = 1;
+    int threads = 256;   // CTA size (autotuned)
+    int blocks_per_sm = 0;
+    int64_t n_sys = 0, n_bodies = 0;
+    int max_n = 0;
+    std::vector<int64_t> off_h;       // [n_sys+1]
+    int64_t *off = nullptr;           // [n_sys+1]
+    int32_t *cnt = nullptr;           // live bodies per system
+    int32_t *order = nullptr;         // systems, largest first
+    double4 *pos = nullptr, *vel = nullptr, *acc = nullptr;
+    double *rad = nullptr, *rest = nullptr;
+    int32_t *ids = nullptr;
+    unsigned *work = nullptr;         // [2]: work counter, merges this launch
+    int *status = nullptr;
+    bool begun = false;
+    uint64_t launches = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    int graph_threads = 0;
+};
+
+namespace gtd {
+
+constexpr int kEnsMaxN = 8192;
+constexpr int kEnsFold = 64;
+
+struct EnsArgs {
+    int n_sys;
+    const int64_t *off;
+    int32_t *cnt;
+    const int32_t *order;
+    double4 *pos, *vel, *acc;
+    double *rad, *rest;
+    int32_t *ids;
+    double G, h;
+    int kdk;     // 0: force only (initial acceleration); 1: kick-drift, force, kick
+    int merge;
+    int stride;  // floats per staged coordinate array (largest system, rounded up to even)
+    unsigned *work;
+    int *status;
+};
+
+__device__ __forceinline__ float ens_rsqrt(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ void ens_merge_into(double4 &po, double4 &vo, double4 &ao, double &ro, double &eo, const double4 &pi,
+                               const double4 &vi, const double4 &ai, double ri, double ei) {
+    const double ma = po.w, mb = pi.w, ms = __dadd_rn(ma, mb);
+    auto mix = [&](double a, double b) { return __ddiv_rn(__dadd_rn(__dmul_rn(ma, a), __dmul_rn(mb, b)), ms); };
+    const double4 np = make_double4(mix(po.x, pi.x), mix(po.y, pi.y), mix(po.z, pi.z), ms);
+    const double4 nv = make_double4(mix(vo.x, vi.x), mix(vo.y, vi.y), mix(vo.z, vi.z), 0.0);
+    const double4 na = make_double4(mix(ao.x, ai.x), mix(ao.y, ai.y), mix(ao.z, ai.z), 0.0);
+    eo = 0.5 * (eo + ei);
+    ro = cbrt(__dadd_rn(__dmul_rn(__dmul_rn(ro, ro), ro), __dmul_rn(__dmul_rn(ri, ri), ri)));
+    po = np;
+    vo = nv;
+    ao = na;
+}
+
+__device__ __forceinline__ bool ens_overlaps(const double4 &a, double ra, const double4 &b, double rb) {
+    const double dx = __dsub_rn(b.x, a.x), dy = __dsub_rn(b.y, a.y), dz = __dsub_rn(b.z, a.z);
+    const double d = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    return d < __dadd_rn(ra, rb);
+}
+
+// The check_overlap scan (merges, restart from index 0 after each) over one system, by one CTA.
+__device__ int ens_merge_scan(int n, double4 *pos, double4 *vel, double4 *acc, double *rad, double *rest,
+                              int32_t *ids, int *sh) {
+    // sh[0] = best, sh[1] = num, sh[2] = o
+    const int t = threadIdx.x, T = blockDim.x;
+    if (t == 0) {
+        sh[1] = n;
+        sh[2] = 0;
+    }
+    __syncthreads();
+    bool restarted = false;
+    while (true) {
+        const int num = sh[1], o = sh[2];
+        if (o >= num) break;
+        const int lo = restarted ? 0 : o + 1;
+        if (t == 0) sh[0] = INT32_MAX;
+        __syncthreads();
+        const double4 po = pos[o];
+        const double ro = rad[o];
+        for (int i = lo + t; i < num; i += T)
+            if (i != o && ens_overlaps(po, ro, pos[i], rad[i])) atomicMin(&sh[0], i);
+        __syncthreads();
+        const int i = sh[0];
+        if (i == INT32_MAX) {
+            if (t == 0) sh[2] = o + 1;
+            restarted = false;
+            __syncthreads();
+            continue;
+        }
+        if (t == 0) {
+            double4 p = pos[o], v = vel[o], a = acc[o];
+            double r = rad[o], e = rest[o];
+            ens_merge_into(p, v, a, r, e, pos[i], vel[i], acc[i], rad[i], rest[i]);
+            pos[o] = p; vel[o] = v; acc[o] = a; rad[o] = r; rest[o] = e;
+        }
+        __syncthreads();
+        for (int base = i; base < num - 1; base += T) {
+            const int k = base + t;
+            const bool act = k < num - 1;
+            double4 p, v, a;
+            double r = 0, e = 0;
+            int32_t id = 0;
+            if (act) { p = pos[k + 1]; v = vel[k + 1]; a = acc[k + 1]; r = rad[k + 1]; e = rest[k + 1]; id = ids[k + 1]; }
+            __syncthreads();
+            if (act) { pos[k] = p; vel[k] = v; acc[k] = a; rad[k] = r; rest[k] = e; ids[k] = id; }
+            __syncthreads();
+        }
+        if (t == 0) {
+            sh[1] = num - 1;
+            sh[2] = i < o ? o - 1 : o;
+        }
+        restarted = true;
+        __syncthreads();
+    }
+    const int out = sh[1];
+    __syncthreads();
+    return out;
+}
+
+// One launch = one KDK step (or the initial force) for every system.
+__global__ void __launch_bounds__(512) ensemble_step_kernel(EnsArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *sx = reinterpret_cast<float *>(smem_raw);
+    float *sy = sx + a.stride;
+    float *sz = sy + a.stride;
+    float *sm = sz + a.stride;
+    __shared__ double red[3][32];
+    __shared__ double cen[3];
+    __shared__ float redr[32];
+    __shared__ int sh[8];
+    __shared__ float rmax_s;
+    const int t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5, nw = (T + 31) >> 5;
+    const double h = a.h, h2 = 0.5 * a.h;
+    while (true) {
+        if (t == 0) sh[3] = (int)atomicAdd(&a.work[0], 1u);
+        __syncthreads();
+        const int item = sh[3];
+        __syncthreads();
+        if (item >= a.n_sys) break;
+        const int s = a.order[item];
+        const int64_t b0 = a.off[s];
+        const int n = a.cnt[s];
+        double4 *pos = a.pos + b0, *vel = a.vel + b0, *acc = a.acc + b0;
+        double *rad = a.rad + b0;
+        // pass 0: kick-drift, force, kick, merge check; pass 1 (only after merges): the force at the
+        // merged state, so the next step's first half kick uses a(x) of the bodies that remain
+        int nc = n;
+        for (int pass = 0; pass < 2; ++pass) {
+            const bool first = pass == 0;
+            double cx = 0.0, cy = 0.0, cz = 0.0;
+            float rmax = 0.f;
+            for (int i = t; i < nc; i += T) {
+                double4 p = pos[i];
+                if (a.kdk && first) {
+                    double4 v = vel[i];
+                    const double4 ac = acc[i];
+                    v.x = fma(h2, ac.x, v.x); v.y = fma(h2, ac.y, v.y); v.z = fma(h2, ac.z, v.z);
+                    p.x = fma(h, v.x, p.x); p.y = fma(h, v.y, p.y); p.z = fma(h, v.z, p.z);
+                    vel[i] = v;
+                    pos[i] = p;
+                }
+                cx += p.x; cy += p.y; cz += p.z;
+                rmax = fmaxf(rmax, (float)rad[i]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                cx += __shfl_xor_sync(0xffffffffu, cx, o);
+                cy += __shfl_xor_sync(0xffffffffu, cy, o);
+                cz += __shfl_xor_sync(0xffffffffu, cz, o);
+                rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+            }
+            if (lane == 0) {
+                red[0][warp] = cx; red[1][warp] = cy; red[2][warp] = cz;
+                redr[warp] = rmax;
+            }
+            __syncthreads();
+            if (t == 0) {
+                double X = 0, Y = 0, Z = 0;
+                float R = 0.f;
+                for (int w = 0; w < nw; ++w) { X += red[0][w]; Y += red[1][w]; Z += red[2][w]; R = fmaxf(R, redr[w]); }
+                cen[0] = X / nc; cen[1] = Y / nc; cen[2] = Z / nc;
+                rmax_s = R;
+            }
+            __syncthreads();
+            const double mx = cen[0], my = cen[1], mz = cen[2];
+            const float rmx = rmax_s;
+            // stage the system: FP32 relative positions and G m (pad to an even count, far and massless)
+            const int npad = (nc + 1) & ~1;
+            for (int i = t; i < npad; i += T) {
+                if (i < nc) {
+                    const double4 p = pos[i];
+                    sx[i] = (float)(p.x - mx); sy[i] = (float)(p.y - my); sz[i] = (float)(p.z - mz);
+                    sm[i] = (float)(a.G * p.w);
+                } else {
+                    sx[i] = 1e30f; sy[i] = 1e30f; sz[i] = 1e30f; sm[i] = 0.f;
+                }
+            }
+            __syncthreads();
+            const float2 *X2 = reinterpret_cast<const float2 *>(sx);
+            const float2 *Y2 = reinterpret_cast<const float2 *>(sy);
+            const float2 *Z2 = reinterpret_cast<const float2 *>(sz);
+            const float2 *M2 = reinterpret_cast<const float2 *>(sm);
+            int flagged = 0;
+            for (int i = t; i < nc; i += T) {
+                const float xi = sx[i], yi = sy[i], zi = sz[i];
+                const float2 nx = make_float2(-xi, -xi), ny = make_float2(-yi, -yi), nz = make_float2(-zi, -zi);
+                double ax = 0.0, ay = 0.0, az = 0.0;
+                unsigned mnr = 0xffffffffu;  // min over j != i of r2 bits, the self pair (r2 = 0) excluded
+                for (int q0 = 0; q0 < npad / 2; q0 += kEnsFold / 2) {
+                    const int q1 = min(q0 + kEnsFold / 2, npad / 2);
+                    float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
+#pragma unroll 4
+                    for (int q = q0; q < q1; ++q) {
+                        const float2 dx = __fadd2_rn(X2[q], nx), dy = __fadd2_rn(Y2[q], ny), dz = __fadd2_rn(Z2[q], nz);
+                        float2 r2 = __fmul2_rn(dx, dx);
+                        r2 = __ffma2_rn(dy, dy, r2);
+                        r2 = __ffma2_rn(dz, dz, r2);
+                        mnr = min(mnr, (unsigned)__float_as_int(r2.x) - 1u);
+                        mnr = min(mnr, (unsigned)__float_as_int(r2.y) - 1u);
+                        // the self pair has r2 == 0: clamping to 1 mm^2 makes its term exactly 0
+                        const float2 inv = make_float2(ens_rsqrt(fmaxf(r2.x, 1e-6f)), ens_rsqrt(fmaxf(r2.y, 1e-6f)));
+                        const float2 inv2 = __fmul2_rn(inv, inv);
+                        float2 sc = __fmul2_rn(M2[q], inv);
+                        sc = __fmul2_rn(sc, inv2);
+                        fx = __ffma2_rn(dx, sc, fx);
+                        fy = __ffma2_rn(dy, sc, fy);
+                        fz = __ffma2_rn(dz, sc, fz);
+                    }
+                    ax += (double)fx.x + (double)fx.y;
+                    ay += (double)fy.x + (double)fy.y;
+                    az += (double)fz.x + (double)fz.y;
+                }
+                if (mnr != 0xffffffffu) {  // some other body exists
+                    const float mind2 = __int_as_float((int)(mnr + 1u));
+                    const float reach = (float)rad[i] + rmx;
+                    if (mind2 < reach * reach * 1.0001f) flagged = 1;
+                }
+                if (a.kdk && first) {
+                    double4 v = vel[i];
+                    v.x = fma(h2, ax, v.x); v.y = fma(h2, ay, v.y); v.z = fma(h2, az, v.z);
+                    vel[i] = v;
+                }
+                acc[i] = make_double4(ax, ay, az, 0.0);
+            }
+            flagged = __syncthreads_or(flagged);
+            if (!first || !flagged || !a.merge) break;
+            const int nn = ens_merge_scan(nc, pos, vel, acc, rad, a.rest + b0, a.ids + b0, sh);
+            if (nn == nc) break;
+            if (t == 0) {
+                a.cnt[s] = nn;
+                atomicAdd(&a.work[1], (unsigned)(nc - nn));
+            }
+            nc = nn;
+            __syncthreads();
+        }
+        __syncthreads();
+    }
+}
+
+int ens_stride(int max_n) { return std::max(2, (max_n + 1) & ~1); }
+int ens_smem_bytes(int max_n) { return 4 * ens_stride(max_n) * (int)sizeof(float); }
+
+}  // namespace gtd
+
+using namespace gtd;
+
+static void ens_release(gtd_ensemble *e) {
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+    cudaFree(e->off); cudaFree(e->cnt); cudaFree(e->order); cudaFree(e->pos); cudaFree(e->vel); cudaFree(e->acc);
+    cudaFree(e->rad); cudaFree(e->rest); cudaFree(e->ids); cudaFree(e->work); cudaFree(e->status);
+    e->off = nullptr; e->cnt = nullptr; e->order = nullptr; e->pos = e->vel = e->acc = nullptr;
+    e->rad = e->rest = nullptr; e->ids = nullptr; e->work = nullptr; e->status = nullptr;
+}
+
+static int ens_launch(gtd_ensemble *e, int kdk) {
+    EnsArgs a{(int)e->n_sys, e->off, e->cnt, e->order, e->pos, e->vel, e->acc, e->rad, e->rest, e->ids,
+              e->G, e->dt, kdk, e->merge, ens_stride(e->max_n), e->work, e->status};
+    const int smem = ens_smem_bytes(e->max_n);
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e->device);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_step_kernel, e->threads, smem);
+    if (per_sm < 1) per_sm = 1;
+    const int grid = (int)std::min<int64_t>((int64_t)dev_sms * per_sm, std::max<int64_t>(e->n_sys, 1));
+    GTD_CUDA(cudaMemsetAsync(e->work, 0, sizeof(unsigned), e->stream));
+    ensemble_step_kernel<<<grid, e->threads, smem, e->stream>>>(a);
+    GTD_CHECK_LAUNCH();
+    e->launches += 1;
+    return GTD_OK;
+}
+
+// Captures `steps` KDK steps (a memset and one persistent launch each) into a CUDA graph.
+static int ens_build_graph(gtd_ensemble *e, int steps) {
+    if (e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    cudaGraph_t g;
+    GTD_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = GTD_OK;
+    const uint64_t before = e->launches;
+    for (int k = 0; k < steps && !rc; ++k) rc = ens_launch(e, 1);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    e->launches = before;  // captured, not launched
+    if (rc) return rc;
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+    ce = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate", __FILE__, __LINE__);
+    e->graph_steps = steps;
+    e->graph_threads = e->threads;
+    return GTD_OK;
+}
+
+static int ens_steps(gtd_ensemble *e, uint64_t steps) {
+    if (!e->begun) {
+        int rc = ens_launch(e, 0);  // initial accelerations (and add-time merges)
+        if (rc) return rc;
+        e->begun = true;
+    }
+    const int chunk = 16;
+    if (steps >= (uint64_t)chunk) {
+        if (!e->graph || e->graph_steps != chunk || e->graph_threads != e->threads) {
+            int rc = ens_build_graph(e, chunk);
+            if (rc) return rc;
+        }
+        while (steps >= (uint64_t)chunk) {
+            GTD_CUDA(cudaGraphLaunch(e->graph, e->stream));
+            e->launches += chunk;
+            steps -= chunk;
+        }
+    }
+    for (uint64_t k = 0; k < steps; ++k) {
+        int rc = ens_launch(e, 1);
+        if (rc) return rc;
+    }
+    return GTD_OK;
+}
+
+extern "C" {
+
+int gtd_ensemble_create(gtd_ensemble **out, int device) {
+    if (!out) return fail(GTD_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int nd = 0;
+    if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0) {
+        cudaGetLastError();
+        return fail(GTD_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= nd) return fail(GTD_ERR_INVALID_ARGUMENT, "device %d out of range", device);
+    GTD_CUDA(cudaSetDevice(device));
+    gtd_ensemble *e = new (std::nothrow) gtd_ensemble();
+    if (!e) return fail(GTD_ERR_OUT_OF_MEMORY, "host allocation failed");
+    e->device = device;
+    GTD_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    GTD_CUDA(cudaEventCreate(&e->ev0));
+    GTD_CUDA(cudaEventCreate(&e->ev1));
+    GTD_CUDA(cudaFuncSetAttribute(ensemble_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  ens_smem_bytes(kEnsMaxN)));
+    *out = e;
+    return GTD_OK;
+}
+
+int gtd_ensemble_destroy(gtd_ensemble *e) {
+    if (!e) return GTD_OK;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    ens_release(e);
+    cudaEventDestroy(e->ev0);
+    cudaEventDestroy(e->ev1);
+    cudaStreamDestroy(e->stream);
+    delete e;
+    return GTD_OK;
+}
+
+int gtd_ensemble_set_params(gtd_ensemble *e, double G, double dt, int merge) {
+    if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
+    if (!(dt > 0)) return fail(GTD_ERR_INVALID_ARGUMENT, "Time-step cannot be zero or negative.");
+    e->G = G;
+    e->dt = dt;
+    e->merge = merge ? 1 : 0;
+    if (e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    return GTD_OK;
+}
+
+int gtd_ensemble_upload(gtd_ensemble *e, int64_t n_systems, const int64_t *offsets, const double *m,
+                        const double *r, const double *rest, const double *x3, const double *v3) {
+    if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
+    if (n_systems < 0 || (n_systems > 0 && (!offsets || !m || !x3)))
+        return fail(GTD_ERR_INVALID_ARGUMENT, "bad ensemble description");
+    cudaSetDevice(e->device);
+    ens_release(e);
+    e->n_sys = n_systems;
+    e->off_h.assign(offsets, offsets + n_systems + 1);
+    const int64_t nb = n_systems ? offsets[n_systems] : 0;
+    e->n_bodies = nb;
+    e->max_n = 0;
+    std::vector<int32_t> cnt((size_t)n_systems), order((size_t)n_systems);
+    for (int64_t s = 0; s < n_systems; ++s) {
+        const int64_t k = offsets[s + 1] - offsets[s];
+        if (k < 0 || offsets[s] < 0) return fail(GTD_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing from 0");
+        if (k > kEnsMaxN) return fail(GTD_ERR_CAPACITY, "system %lld has %lld bodies; the ensemble kernel holds %d",
+                                      (long long)s, (long long)k, kEnsMaxN);
+        cnt[(size_t)s] = (int32_t)k;
+        e->max_n = std::max(e->max_n, (int)k);
+    }
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return cnt[a] > cnt[b]; });
+    std::vector<double4> hp((size_t)nb), hv((size_t)nb);
+    std::vector<double> hr((size_t)nb), he((size_t)nb);
+    std::vector<int32_t> hid((size_t)nb);
+    for (int64_t s = 0; s < n_systems; ++s)
+        for (int64_t i = offsets[s]; i < offsets[s + 1]; ++i) {
+            if (m[i] < 0) return fail(GTD_ERR_INVALID_ARGUMENT, "negative mass at body %lld", (long long)i);
+            hp[(size_t)i] = make_double4(x3[3 * i], x3[3 * i + 1], x3[3 * i + 2], m[i]);
+            hv[(size_t)i] = v3 ? make_double4(v3[3 * i], v3[3 * i + 1], v3[3 * i + 2], 0.0) : make_double4(0, 0, 0, 0);
+            hr[(size_t)i] = r ? r[i] : 0.0;
+            he[(size_t)i] = rest ? rest[i] : 1.0;
+            hid[(size_t)i] = (int32_t)(i - offsets[s]);
+        }
+    const size_t b4 = sizeof(double4) * (size_t)std::max<int64_t>(nb, 1);
+    GTD_CUDA(cudaMalloc(&e->off, sizeof(int64_t) * (size_t)(n_systems + 1)));
+    GTD_CUDA(cudaMalloc(&e->cnt, sizeof(int32_t) * (size_t)std::max<int64_t>(n_systems, 1)));
+    GTD_CUDA(cudaMalloc(&e->order, sizeof(int32_t) * (size_t)std::max<int64_t>(n_systems, 1)));
+    GTD_CUDA(cudaMalloc(&e->pos, b4));
+    GTD_CUDA(cudaMalloc(&e->vel, b4));
+    GTD_CUDA(cudaMalloc(&e->acc, b4));
+    GTD_CUDA(cudaMalloc(&e->rad, sizeof(double) * (size_t)std::max<int64_t>(nb, 1)));
+    GTD_CUDA(cudaMalloc(&e->rest, sizeof(double) * (size_t)std::max<int64_t>(nb, 1)));
+    GTD_CUDA(cudaMalloc(&e->ids, sizeof(int32_t) * (size_t)std::max<int64_t>(nb, 1)));
+    GTD_CUDA(cudaMalloc(&e->work, 4 * sizeof(unsigned)));
+    GTD_CUDA(cudaMalloc(&e->status, sizeof(int)));
+    GTD_CUDA(cudaMemcpy(e->off, offsets, sizeof(int64_t) * (size_t)(n_systems + 1), cudaMemcpyHostToDevice));
+    if (n_systems) {
+        GTD_CUDA(cudaMemcpy(e->cnt, cnt.data(), sizeof(int32_t) * cnt.size(), cudaMemcpyHostToDevice));
+        GTD_CUDA(cudaMemcpy(e->order, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice));
+    }
+    if (nb) {
+        GTD_CUDA(cudaMemcpy(e->pos, hp.data(), b4, cudaMemcpyHostToDevice));
+        GTD_CUDA(cudaMemcpy(e->vel, hv.data(), b4, cudaMemcpyHostToDevice));
+        GTD_CUDA(cudaMemset(e->acc, 0, b4));
+        GTD_CUDA(cudaMemcpy(e->rad, hr.data(), sizeof(double) * (size_t)nb, cudaMemcpyHostToDevice));
+        GTD_CUDA(cudaMemcpy(e->rest, he.data(), sizeof(double) * (size_t)nb, cudaMemcpyHostToDevice));
+        GTD_CUDA(cudaMemcpy(e->ids, hid.data(), sizeof(int32_t) * (size_t)nb, cudaMemcpyHostToDevice));
+    }
+    GTD_CUDA(cudaMemset(e->work, 0, 4 * sizeof(unsigned)));
+    GTD_CUDA(cudaMemset(e->status, 0, sizeof(int)));
+    e->begun = false;
+    return GTD_OK;
+}
+
+int gtd_ensemble_evolve(gtd_ensemble *e, uint64_t steps, int64_t *elapsed_ns) {
+    if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
+    if (elapsed_ns) *elapsed_ns = 0;
+    if (e->n_sys == 0 || steps == 0) return GTD_OK;
+    cudaSetDevice(e->device);
+    GTD_CUDA(cudaEventRecord(e->ev0, e->stream));
+    int rc = ens_steps(e, steps);
+    if (rc) return rc;
+    GTD_CUDA(cudaEventRecord(e->ev1, e->stream));
+    GTD_CUDA(cudaEventSynchronize(e->ev1));
+    float ms = 0.f;
+    GTD_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    if (elapsed_ns) *elapsed_ns = (int64_t)((double)ms * 1e6);
+    return GTD_OK;
+}
+
+int gtd_ensemble_counts(gtd_ensemble *e, int64_t *counts, uint64_t *merges, uint64_t *launches) {
+    if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
+    cudaSetDevice(e->device);
+    GTD_CUDA(cudaStreamSynchronize(e->stream));
+    if (counts && e->n_sys) {
+        std::vector<int32_t> c((size_t)e->n_sys);
+        GTD_CUDA(cudaMemcpy(c.data(), e->cnt, sizeof(int32_t) * c.size(), cudaMemcpyDeviceToHost));
+        for (int64_t s = 0; s < e->n_sys; ++s) counts[s] = c[(size_t)s];
+    }
+    if (merges) {
+        unsigned w[2] = {0, 0};
+        GTD_CUDA(cudaMemcpy(w, e->work, sizeof(w), cudaMemcpyDeviceToHost));
+        *merges = w[1];
+    }
+    if (launches) *launches = e->launches;
+    return GTD_OK;
+}
+
+int gtd_ensemble_download(gtd_ensemble *e, double *m, double *r, double *rest, double *x3, double *v3,
+                          double *a3) {
+    if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
+    cudaSetDevice(e->device);
+    GTD_CUDA(cudaStreamSynchronize(e->stream));
+    const int64_t nb = e->n_bodies;
+    if (!nb) return GTD_OK;
+    std::vector<double4> hp((size_t)nb), hv((size_t)nb), ha((size_t)nb);
+    std::vector<double> hr((size_t)nb), he((size_t)nb);
+    GTD_CUDA(cudaMemcpy(hp.data(), e->pos, sizeof(double4) * (size_t)nb, cudaMemcpyDeviceToHost));
+    GTD_CUDA(cudaMemcpy(hv.data(), e->vel, sizeof(double4) * (size_t)nb, cudaMemcpyDeviceToHost));
+    GTD_CUDA(cudaMemcpy(ha.data(), e->acc, sizeof(double4) * (size_t)nb, cudaMemcpyDeviceToHost));
+    GTD_CUDA(cudaMemcpy(hr.data(), e->rad, sizeof(double) * (size_t)nb, cudaMemcpyDeviceToHost));
+    GTD_CUDA(cudaMemcpy(he.data(), e->rest, sizeof(double) * (size_t)nb, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nb; ++i) {
+        if (m) m[i] = hp[(size_t)i].w;
+        if (x3) { x3[3 * i] = hp[(size_t)i].x; x3[3 * i + 1] = hp[(size_t)i].y; x3[3 * i + 2] = hp[(size_t)i].z; }
+        if (v3) { v3[3 * i] = hv[(size_t)i].x; v3[3 * i + 1] = hv[(size_t)i].y; v3[3 * i + 2] = hv[(size_t)i].z; }
+        if (a3) { a3[3 * i] = ha[(size_t)i].x; a3[3 * i + 1] = ha[(size_t)i].y; a3[3 * i + 2] = ha[(size_t)i].z; }
+        if (r) r[i] = hr[(size_t)i];
+        if (rest) rest[i] = he[(size_t)i];
+    }
+    return GTD_OK;
+}
+
+int gtd_ensemble_set_threads(gtd_ensemble *e, int threads) {
+    if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
+    if (threads != 64 && threads != 128 && threads != 256 && threads != 512)
+        return fail(GTD_ERR_INVALID_ARGUMENT, "threads must be 64, 128, 256 or 512");
+    e->threads = threads;
+    return GTD_OK;
+}
+
+// Times one step for each CTA size on a copy of the current state (restored afterwards) and keeps
+// the fastest: the project's tile autotuner for the ensemble.
+int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
+    if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
+    if (e->n_sys == 0) return fail(GTD_ERR_INVALID_ARGUMENT, "autotune needs systems");
+    cudaSetDevice(e->device);
+    const int64_t nb = e->n_bodies;
+    const size_t b4 = sizeof(double4) * (size_t)nb;
+    double4 *sp, *sv, *sa;
+    double *sr, *se;
+    int32_t *si, *sc;
+    GTD_CUDA(cudaMalloc(&sp, b4)); GTD_CUDA(cudaMalloc(&sv, b4)); GTD_CUDA(cudaMalloc(&sa, b4));
+    GTD_CUDA(cudaMalloc(&sr, 8 * (size_t)nb)); GTD_CUDA(cudaMalloc(&se, 8 * (size_t)nb));
+    GTD_CUDA(cudaMalloc(&si, 4 * (size_t)nb)); GTD_CUDA(cudaMalloc(&sc, 4 * (size_t)e->n_sys));
+    auto save = [&](bool back) -> int {
+        auto cp = [&](void *dst, void *src, size_t bytes) { return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, e->stream); };
+        cudaError_t c = cudaSuccess;
+        if (!back) {
+            c = cp(sp, e->pos, b4); if (!c) c = cp(sv, e->vel, b4); if (!c) c = cp(sa, e->acc, b4);
+            if (!c) c = cp(sr, e->rad, 8 * nb); if (!c) c = cp(se, e->rest, 8 * nb); if (!c) c = cp(si, e->ids, 4 * nb);
+            if (!c) c = cp(sc, e->cnt, 4 * e->n_sys);
+        } else {
+            c = cp(e->pos, sp, b4); if (!c) c = cp(e->vel, sv, b4); if (!c) c = cp(e->acc, sa, b4);
+            if (!c) c = cp(e->rad, sr, 8 * nb); if (!c) c = cp(e->rest, se, 8 * nb); if (!c) c = cp(e->ids, si, 4 * nb);
+            if (!c) c = cp(e->cnt, sc, 4 * e->n_sys);
+        }
+        return c == cudaSuccess ? GTD_OK : cuda_fail(c, "autotune state copy", __FILE__, __LINE__);
+    };
+    int rc = save(false);
+    const bool was_begun = e->begun;
+    const int cands[] = {128, 256, 512};
+    int best = e->threads;
+    double bestv = 1e300;
+    for (int c : cands) {
+        if (rc) break;
+        e->threads = c;
+        for (int rep = 0; rep < 3 && !rc; ++rep) {
+            if ((rc = cudaEventRecord(e->ev0, e->stream) ? GTD_ERR_CUDA : GTD_OK)) break;
+            rc = ens_launch(e, 1);
+            if (rc) break;
+            cudaEventRecord(e->ev1, e->stream);
+            cudaEventSynchronize(e->ev1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+            if (rep > 0 && ms < bestv) {
+                bestv = ms;
+                best = c;
+            }
+            if (!rc) rc = save(true);
+        }
+    }
+    e->threads = best;
+    e->begun = was_begun;
+    cudaStreamSynchronize(e->stream);
+    cudaFree(sp); cudaFree(sv); cudaFree(sa); cudaFree(sr); cudaFree(se); cudaFree(si); cudaFree(sc);
+    if (rc) return rc;
+    GTD_CUDA(cudaMemset(e->work, 0, 4 * sizeof(unsigned)));
+    if (best_threads) *best_threads = best;
+    if (best_ms) *best_ms = bestv;
+    return GTD_OK;
+}
+
+}  // extern "C"

@@ -167,6 +167,51 @@ GTD_API int gtd_bh_tree_download(gtd_system *sys, uint64_t *codes, int32_t *perm
  * last gtd_bh_build.  n_inter (per body, optional) counts accepted cells and leaves. */
 GTD_API int gtd_bh_accelerations(gtd_system *sys, double *a3, uint32_t *n_inter);
 
+/* ---- batched ensemble of independent systems ------------------------------------------------
+ * Replaces the drivers' pattern of one gtd::system per std::thread (bdsim.cpp:82-113): every
+ * system advances by leapfrog KDK (gregsys.hpp:2946-2990) with FP64 state and FP32 pair forces,
+ * one persistent launch per step for all systems, the step loop replayed as a CUDA graph, and
+ * overlap merges with body::operator+= in check_overlap's scan order (gregsys.hpp:307-342). */
+typedef struct gtd_ensemble gtd_ensemble;
+
+GTD_API int gtd_ensemble_create(gtd_ensemble **out, int device);
+GTD_API int gtd_ensemble_destroy(gtd_ensemble *ens);
+/* G, dt (as gtd_system_set_params) and merge != 0 to merge overlapping bodies after each step. */
+GTD_API int gtd_ensemble_set_params(gtd_ensemble *ens, double G, double dt, int merge);
+/* System s owns bodies [offsets[s], offsets[s+1]) (at most 8192 per system); r, rest, v3 may be
+ * NULL.  The first evolve computes the initial accelerations (and add-time merges). */
+GTD_API int gtd_ensemble_upload(gtd_ensemble *ens, int64_t n_systems, const int64_t *offsets, const double *m,
+                                const double *r, const double *rest, const double *x3, const double *v3);
+/* Advances every system `steps` KDK steps; *elapsed_ns is the device time (CUDA events). */
+GTD_API int gtd_ensemble_evolve(gtd_ensemble *ens, uint64_t steps, int64_t *elapsed_ns);
+/* Live bodies per system (counts[n_systems]), merges so far, kernel launches so far. */
+GTD_API int gtd_ensemble_counts(gtd_ensemble *ens, int64_t *counts, uint64_t *merges, uint64_t *launches);
+/* State at the upload offsets: system s's survivors occupy the first counts[s] rows of its range,
+ * in upload order. */
+GTD_API int gtd_ensemble_download(gtd_ensemble *ens, double *m, double *r, double *rest, double *x3, double *v3,
+                                  double *a3);
+/* CTA size of the step kernel (64, 128, 256 or 512), or let the autotuner time 128/256/512 on the
+ * current state (restored afterwards) and keep the fastest. */
+GTD_API int gtd_ensemble_set_threads(gtd_ensemble *ens, int threads);
+GTD_API int gtd_ensemble_autotune(gtd_ensemble *ens, int *best_threads, double *best_ms);
+
+/* ---- adjoint of the FP64 leapfrog KDK evolve (no counterpart in the reference) ---------------
+ * Gradients of a loss on the final state of evolve(leapfrog_kdk) (gregsys.hpp:2946-2990) with
+ * respect to the initial positions, velocities and masses, by a hand-written reverse sweep with
+ * checkpoints every `checkpoint_every` steps and recomputation in between.  All arrays are DEVICE
+ * pointers (n x 3 or n doubles, row-major); `stream` is a cudaStream_t or NULL. */
+typedef struct gtd_adjoint gtd_adjoint;
+
+GTD_API int gtd_adjoint_create(gtd_adjoint **out, int device, int64_t n, uint64_t steps, uint64_t checkpoint_every,
+                               double G, double dt);
+GTD_API int gtd_adjoint_destroy(gtd_adjoint *adj);
+GTD_API int gtd_adjoint_forward(gtd_adjoint *adj, const double *x0, const double *v0, const double *m, double *xT,
+                                double *vT, void *stream);
+/* gxT = dL/dx_T (required), gvT = dL/dv_T (may be NULL) -> gx0, gv0, gm (any may be NULL). */
+GTD_API int gtd_adjoint_backward(gtd_adjoint *adj, const double *gxT, const double *gvT, double *gx0, double *gv0,
+                                 double *gm, void *stream);
+GTD_API int gtd_adjoint_launch_count(const gtd_adjoint *adj, uint64_t *count);
+
 #ifdef __cplusplus
 }
 #endif

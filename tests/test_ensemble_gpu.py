@@ -1,0 +1,99 @@
+"""Batched ensemble (one persistent launch per step for all systems) against the oracle run
+system by system: leapfrog KDK from the reference's evolve (gregsys.hpp:2946-2990) and, with
+merging, the check_overlap scan with body::operator+= after every step."""
+import numpy as np
+import pytest
+
+from gregpackagescpp_b200.ensemble import Ensemble
+from gregpackagescpp_b200.ics import AU, ensemble
+
+pytestmark = pytest.mark.gpu
+G = 6.674e-11
+DT = 600.0
+
+
+def oracle_run(oracle, m, r, rest, x, v, steps, merge):
+    """KDK one step at a time (evolve recomputes a(x), equal to the carried one), merging after each."""
+    Gl = oracle.G("M66743:66740,D1:1,T1:1")
+    a = np.zeros_like(x)
+    for _ in range(steps):
+        x, v, a = oracle.evolve(16, m, x, v, DT, 1, Gl)
+        if merge:
+            rows = np.concatenate([m[:, None], r[:, None], rest[:, None], x, v, a], axis=1)
+            rows = oracle.merge_overlapping(rows)
+            m, r, rest = rows[:, 0].copy(), rows[:, 1].copy(), rows[:, 2].copy()
+            x, v, a = rows[:, 3:6].copy(), rows[:, 6:9].copy(), rows[:, 9:12].copy()
+    return m, r, x, v
+
+
+def test_kdk_no_merge_vs_oracle(gpu, oracle):
+    off, m, r, x, v = ensemble(24, 71, n_min=3, n_max=300)
+    e = Ensemble(off, m, x, v, r, merge=False, dt=DT)
+    e.evolve(20)
+    st = e.state()
+    for s in range(24):
+        b, k = off[s], off[s + 1]
+        mo, ro, xo, vo = oracle_run(oracle, m[b:k], r[b:k], np.ones(k - b), x[b:k], v[b:k], 20, False)
+        assert np.abs(st[s]["x"] - xo).max() / np.abs(xo).max() < 1e-11
+        assert np.abs(st[s]["v"] - vo).max() / np.abs(vo).max() < 1e-7
+
+
+def test_merges_vs_oracle(gpu, oracle):
+    off, m, r, x, v = ensemble(12, 72, n_min=3, n_max=200, r_ball=0.2 * AU)
+    r = r * 30.0  # inflate radii so that merges happen within a few steps
+    rest = np.random.default_rng(3).uniform(0, 1, len(m))
+    e = Ensemble(off, m, x, v, r, rest, merge=True, dt=DT)
+    e.evolve(6)
+    st = e.state()
+    counts, merges, _ = e.counts()
+    assert merges > 0
+    for s in range(12):
+        b, k = off[s], off[s + 1]
+        # the ensemble merges at upload (add-time check) too: merge the initial state first
+        rows = np.concatenate([m[b:k, None], r[b:k, None], rest[b:k, None], x[b:k], v[b:k], np.zeros((k - b, 3))], 1)
+        rows = oracle.merge_overlapping(rows)
+        mo, ro, xo, vo = oracle_run(oracle, rows[:, 0].copy(), rows[:, 1].copy(), rows[:, 2].copy(),
+                                    rows[:, 3:6].copy(), rows[:, 6:9].copy(), 6, True)
+        assert counts[s] == len(mo)
+        np.testing.assert_allclose(st[s]["m"], mo, rtol=1e-15)
+        assert np.abs(st[s]["x"] - xo).max() / np.abs(xo).max() < 1e-10
+        p_gpu = (st[s]["m"][:, None] * st[s]["v"]).sum(0)
+        p_orc = (mo[:, None] * vo).sum(0)
+        assert np.abs(p_gpu - p_orc).max() <= 1e-6 * (mo[:, None] * np.abs(vo)).sum()
+
+
+def test_graph_replay_equals_single_launches(gpu):
+    off, m, r, x, v = ensemble(40, 73, n_min=3, n_max=400)
+    a = Ensemble(off, m, x, v, r, merge=True, dt=DT)
+    b = Ensemble(off, m, x, v, r, merge=True, dt=DT)
+    a.evolve(40)             # 2 graph replays of 16 steps + 8 launches
+    for _ in range(40):
+        b.evolve(1)          # 40 single launches
+    sa, sb = a.state(), b.state()
+    for s in range(40):
+        assert np.array_equal(sa[s]["x"], sb[s]["x"]) and np.array_equal(sa[s]["v"], sb[s]["v"])
+    _, _, la = a.counts()
+    assert la == 41
+
+
+def test_autotune_restores_state(gpu):
+    off, m, r, x, v = ensemble(64, 74, n_min=3, n_max=1024)
+    a = Ensemble(off, m, x, v, r, merge=True, dt=DT)
+    t, ms = a.autotune()
+    assert t in (128, 256, 512) and ms > 0
+    st = a.state()
+    assert all(np.array_equal(st[s]["x"], x[off[s]:off[s + 1]]) for s in range(64))
+    a.evolve(3)
+    b = Ensemble(off, m, x, v, r, merge=True, dt=DT)
+    b.set_threads(t)
+    b.evolve(3)
+    sa, sb = a.state(), b.state()
+    assert all(np.array_equal(sa[s]["x"], sb[s]["x"]) for s in range(64))
+
+
+def test_capacity_limit(gpu):
+    off = np.array([0, 9000])
+    m = np.ones(9000)
+    x = np.random.default_rng(0).normal(size=(9000, 3))
+    with pytest.raises(Exception):
+        Ensemble(off, m, x)
