@@ -56,6 +56,15 @@ def parse_args():
                    help="instead of the benchmark: evolve the workload this many steps in both the mixed and the "
                         "FP64 path and report |dE/E| and momentum drift every --drift-every steps")
     p.add_argument("--drift-every", type=int, default=100)
+    p.add_argument("--workload", choices=["direct-mixed", "direct-fp64-1024", "bh", "ensemble", "adjoint"],
+                   default="direct-mixed", help="direct-mixed is the headline; the others print their own line")
+    p.add_argument("--bh-n", type=int, default=4194304)
+    p.add_argument("--bh-cpu-n", type=int, default=20000)
+    p.add_argument("--ens-systems", type=int, default=4096)
+    p.add_argument("--adj-n", type=int, default=16384)
+    p.add_argument("--adj-steps", type=int, default=2000)
+    p.add_argument("--adj-every", type=int, default=45)
+    p.add_argument("--adj-fd", type=int, default=0)
     return p.parse_args()
 
 
@@ -455,6 +464,209 @@ def run_drift(args, local):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------------------------------------------------
+# secondary workloads (--workload): the other configurations of the path, one JSON line each
+# ------------------------------------------------------------------------------------------------
+def _events(stream):
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return a, b
+
+
+def run_fp64_small(args, local):
+    """Plain direct summation as the reference runs it: N=1024 Plummer, FP64, leapfrog KDK,
+    dt=3600 s, 1000 steps; final state against the reference CPU run of the same call."""
+    from gregpackagescpp_b200 import System
+    from gregpackagescpp_b200.ics import UNITS_G6674, plummer
+    n, steps = 1024, 1000
+    m, x, v = plummer(n, args.seed)
+    s = System(m, x, v, timestep=3600.0, num_iterations=steps, units_format=UNITS_G6674, device=local)
+    s.evolve(16)  # warm-up (same call)
+    s = System(m, x, v, timestep=3600.0, num_iterations=steps, units_format=UNITS_G6674, device=local)
+    t0 = time.perf_counter()
+    ns = s.evolve(16)
+    wall = time.perf_counter() - t0
+    inter = (steps + 1) * n * (n - 1)
+    line = {"workload": "direct FP64, N=1024 Plummer, leapfrog KDK dt=3600 s, 1000 steps", "unit": UNIT,
+            "device_value": inter / (ns * 1e-9), "e2e_value": inter / wall, "device_s": ns * 1e-9, "e2e_s": wall}
+    try:
+        from oracle.oracle import RefOracle
+        if RefOracle.available():
+            xo, vo, _, ref_ns = RefOracle().evolve(16, m, x, v, 3600.0, steps, UNITS_G6674)
+            line["reference_cpu"] = {"value": inter / (ref_ns * 1e-9), "s": ref_ns * 1e-9, "cores": 1}
+            line["final_state_rel_err"] = {"x": float(np.abs(s.x - xo).max() / np.abs(xo).max()),
+                                           "v": float(np.abs(s.v - vo).max() / np.abs(vo).max())}
+    except Exception as exc:  # the reference library is optional on a box
+        line["reference_cpu"] = {"unavailable": str(exc)}
+    print(json.dumps(line), flush=True)
+
+
+def run_bh(args, local):
+    """Barnes-Hut: two Plummer spheres of 2^21 bodies each on a parabolic approach, FP32 tree
+    (T=float geometry, FP64 moments), theta=0.5, leapfrog KDK dt=3600 s; per-phase device times."""
+    from gregpackagescpp_b200 import _lib
+    from gregpackagescpp_b200._lib import check
+    from gregpackagescpp_b200.ics import two_plummer
+    L = _lib.load()
+    n_each = args.bh_n // 2
+    m, x, v = two_plummer(n_each, args.seed)
+    n = len(m)
+    x3, v3 = np.ascontiguousarray(x.reshape(-1)), np.ascontiguousarray(v.reshape(-1))
+    h = C.c_void_p()
+    check(L.gtd_system_create(C.byref(h), local, _lib.PREC_F64))
+    check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, args.steps, 0.0, 0.5))
+    check(L.gtd_system_upload(h, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
+    check(L.gtd_bh_set_tree_float(h, 1))
+    # phase timing: build, walk
+    import torch
+    p = C.c_void_p()
+    check(L.gtd_system_stream(h, C.byref(p)))
+    st = torch.cuda.ExternalStream(p.value, device=torch.device("cuda", local))
+    cnt = np.zeros(n, np.uint32)
+    check(L.gtd_bh_build(h, 1))
+    check(L.gtd_bh_accelerations(h, None, cnt.ctypes.data))  # warm-up
+    tb, tw = [], []
+    for _ in range(3):
+        e0, e1 = _events(st)
+        e0.record(st)
+        check(L.gtd_bh_build(h, 1))
+        e1.record(st)
+        e1.synchronize()
+        tb.append(e0.elapsed_time(e1))
+        e0.record(st)
+        check(L.gtd_bh_accelerations(h, None, None))
+        e1.record(st)
+        e1.synchronize()
+        tw.append(e0.elapsed_time(e1))
+    nn, nl = C.c_int64(), C.c_int64()
+    check(L.gtd_bh_tree_size(h, C.byref(nn), C.byref(nl), None))
+    inter = float(cnt.astype(np.float64).sum())
+    # the reference schedule end to end: evolve(leapfrog_kdk | barnes_hut) for --steps steps
+    ns = C.c_int64()
+    check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, args.steps, 0.0, 0.5))
+    check(L.gtd_system_upload(h, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
+    check(L.gtd_system_evolve(h, 16 | 65536, C.byref(ns)))
+    check(L.gtd_system_destroy(h))
+    build_ms, walk_ms = float(np.median(tb)), float(np.median(tw))
+    # algorithmic HBM bytes of one build: codes 16 B/body in + 12 B out, 8 radix passes x 24 B/body,
+    # node emission ~48 B/node, moments 32 B/node read + write
+    build_bytes = n * (28 + 8 * 24) + nn.value * (48 + 64)
+    line = {"workload": f"Barnes-Hut, two Plummer spheres N={n}, theta=0.5, FP32 tree, FP64 moments",
+            "n_bodies": n, "n_nodes": nn.value, "n_leaves": nl.value, "interactions_per_walk": inter,
+            "interactions_per_body": inter / n, "build_ms": build_ms, "walk_ms": walk_ms,
+            "walk_interactions_per_s": inter / (walk_ms * 1e-3),
+            "walk_flops_20_per_interaction_TFLOPs": 20 * inter / (walk_ms * 1e-3) / 1e12,
+            "build_algorithmic_GBs": build_bytes / (build_ms * 1e-3) / 1e9,
+            "evolve_steps": args.steps, "evolve_s": ns.value * 1e-9,
+            "steps_per_s": args.steps / (ns.value * 1e-9)}
+    try:
+        from gregpackagescpp_b200.ics import two_plummer as tp
+        from oracle.oracle import RefOracle
+        if RefOracle.available():
+            ms_, xs_, vs_ = tp(args.bh_cpu_n // 2, args.seed)
+            _, _, _, b_ns, w_ns = RefOracle().bh_kdk(ms_, xs_, vs_, 3600.0, 0, 0.5)
+            _, rcnt = RefOracle().bh_acc(xs_, ms_, 0.5)
+            line["reference_cpu"] = {"n_bodies": len(ms_), "build_s": b_ns * 1e-9, "walk_s": w_ns * 1e-9,
+                                     "walk_interactions_per_s": rcnt / (w_ns * 1e-9), "cores": 1}
+    except Exception as exc:
+        line["reference_cpu"] = {"unavailable": str(exc)}
+    print(json.dumps(line), flush=True)
+
+
+def run_ensemble(args, local):
+    """4096 independent systems, N ~ U{3..2048}, log-uniform masses, radii from 1500 kg/m^3,
+    positions in a 10 AU ball, sigma_v = 5 km/s; FP64 state, FP32 forces, merges; KDK dt=600 s."""
+    from gregpackagescpp_b200.ensemble import Ensemble
+    from gregpackagescpp_b200.ics import ensemble
+    off, m, r, x, v = ensemble(args.ens_systems, 4)
+    e = Ensemble(off, m, x, v, r, merge=True, dt=600.0, device=local)
+    threads, tune_ms = e.autotune()
+    e.evolve(args.warmup)
+    counts0, merges0, l0 = e.counts()
+    K = max(args.steps, 16)
+    ns = e.evolve(K)
+    counts, merges, l1 = e.counts()
+    inter = float((counts.astype(np.float64) * (counts - 1)).sum())
+    secs = ns * 1e-9
+    line = {"workload": f"ensemble of {len(off) - 1} systems, N~U{{3..2048}}, KDK dt=600 s, merges, FP32 forces",
+            "unit": "ensemble steps/s", "value": (len(off) - 1) * K / secs, "system_steps_per_s": (len(off) - 1) * K / secs,
+            "steps": K, "ms_per_step": 1e3 * secs / K, "pair_interactions_per_s": inter * K / secs,
+            "bodies": int(off[-1]), "merges_during_timed": int(merges - merges0), "autotuned_threads": threads,
+            "gpu_launches": int(l1 - l0), "launch": "one persistent launch per step, replayed from a CUDA graph"}
+    try:
+        from oracle.oracle import RefOracle
+        if RefOracle.available():
+            # the reference's per-system evolve on a sample of systems, one core
+            import time as _t
+            ro = RefOracle()
+            rng = np.random.default_rng(0)
+            tot_i, tot_s = 0.0, 0.0
+            for s in rng.choice(len(off) - 1, 24, replace=False):
+                b, k = off[s], off[s + 1]
+                if k - b < 2:
+                    continue
+                _, _, _, rns = ro.evolve(16, m[b:k], x[b:k], v[b:k], 600.0, 4, "M66743:66740,D1:1,T1:1",
+                                         r=r[b:k], coll=0)
+                tot_i += 5.0 * (k - b) * (k - b - 1)
+                tot_s += rns * 1e-9
+            ref_ips = tot_i / tot_s
+            line["reference_cpu"] = {"pair_interactions_per_s_per_core": ref_ips,
+                                     "ensemble_steps_per_s_per_core_est": ref_ips / (inter / (len(off) - 1)),
+                                     "sample": "24 random systems, evolve(leapfrog_kdk) 4 steps, collisions off"}
+    except Exception as exc:
+        line["reference_cpu"] = {"unavailable": str(exc)}
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args, local):
+    """Adjoint: N=16384 Plummer, FP64 KDK dt=3600 s, 2000 steps, checkpoints every 45 steps;
+    loss = mean |x_T - x*|^2 with x* = forward final + N(0, (0.01 AU)^2)."""
+    import torch
+
+    from gregpackagescpp_b200.adjoint import leapfrog_final_state
+    from gregpackagescpp_b200.ics import AU, plummer
+    n, T, every = args.adj_n, args.adj_steps, args.adj_every
+    m, x, v = plummer(n, 5)
+    dev = torch.device("cuda", local)
+    tm, tx, tv = (torch.tensor(a, dtype=torch.float64, device=dev) for a in (m, x, v))
+    with torch.no_grad():
+        xT, _ = leapfrog_final_state(tx, tv, tm, 6.674e-11, 3600.0, T, every)
+    g = torch.Generator(device=dev).manual_seed(7)
+    target = xT + 0.01 * AU * torch.randn(xT.shape, dtype=torch.float64, device=dev, generator=g)
+    xa, va, ma = tx.clone().requires_grad_(), tv.clone().requires_grad_(), tm.clone().requires_grad_()
+    st = torch.cuda.current_stream()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(st)
+    xT, _ = leapfrog_final_state(xa, va, ma, 6.674e-11, 3600.0, T, every)
+    loss = ((xT - target) ** 2).sum(-1).mean()
+    e1.record(st)
+    loss.backward()
+    e2.record(st)
+    torch.cuda.synchronize()
+    fwd, bwd = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    line = {"workload": f"adjoint KDK N={n}, {T} steps, checkpoints every {every}", "forward_ms": fwd,
+            "backward_ms": bwd, "backward_over_forward": bwd / fwd, "total_over_forward": (fwd + bwd) / fwd}
+    if args.adj_fd > 0:
+        rng = np.random.default_rng(8)
+        errs = []
+        for which, base, grad in (("x", tx, xa.grad), ("v", tv, va.grad), ("m", tm, ma.grad)):
+            flat = base.reshape(-1)
+            for idx in rng.choice(flat.numel(), max(1, args.adj_fd // 3), replace=False):
+                hs = 1e-6 * abs(float(flat[idx]))
+                vals = []
+                for sgn in (1, -1):
+                    args3 = [tx.clone(), tv.clone(), tm.clone()]
+                    args3["xvm".index(which)].reshape(-1)[idx] += sgn * hs
+                    with torch.no_grad():
+                        y, _ = leapfrog_final_state(*args3, 6.674e-11, 3600.0, T, every)
+                        vals.append(float(((y - target) ** 2).sum(-1).mean()))
+                fd = (vals[0] - vals[1]) / (2 * hs)
+                errs.append(abs(float(grad.reshape(-1)[idx]) - fd) / max(abs(fd), 1e-300))
+        line["fd_check"] = {"coords": len(errs), "h_rel": 1e-6, "max_rel_err": max(errs),
+                            "median_rel_err": float(np.median(errs))}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_init()
@@ -464,6 +676,10 @@ def main():
         elif args.drift_steps > 0:
             if rank == 0:
                 run_drift(args, local)
+        elif args.workload != "direct-mixed":
+            if rank == 0:
+                {"direct-fp64-1024": run_fp64_small, "bh": run_bh, "ensemble": run_ensemble,
+                 "adjoint": run_adjoint}[args.workload](args, local)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -463,6 +463,19 @@ int gtd_system_upload(gtd_system *s, int64_t n, const double *m, const double *r
     return GTD_OK;
 }
 
+int gtd_system_survivors(gtd_system *s, int64_t *upload_index) {
+    if (!s || !upload_index) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(s->device);
+    const int64_t n = s->n;
+    if (n == 0) return GTD_OK;
+    std::vector<int32_t> ids((size_t)n);
+    GTD_CUDA(cudaMemcpyAsync(ids.data(), s->ids, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    std::sort(ids.begin(), ids.end());
+    for (int64_t i = 0; i < n; ++i) upload_index[i] = ids[(size_t)i];
+    return GTD_OK;
+}
+
 int gtd_system_num_bodies(const gtd_system *s, int64_t *n) {
     if (!s || !n) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
     *n = s->n;

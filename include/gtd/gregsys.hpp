@@ -1,0 +1,294 @@
+// Drop-in gtd::system (GregW10/GregPackagesCPP gregsys.hpp:135-3612) whose evolve() runs on the
+// B200 through the C ABI (gtd_b200.h).  Same template parameters, method flags, constructors,
+// setters and evolve() contract; the std::vector<body> stays authoritative on the host between
+// calls and is gathered to the device SoA at evolve() entry and scattered back at exit.
+//
+// Differences, all documented in the engine: no long double arithmetic on the device (FP64 is used
+// for every T); trajectory recording (memFreq), file output (fileFreq) and progress printing are
+// not performed; evolve-time merges use check_overlap's scan as that routine intends.
+#ifndef GTD_B200_GREGSYS_HPP
+#define GTD_B200_GREGSYS_HPP
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <initializer_list>
+#include <regex>
+#include <string>
+#include <vector>
+
+#include "greg8tree.hpp"
+#include "gregbod.hpp"
+
+namespace gtd {
+
+template <isNumWrapper M = long double, isNumWrapper R = long double, isNumWrapper T = long double,
+          bool prog = false, bool mergeOverlappingBodies = false, int collisions = 0, uint64_t memFreq = 0,
+          uint64_t fileFreq = 1, bool binaryFile = true>
+class system {
+public:
+    static constexpr int two_body = GTD_TWO_BODY;
+    static constexpr int euler = GTD_EULER;
+    static constexpr int modified_euler = GTD_MODIFIED_EULER;
+    static constexpr int midpoint = GTD_MIDPOINT;
+    static constexpr int leapfrog_kdk = GTD_LEAPFROG_KDK;
+    static constexpr int leapfrog_dkd = GTD_LEAPFROG_DKD;
+    static constexpr int rk4 = GTD_RK4;
+    static constexpr int rk3_8 = GTD_RK3_8;
+    static constexpr int barnes_hut = GTD_BARNES_HUT;
+    static constexpr int fast_multipole = 131'072;
+    static constexpr int no_coll_check = 0;
+    static constexpr int overlap_coll_check = 3;
+    static constexpr int pred_coll_check = 7;
+    static constexpr long double G_SI = 0.000'000'000'066'743;
+    static_assert(collisions <= pred_coll_check && !(collisions & (collisions + 1)),
+                  "Invalid collision-checking option.");
+    using bod_t = body<M, R, T, memFreq>;
+
+private:
+    std::vector<bod_t> bods;
+    long double G = 66'743e-15L;
+    long double eps = 0, dt = 1, bh_theta = 3.14159265358979323846L / 3;
+    uint64_t iterations = 1'000;
+    long double time_elapsed{};
+    bool mixed = false;
+    gtd_system *dev = nullptr;
+    int device = 0;
+
+    void parse_units_format(const std::string &str) {  // gregsys.hpp:245-282
+        static const std::regex re{R"(^\s*(m|M)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(d|D)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(t|T)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*$)\d*[1-9]+\d*\s*$)"};
+        if (!std::regex_match(str, re))
+            throw std::invalid_argument{"The units_format string passed, \"" + str +
+                                        "\", does not match the format required:\n\"Ma:b,Dc:x,Ty:z\"."};
+        uint64_t v[6];
+        int k = 0;
+        static const std::regex digits{R"(\d+)"};
+        for (std::sregex_iterator it{str.begin(), str.end(), digits}, end; it != end && k < 6; ++it)
+            v[k++] = std::stoull(it->str());
+        const uint64_t m_den = v[0], m_num = v[1], d_num = v[2], d_den = v[3], t_den = v[4], t_num = v[5];
+        G = 66'743;
+        G *= m_num * d_num * d_num * d_num * t_num * t_num;
+        G /= m_den * d_den * d_den * d_den * t_den * t_den;
+        G /= 1'000'000'000'000'000;
+    }
+    void ensure_device() {
+        if (!dev) throw_status(gtd_system_create(&dev, device, mixed ? GTD_PREC_MIXED : GTD_PREC_F64));
+    }
+    int coll_mode() const {
+        if constexpr (collisions == overlap_coll_check) return mergeOverlappingBodies ? GTD_MERGE_COLL : GTD_OVERLAP_COLL;
+        return GTD_NO_COLL;
+    }
+    void push() {
+        ensure_device();
+        const int64_t n = (int64_t)bods.size();
+        std::vector<double> m(n), r(n), e(n), x(3 * n), v(3 * n);
+        for (int64_t i = 0; i < n; ++i) {
+            const bod_t &b = bods[i];
+            m[i] = (double)b.mass_;
+            r[i] = (double)b.radius;
+            e[i] = (double)b.rest_c;
+            x[3 * i] = (double)b.curr_pos.x; x[3 * i + 1] = (double)b.curr_pos.y; x[3 * i + 2] = (double)b.curr_pos.z;
+            v[3 * i] = (double)b.curr_vel.x; v[3 * i + 1] = (double)b.curr_vel.y; v[3 * i + 2] = (double)b.curr_vel.z;
+        }
+        throw_status(gtd_system_set_params(dev, (double)G, (double)dt, iterations, (double)eps, (double)bh_theta));
+        throw_status(gtd_system_set_collisions(dev, coll_mode()));
+        throw_status(gtd_bh_set_tree_float(dev, std::is_same_v<T, float> ? 1 : 0));
+        throw_status(gtd_system_upload(dev, n, m.data(), r.data(), e.data(), x.data(), v.data()));
+    }
+    void pull() {
+        int64_t n = 0;
+        throw_status(gtd_system_num_bodies(dev, &n));
+        std::vector<double> m(n), r(n), e(n), x(3 * n), v(3 * n), a(3 * n);
+        throw_status(gtd_system_download(dev, &n, m.data(), r.data(), e.data(), x.data(), v.data(), a.data()));
+        if ((size_t)n < bods.size()) {
+            // merges: the survivors (by upload index) keep their body objects and relative order
+            std::vector<int64_t> idx(n);
+            throw_status(gtd_system_survivors(dev, idx.data()));
+            std::vector<bod_t> kept;
+            kept.reserve(n);
+            for (int64_t i = 0; i < n; ++i) kept.emplace_back(std::move(bods[(size_t)idx[i]]));
+            bods.swap(kept);
+        }
+        for (int64_t i = 0; i < n; ++i) {
+            bod_t &b = bods[i];
+            b.mass_ = (M)m[i];
+            b.radius = (R)r[i];
+            b.rest_c = e[i];
+            b.curr_pos = vector3D<T>{(T)x[3 * i], (T)x[3 * i + 1], (T)x[3 * i + 2]};
+            b.curr_vel = vector3D<T>{(T)v[3 * i], (T)v[3 * i + 1], (T)v[3 * i + 2]};
+            b.acc = vector3D<T>{(T)a[3 * i], (T)a[3 * i + 1], (T)a[3 * i + 2]};
+        }
+    }
+    void check_dt() {
+        if (dt <= 0) throw std::invalid_argument{"Time-step cannot be zero or negative.\n"};
+    }
+
+public:
+    system() : G{G_SI} {}
+    explicit system(long double timestep, uint64_t num_iterations, const char *units_format)
+        : dt{timestep}, iterations{num_iterations} {
+        check_dt();
+        parse_units_format(units_format);
+    }
+    system(std::vector<bod_t> bodies, long double timestep = 1, uint64_t num_iterations = 1'000,
+           const char *units_format = "M1:1,D1:1,T1:1", bool allow_overlapping_bodies = false)
+        : bods{std::move(bodies)}, dt{timestep}, iterations{num_iterations} {
+        check_dt();
+        if (!allow_overlapping_bodies) check_overlap();
+        parse_units_format(units_format);
+    }
+    system(const std::initializer_list<bod_t> &list) : bods{list}, G{G_SI} { check_overlap(); }
+    system(const system &other) : bods{other.bods}, G{other.G}, eps{other.eps}, dt{other.dt},
+                                  bh_theta{other.bh_theta}, iterations{other.iterations}, mixed{other.mixed} {}
+    system &operator=(const system &) = delete;
+    ~system() { gtd_system_destroy(dev); }
+
+    // ---- check_overlap (gregsys.hpp:307-342) on the device --------------------------------------
+    void check_overlap() {
+        if (bods.size() < 2) return;
+        push();
+        int32_t pair[2] = {0, 0};
+        throw_status(gtd_system_check_overlap(dev, mergeOverlappingBodies ? 1 : 0, pair));
+        if constexpr (mergeOverlappingBodies) pull();
+    }
+
+    // ---- accessors and setters (gregsys.hpp:1627-1672) ------------------------------------------
+    typename std::vector<bod_t>::size_type num_bodies() const noexcept { return bods.size(); }
+    long double elapsed_time() const noexcept { return time_elapsed; }
+    long double G_val() const noexcept { return G; }
+    bool set_iterations(uint64_t number) noexcept {
+        if (!number) return false;
+        iterations = number;
+        return true;
+    }
+    bool set_timestep(const long double &delta_t) noexcept {
+        if (delta_t <= 0) return false;
+        dt = delta_t;
+        return true;
+    }
+    void set_G_units(const char *units_format) { parse_units_format(units_format); }
+    bool set_softening(long double e) noexcept {
+        if (e < sqrtl(std::numeric_limits<long double>::min())) return false;
+        eps = e;
+        return true;
+    }
+    bool set_bh_opening_angle(long double theta) {
+        if (theta < 0 || theta >= 3.14159265358979323846L) return false;
+        bh_theta = theta;
+        return true;
+    }
+    // Engine extension: FP32 pair forces with FP64 Kahan sums (true) or FP64 throughout (false).
+    void use_mixed_precision(bool on) {
+        if (on != mixed) {
+            gtd_system_destroy(dev);
+            dev = nullptr;
+            mixed = on;
+        }
+    }
+    void set_device(int d) {
+        gtd_system_destroy(dev);
+        dev = nullptr;
+        device = d;
+    }
+
+    system &add_body(const bod_t &b, bool chk_overlap = true) {
+        bods.emplace_back(b);
+        if (chk_overlap) check_overlap();
+        return *this;
+    }
+    template <typename... Args>
+    system &emplace_body(bool chk_overlap, Args &&...args) {
+        bods.emplace_back(std::forward<Args>(args)...);
+        if (chk_overlap) check_overlap();
+        return *this;
+    }
+    system &add_bodies(const std::vector<bod_t> &bodies, bool chk_overlap = true) {
+        bods.insert(bods.end(), bodies.begin(), bodies.end());
+        if (chk_overlap) check_overlap();
+        return *this;
+    }
+    bool remove_body(uint64_t id) {
+        for (auto it = bods.begin(); it != bods.end(); ++it)
+            if (it->get_id() == id) {
+                bods.erase(it);
+                return true;
+            }
+        return false;
+    }
+    const bod_t &get_body(uint64_t id) const {
+        for (const auto &b : bods)
+            if (b.get_id() == id) return b;
+        throw std::invalid_argument("The id passed does not correspond to any body present in this system object.\n");
+    }
+    const bod_t &front() const {
+        if (bods.empty()) throw std::logic_error{"gtd::system<>::front cannot be called on an empty gtd::system object.\n"};
+        return bods.front();
+    }
+    const bod_t &back() const {
+        if (bods.empty()) throw std::logic_error{"gtd::system<>::back cannot be called on an empty gtd::system object.\n"};
+        return bods.back();
+    }
+    const bod_t &operator[](typename std::vector<bod_t>::size_type i) const { return bods[i]; }
+    auto begin() { return bods.begin(); }
+    auto end() { return bods.end(); }
+    auto begin() const { return bods.cbegin(); }
+    auto end() const { return bods.cend(); }
+
+    // ---- evolve (gregsys.hpp:2593-3071) -----------------------------------------------------------
+    template <typename evFuncT = std::nullptr_t, typename bodFuncT = std::nullptr_t,
+              typename bodsFuncT = std::nullptr_t>
+        requires(std::same_as<evFuncT, std::nullptr_t> || requires(evFuncT f) { { f() } -> std::same_as<bool>; }) &&
+                (std::same_as<bodFuncT, std::nullptr_t> || requires(bodFuncT f, bod_t &b) { { f(b) } -> std::same_as<void>; }) &&
+                (std::same_as<bodsFuncT, std::nullptr_t> ||
+                 requires(bodsFuncT f, std::vector<bod_t> &v) { { f(v) } -> std::same_as<void>; })
+    const std::chrono::nanoseconds evolve(int integration_method = leapfrog_kdk,
+                                          const evFuncT &continue_ev_if = nullptr,
+                                          const bodFuncT &for_each_bod = nullptr,
+                                          const bodsFuncT &for_all_bods = nullptr) {
+        if (bods.empty()) return std::chrono::nanoseconds::zero();
+        push();
+        if constexpr (std::same_as<evFuncT, std::nullptr_t> && std::same_as<bodFuncT, std::nullptr_t> &&
+                      std::same_as<bodsFuncT, std::nullptr_t>) {
+            int64_t ns = 0;
+            throw_status(gtd_system_evolve(dev, integration_method, &ns));
+            pull();
+            time_elapsed = iterations * dt;
+            return std::chrono::nanoseconds{ns};
+        } else {
+            // callbacks see the bodies every step: the state makes a host round trip per step
+            const auto start = std::chrono::steady_clock::now();
+            throw_status(gtd_system_evolve_begin(dev, integration_method));
+            uint64_t steps = 0;
+            while (true) {
+                if constexpr (std::same_as<evFuncT, std::nullptr_t>) {
+                    if (steps >= iterations) break;
+                } else {
+                    if (!continue_ev_if()) break;
+                }
+                throw_status(gtd_system_evolve_steps(dev, 1));
+                ++steps;
+                pull();
+                if constexpr (!std::same_as<bodsFuncT, std::nullptr_t>) for_all_bods(bods);
+                if constexpr (!std::same_as<bodFuncT, std::nullptr_t>)
+                    for (bod_t &b : bods) for_each_bod(b);
+                push();
+                throw_status(gtd_system_evolve_begin(dev, integration_method));
+            }
+            pull();
+            time_elapsed = steps * dt;
+            return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - start);
+        }
+    }
+};
+
+typedef system<long double, long double, long double> sys;
+typedef system<long double, long double, long double, false, false, 3> sys_c;
+typedef system<long double, long double, long double, false, true> sys_m;
+typedef system<long double, long double, long double, false, true, 3> sys_mc;
+typedef system<long double, long double, long double, false, false, 0, 0, 0, false> sys_n;
+typedef system<long double, long double, long double, false, false, 3, 0, 0, false> sys_c_n;
+typedef system<long double, long double, long double, false, true, 0, 0, 0, false> sys_m_n;
+
+}  // namespace gtd
+#endif

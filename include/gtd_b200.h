@@ -100,6 +100,9 @@ GTD_API int gtd_system_upload(gtd_system *sys, int64_t n, const double *m, const
 GTD_API int gtd_system_download(gtd_system *sys, int64_t *n, double *m, double *r, double *rest, double *x3, double *v3,
                         double *a3);
 GTD_API int gtd_system_num_bodies(const gtd_system *sys, int64_t *n);
+/* Upload indices of the current bodies in download order (ascending): after merges, which of the
+ * uploaded bodies survived (their state holds the merged result). */
+GTD_API int gtd_system_survivors(gtd_system *sys, int64_t *upload_index);
 
 /* gtd::system::evolve(method) with no callbacks (gregsys.hpp:2593-3071): `iterations` steps of
  * the method on the device, one upload/download around it done by the caller.  *elapsed_ns is

@@ -1,0 +1,96 @@
+// Drop-in check: code written against the reference's gtd::system / gtd::bh_tree API, compiled
+// against include/gtd/*.hpp and run on the B200, compared with the CPU oracle (test infrastructure).
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "gtd/gregsys.hpp"
+#include "nbody_oracle.h"
+
+using sys_t = gtd::system<double, double, double, false, false, 0, 0, 0, false>;
+using csys_t = gtd::system<double, double, double, false, false, 3, 0, 0, false>;
+using bod = sys_t::bod_t;
+
+static std::vector<bod> make(int n, unsigned seed, double rad) {
+    std::vector<bod> v;
+    unsigned long long s = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+    auto u = [&]() { s = s * 6364136223846793005ULL + 1442695040888963407ULL; return ((s >> 11) + 0.5) / 9007199254740992.0; };
+    for (int i = 0; i < n; ++i) {
+        const double x = (u() - .5) * 3e11, y = (u() - .5) * 3e11, z = (u() - .5) * 3e11;
+        v.emplace_back(1e30 / n * (0.5 + u()), rad, gtd::vector3D<double>{x, y, z},
+                       gtd::vector3D<double>{(u() - .5) * 4e4, (u() - .5) * 4e4, (u() - .5) * 4e4}, u());
+    }
+    return v;
+}
+
+template <typename S>
+static double compare(S &s, const std::vector<bod> &init, int method, int coll, uint64_t steps) {
+    const int n = (int)init.size();
+    std::vector<double> m(n), r(n), e(n), x(3 * n), v(3 * n), a(3 * n);
+    for (int i = 0; i < n; ++i) {
+        m[i] = init[i].mass(); r[i] = init[i].rad(); e[i] = (double)init[i].restitution();
+        x[3 * i] = init[i].pos().x; x[3 * i + 1] = init[i].pos().y; x[3 * i + 2] = init[i].pos().z;
+        v[3 * i] = init[i].vel().x; v[3 * i + 1] = init[i].vel().y; v[3 * i + 2] = init[i].vel().z;
+    }
+    long double G;
+    orc_G_units_into(66743, 66740, 1, 1, 1, 1, &G);
+    orc_evolve(method, coll, n, m.data(), r.data(), e.data(), x.data(), v.data(), a.data(), 3600.0L, steps, &G);
+    double err = 0, scale = 0;
+    for (int i = 0; i < n; ++i) {
+        err = std::fmax(err, std::fabs(s[i].pos().x - x[3 * i]) + std::fabs(s[i].pos().y - x[3 * i + 1]) +
+                                 std::fabs(s[i].pos().z - x[3 * i + 2]));
+        scale = std::fmax(scale, std::fabs(x[3 * i]));
+    }
+    return err / scale;
+}
+
+int main() {
+    int fails = 0;
+    const auto init = make(300, 7, 1.0);
+    for (int method : {sys_t::euler, sys_t::modified_euler, sys_t::midpoint, sys_t::leapfrog_kdk, sys_t::leapfrog_dkd}) {
+        sys_t s{init, 3600, 10, "M66743:66740,D1:1,T1:1", true};
+        s.evolve(method);
+        const double err = compare(s, init, method, 0, 10);
+        std::printf("method %d: max rel position error %.3e\n", method, err);
+        fails += !(err < 1e-12);
+    }
+    {  // overlap restitution (collisions = 3)
+        const auto ci = make(200, 9, 1.5e10);
+        csys_t s{ci, 3600, 5, "M66743:66740,D1:1,T1:1", true};
+        s.evolve(csys_t::leapfrog_kdk);
+        const double err = compare(s, ci, 16, 3, 5);
+        std::printf("collisions: max rel position error %.3e\n", err);
+        fails += !(err < 1e-11);
+    }
+    {  // add-time overlap check throws like the reference
+        auto ov = make(20, 11, 1.0);
+        ov.back() = bod{1e20, 5e11, ov.front().pos(), ov.front().vel(), 1.0};
+        bool thrown = false;
+        try {
+            sys_t s{ov, 1, 1, "M1:1,D1:1,T1:1", false};
+        } catch (const gtd::overlapping_bodies_error &) {
+            thrown = true;
+        }
+        std::printf("overlap check threw: %d\n", (int)thrown);
+        fails += !thrown;
+    }
+    {  // octree leaf order against the host rebuild
+        const auto bi = make(2000, 13, 1.0);
+        gtd::bh_tree<double, double, double, 0> tree;
+        tree.add_bodies(bi);
+        std::vector<double> m(bi.size()), x(3 * bi.size());
+        for (size_t i = 0; i < bi.size(); ++i) {
+            m[i] = bi[i].mass(); x[3 * i] = bi[i].pos().x; x[3 * i + 1] = bi[i].pos().y; x[3 * i + 2] = bi[i].pos().z;
+        }
+        orc_tree t;
+        orc_bh_build((int)bi.size(), x.data(), m.data(), 0, &t);
+        const auto order = tree.leaf_order();
+        bool same = (int)tree.cells().size() == t.n_nodes && (int)order.size() == t.n;
+        for (int k = 0; same && k < t.n; ++k) same = order[k] == &bi[t.perm[k]];
+        orc_bh_free(&t);
+        std::printf("octree leaf order matches host rebuild: %d\n", (int)same);
+        fails += !same;
+    }
+    std::printf(fails ? "FAIL\n" : "OK\n");
+    return fails ? 1 : 0;
+}
