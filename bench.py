@@ -59,7 +59,7 @@ def parse_args():
     p.add_argument("--workload", choices=["direct-mixed", "direct-fp64-1024", "bh", "ensemble", "adjoint"],
                    default="direct-mixed", help="direct-mixed is the headline; the others print their own line")
     p.add_argument("--bh-n", type=int, default=4194304)
-    p.add_argument("--bh-cpu-n", type=int, default=20000)
+    p.add_argument("--bh-cpu-n", type=int, default=10000)
     p.add_argument("--ens-systems", type=int, default=4096)
     p.add_argument("--adj-n", type=int, default=16384)
     p.add_argument("--adj-steps", type=int, default=2000)
@@ -562,7 +562,7 @@ def run_bh(args, local):
     try:
         from gregpackagescpp_b200.ics import two_plummer as tp
         from oracle.oracle import RefOracle
-        if RefOracle.available():
+        if RefOracle.available() and args.bh_cpu_n > 0:
             ms_, xs_, vs_ = tp(args.bh_cpu_n // 2, args.seed)
             _, _, _, b_ns, w_ns = RefOracle().bh_kdk(ms_, xs_, vs_, 3600.0, 0, 0.5)
             _, rcnt = RefOracle().bh_acc(xs_, ms_, 0.5)
