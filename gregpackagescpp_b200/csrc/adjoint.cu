@@ -203,6 +203,7 @@ static int adj_force(gtd_adjoint *A, const double4 *x, cudaStream_t st) {
     sa.n = A->n;
     sa.src = x;
     sa.cur = x;
+    sa.vel = A->v;
     sa.acc = A->a;
     rc = launch_integrate(A->fplan, A->fpart, EPI_ACC, sa, st);
     A->launches += 2;

@@ -457,12 +457,13 @@ __global__ void integrate_kernel(IntArgs a) {
     }
     const StepArgs &st = a.st;
     const double h = st.h, h2 = 0.5 * st.h;
+    if (a.epi == EPI_ACC) {  // the force alone: position and velocity are not read
+        st.acc[i] = make_double4(ax, ay, az, 0.0);
+        return;
+    }
     const double4 x = st.cur[i];
     double4 v = st.vel[i];
     switch (a.epi) {
-        case EPI_ACC:
-            st.acc[i] = make_double4(ax, ay, az, 0.0);
-            break;
         case EPI_KDK: {
             st.acc[i] = make_double4(ax, ay, az, 0.0);
             v.x = fma(h2, ax, v.x); v.y = fma(h2, ay, v.y); v.z = fma(h2, az, v.z);
