@@ -78,10 +78,13 @@ def test_adjoint_vs_central_differences(gpu):
     loss_of(xa, va, ma).backward()
     rng = np.random.default_rng(7)
     checks = 0
-    for which, base, grad in (("x", x, xa.grad), ("v", v, va.grad), ("m", m, ma.grad)):
+    # h = 1e-6 relative for positions and velocities.  For masses a 1e-6 relative step moves the
+    # FP64 loss by only ~1e5 ulps, so the central difference itself carries ~1e-4 roundoff error;
+    # 1e-4 relative keeps its truncation and roundoff errors below 1e-5.
+    for which, base, grad, hrel in (("x", x, xa.grad, 1e-6), ("v", v, va.grad, 1e-6), ("m", m, ma.grad, 1e-4)):
         flat = base.reshape(-1)
         for idx in rng.choice(flat.numel(), 6, replace=False):
-            hstep = 1e-6 * abs(float(flat[idx]))
+            hstep = hrel * abs(float(flat[idx]))
             args = [x, v, m]
             k = "xvm".index(which)
             plus, minus = [a.clone() for a in args], [a.clone() for a in args]
@@ -90,7 +93,7 @@ def test_adjoint_vs_central_differences(gpu):
             with torch.no_grad():
                 fd = (float(loss_of(*plus)) - float(loss_of(*minus))) / (2 * hstep)
             g = float(grad.reshape(-1)[idx])
-            assert abs(g - fd) <= 1e-5 * max(abs(fd), 1e-30) + 1e-5 * float(grad.abs().max()) * 1e-3, (which, idx, g, fd)
+            assert abs(g - fd) <= 1e-5 * abs(fd) + 1e-7 * float(grad.abs().max()), (which, idx, g, fd)
             checks += 1
     assert checks == 18
 
