@@ -170,6 +170,24 @@ GTD_API int gtd_bh_tree_download(gtd_system *sys, uint64_t *codes, int32_t *perm
  * last gtd_bh_build.  n_inter (per body, optional) counts accepted cells and leaves. */
 GTD_API int gtd_bh_accelerations(gtd_system *sys, double *a3, uint32_t *n_inter);
 
+/* ---- direct-sum accelerations that allocate nothing ------------------------------------------
+ * No counterpart in the reference.  For callers that cannot let a library call cudaMalloc: a
+ * process whose device memory is already owned by a pool (a PyTorch caching allocator, a code that
+ * reserves everything at start-up) may have none to give, and cudaMalloc/cudaFree synchronise the
+ * device, stalling other streams inside a running loop.  The caller passes device buffers: pm4 =
+ * n x 4 doubles (x, y, z, m), 16-byte aligned; acc3 = n x 3 doubles, written with the accelerations
+ * sum_j G m_j (x_j - x_i) / |x_j - x_i|^3 (as gtd_system_accelerations).  The only scratch, the
+ * force kernel's partial sums, lives in a fixed 8 MiB device array compiled into the library (every
+ * GPU that loads the library holds it until the process exits); n is limited to 65536 and larger n
+ * is rejected with GTD_ERR_CAPACITY.  The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress), so make the first call on each device before any stream capture.  All
+ * calls share the array: calls whose work overlaps on the GPU (different streams, or different
+ * host threads) race on it and must be serialised by the caller.  Nothing in it needs clearing
+ * between calls (every partial sum read is written first by the same call).  stream: a
+ * cudaStream_t or NULL; the call returns after enqueueing. */
+GTD_API int gtd_direct_accelerations_noalloc(int64_t n, const double *pm4, double G, int precision, double *acc3,
+                                             void *stream);
+
 /* ---- batched ensemble of independent systems ------------------------------------------------
  * Replaces the drivers' pattern of one gtd::system per std::thread (bdsim.cpp:82-113): every
  * system advances by leapfrog KDK (gregsys.hpp:2946-2990) with FP64 state and FP32 pair forces,
