@@ -8,7 +8,7 @@ force evaluation of N(N-1) ordered pair-interactions, kick).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU: the north-star path runs on one GPU; N > 1 runs N independent replicas (one process
+Multi-GPU: the hot path runs on one GPU; N > 1 runs N independent replicas (one process
 per GPU, no data-path collective; "scaling": "weak").  The reference arm times the reference's
 own single-threaded CPU evolve (oracle/_ref, built from the reference headers; the C port under
 oracle/ where that library is absent) on all host cores, as independent copies.
@@ -37,6 +37,10 @@ sys.path.insert(0, ROOT)
 METRIC = "pair-interactions/s mixed vs FP64 GPU at |ΔE/E|≤1e-6; ensemble steps/s"
 UNIT = "pair-interactions/s"
 FLOPS_PER_INTERACTION = 20
+# dram__bytes_read.sum + dram__bytes_write.sum of one force_mixed_kernel launch, from an ncu capture
+# (--metrics dram__bytes_read.sum,dram__bytes_write.sum) of this workload: (N, variant) -> bytes.
+# The positions (N x 32 B = 8.39 MB at N = 262144) are read once; the partial sums stay in L2.
+NCU_FORCE_TRAFFIC = {(262144, 8): 8688384 + 5120}
 
 
 def parse_args():
@@ -52,6 +56,8 @@ def parse_args():
     p.add_argument("--e2e-iterations", type=int, default=5)
     p.add_argument("--cpu-sample-n", type=int, default=8192)
     p.add_argument("--cpu-sample-steps", type=int, default=3)
+    p.add_argument("--cpu-baseline-steps", type=int, default=40,
+                   help="steps of the single-core reference sample beside the GPU line (~10 s at N=8192)")
     p.add_argument("--drift-steps", type=int, default=0,
                    help="instead of the benchmark: evolve the workload this many steps in both the mixed and the "
                         "FP64 path and report |dE/E| and momentum drift every --drift-every steps")
@@ -65,6 +71,8 @@ def parse_args():
     p.add_argument("--adj-steps", type=int, default=2000)
     p.add_argument("--adj-every", type=int, default=45)
     p.add_argument("--adj-fd", type=int, default=0)
+    p.add_argument("--mixed-variant", type=int, default=-1,
+                   help="use this mixed force-kernel variant instead of the autotuner's choice")
     return p.parse_args()
 
 
@@ -287,7 +295,11 @@ def run_ours(args, rank, world, local):
     tuned = {}
     for name, h in (("mixed", hmx), ("fp64", h64)):
         best, best_ms = C.c_int(), C.c_double()
-        check(L.gtd_system_autotune_direct(h, 3, C.byref(best), C.byref(best_ms)))
+        if name == "mixed" and args.mixed_variant >= 0:
+            check(L.gtd_system_set_direct_variant(h, args.mixed_variant))
+            best.value, best_ms.value = args.mixed_variant, float("nan")
+        else:
+            check(L.gtd_system_autotune_direct(h, 3, C.byref(best), C.byref(best_ms)))
         ii, fold = C.c_int(), C.c_int()
         check(L.gtd_direct_variant_info(_lib.PREC_MIXED if name == "mixed" else _lib.PREC_F64, best.value,
                                         C.byref(ii), C.byref(fold)))
@@ -389,11 +401,11 @@ def run_ours(args, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample_n > 0:
         stage("cpu baseline sample")
-        cval, kind, secs = cpu_sample(args.cpu_sample_n, args.cpu_sample_steps, args.seed, 1)
+        cval, kind, secs = cpu_sample(args.cpu_sample_n, args.cpu_baseline_steps, args.seed, 1)
         cpu = {"value": cval, "unit": UNIT, "cores": 1, "kind": kind,
                "sample": f"the reference evolve(leapfrog_kdk) (single-threaded by design) on an N="
-                         f"{args.cpu_sample_n} Plummer sphere, {args.cpu_sample_steps} step(s) "
-                         f"({args.cpu_sample_steps + 1} force evaluations), {secs:.1f} s of evolve time"}
+                         f"{args.cpu_sample_n} Plummer sphere, {args.cpu_baseline_steps} step(s) "
+                         f"({args.cpu_baseline_steps + 1} force evaluations), {secs:.1f} s of evolve time"}
 
     if rank == 0:
         line = {
@@ -410,7 +422,10 @@ def run_ours(args, rank, world, local):
                          "acc_rel_err_median": float(np.median(rel)), "acc_rel_err_max": float(rel.max()),
                          "energy_drift_rel": drift, "energy_drift_steps": W + K},
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
-                         "unit": "TFLOP/s", "frac": achieved / peak.value, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak.value,
+                         "traffic": NCU_FORCE_TRAFFIC.get((n, tuned["mixed"]["variant"])),
+                         "traffic_unit": "bytes per launch (ncu dram read + write)",
+                         "algorithmic_bytes": 32 * n,
                          "kernel": "force_mixed_kernel", "flops_per_interaction": FLOPS_PER_INTERACTION,
                          "peak_source": "measured FFMA/FFMA2 microkernel on this GPU (gtd_measure_fma_peak)",
                          "fp64_peak": peak64.value / 1e12},
@@ -647,9 +662,12 @@ def run_adjoint(args, local):
     line = {"workload": f"adjoint KDK N={n}, {T} steps, checkpoints every {every}", "forward_ms": fwd,
             "backward_ms": bwd, "backward_over_forward": bwd / fwd, "total_over_forward": (fwd + bwd) / fwd}
     if args.adj_fd > 0:
-        # central differences of the library's own FP64 forward; h relative to the coordinate:
-        # 1e-6 for positions and velocities, 1e-4 for masses (a 1e-6 mass step moves the FP64 loss
-        # by so few ulps that the difference quotient itself has ~1e-4 roundoff error)
+        # central differences of the library's own FP64 forward, h relative to the coordinate, at
+        # two steps per group: the specified 1e-6 for positions and velocities (1e-4 for masses,
+        # whose derivatives are small next to the loss) and 10x that.  Both carry roundoff of the
+        # FP64 loss divided by h, which at the small step is ~1e-5 of the components that are small
+        # next to the largest one; the larger step divides it by ten while the truncation error
+        # stays below it (|D(h) - D(10h)| is reported as the quotients' own disagreement).
         rng = np.random.default_rng(8)
         fd_out = {}
 
@@ -665,14 +683,23 @@ def run_adjoint(args, local):
                     vals.append(float(((y - target) ** 2).sum(-1).mean()))
             return (vals[0] - vals[1]) / (2 * hs)
 
+        def summary(g, d):
+            err = np.abs(g - d)
+            rel = err / np.maximum(np.abs(d), 1e-300)
+            return {"max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
+                    "normwise_rel_err": float(err.max() / np.abs(d).max()), "within_1e-5": int((rel <= 1e-5).sum())}
+
         for which, grad, hrel in (("x", xa.grad, 1e-6), ("v", va.grad, 1e-6), ("m", ma.grad, 1e-4)):
             flat = grad.reshape(-1)
-            errs = []
+            g, d1, d2 = [], [], []
             for idx in rng.choice(flat.numel(), max(1, args.adj_fd // 3), replace=False):
-                fd = fd_at(which, idx, hrel)
-                errs.append(abs(float(flat[idx]) - fd) / max(abs(fd), 1e-300))
-            fd_out[which] = {"coords": len(errs), "h_rel": hrel, "max_rel_err": max(errs),
-                             "median_rel_err": float(np.median(errs))}
+                g.append(float(flat[idx]))
+                d1.append(fd_at(which, idx, hrel))
+                d2.append(fd_at(which, idx, 10 * hrel))
+            g, d1, d2 = np.array(g), np.array(d1), np.array(d2)
+            fd_out[which] = {"coords": len(g), f"h_rel_{hrel:g}": summary(g, d1),
+                             f"h_rel_{10 * hrel:g}": summary(g, d2),
+                             "fd_h_vs_10h_normwise": float(np.abs(d1 - d2).max() / np.abs(d2).max())}
         line["fd_check"] = fd_out
     print(json.dumps(line), flush=True)
 

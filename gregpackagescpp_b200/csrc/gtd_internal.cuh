@@ -69,6 +69,11 @@ struct StepArgs {
 ForcePlan make_plan(int64_t n, int precision, int device, int variant);
 int variant_count(int precision);
 int variant_info(int precision, int variant, int *i_per_thread, int *fold);
+// Process-wide autotune results: a handle without a pinned variant takes the variant last tuned on
+// its device for its precision and size class (the bit length of N), else default_variant.
+int default_variant(int precision, int64_t n);
+void remember_variant(int device, int precision, int64_t n, int variant);
+int tuned_variant(int device, int precision, int64_t n);
 size_t partial_bytes(const ForcePlan &p);
 // Force on every body of `src` (positions + G-free masses), written as partial sums.
 int launch_force(int precision, const ForcePlan &p, const double4 *src, double G, double *partials,

@@ -36,7 +36,8 @@ struct gtd_system {
     // direct summation
     gtd::ForcePlan plan;
     int plan_prec = -1;
-    int variant = 0;  // force-kernel variant (gtd_system_set_direct_variant / autotune)
+    int variant = 0;              // force-kernel variant in use
+    bool variant_pinned = false;  // set by gtd_system_set_direct_variant; else the process-wide choice
     double *partials = nullptr;
     size_t part_bytes = 0;
     double *escratch = nullptr;

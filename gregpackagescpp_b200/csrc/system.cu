@@ -94,6 +94,7 @@ void release_bodies(gtd_system *s) {
 }
 
 int ensure_plan(gtd_system *s) {
+    if (!s->variant_pinned) s->variant = tuned_variant(s->device, s->precision, s->n);
     if (s->plan.n == s->n && s->plan_prec == s->precision && s->plan.variant == s->variant && s->partials)
         return GTD_OK;
     s->plan = make_plan(s->n, s->precision, s->device, s->variant);
@@ -646,9 +647,9 @@ int gtd_direct_variant_info(int precision, int variant, int *i_per_thread, int *
 
 int gtd_system_set_direct_variant(gtd_system *s, int variant) {
     if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
-    if (variant < 0) variant = 0;
     if (variant >= variant_count(s->precision)) return fail(GTD_ERR_INVALID_ARGUMENT, "variant %d out of range", variant);
-    s->variant = variant;
+    s->variant_pinned = variant >= 0;
+    if (variant >= 0) s->variant = variant;
     return GTD_OK;
 }
 
@@ -659,8 +660,13 @@ int gtd_system_autotune_direct(gtd_system *s, int reps, int *best, double *best_
     if (reps < 1) reps = 1;
     int rc = maybe_reorder(s, true);
     if (rc) return rc;
-    const int prev = s->variant;
-    int arg = prev;
+    struct RestorePin {
+        gtd_system *s;
+        bool pinned;
+        ~RestorePin() { s->variant_pinned = pinned; }
+    } restore{s, s->variant_pinned};
+    s->variant_pinned = true;  // while timing, ensure_plan keeps the variant under test
+    int arg = s->variant;
     double bestv = 1e300;
     for (int v = 0; v < variant_count(s->precision); ++v) {
         s->variant = v;
@@ -687,6 +693,8 @@ int gtd_system_autotune_direct(gtd_system *s, int reps, int *best, double *best_
         }
     }
     s->variant = arg;
+    remember_variant(s->device, s->precision, s->n, arg);
+    s->variant_pinned = restore.pinned;
     rc = ensure_plan(s);
     if (rc) return rc;
     if (best) *best = arg;

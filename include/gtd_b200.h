@@ -138,9 +138,12 @@ GTD_API int gtd_system_stream(const gtd_system *sys, void **stream);
 GTD_API int gtd_system_time_force_kernels(gtd_system *sys, int enable);
 GTD_API int gtd_system_force_timing(gtd_system *sys, double *total_ms, uint64_t *launches, int reset);
 /* Force-kernel variants (i-bodies per thread; for GTD_PREC_MIXED also the j-bodies summed in FP32
- * between FP64 folds).  Variant 0 is the default.  gtd_system_autotune_direct times every variant
- * on the handle's current bodies (a warm-up and `reps` timed force launches each, median) and keeps
- * the fastest for the handle; it leaves the bodies untouched apart from their order on the device. */
+ * between FP64 folds).  gtd_system_autotune_direct times every variant on the handle's current
+ * bodies (a warm-up and `reps` timed force launches each, median), keeps the fastest for the handle
+ * and remembers it for the process: every handle without a pinned variant on the same device, with
+ * the same precision and an N of the same bit length, then uses it (untuned: a fixed choice by
+ * precision and N).  It leaves the bodies untouched apart from their order on the device.
+ * gtd_system_set_direct_variant pins a variant for the handle; variant < 0 unpins it. */
 GTD_API int gtd_direct_variant_count(int precision, int *count);
 GTD_API int gtd_direct_variant_info(int precision, int variant, int *i_per_thread, int *fold);
 GTD_API int gtd_system_set_direct_variant(gtd_system *sys, int variant);

@@ -78,10 +78,11 @@ def test_adjoint_vs_central_differences(gpu):
     loss_of(xa, va, ma).backward()
     rng = np.random.default_rng(7)
     checks = 0
-    # h = 1e-6 relative for positions and velocities.  For masses a 1e-6 relative step moves the
-    # FP64 loss by only ~1e5 ulps, so the central difference itself carries ~1e-4 roundoff error;
-    # 1e-4 relative keeps its truncation and roundoff errors below 1e-5.
-    for which, base, grad, hrel in (("x", x, xa.grad, 1e-6), ("v", v, va.grad, 1e-6), ("m", m, ma.grad, 1e-4)):
+    # h = 1e-6 relative for positions and velocities.  The mass derivatives are small next to the
+    # FP64 loss, so their central differences are roundoff-bound: on this problem (checked with an
+    # exact-autograd FP64 forward) the error relative to max|grad| is ~1e-7 at h = 1e-4 and ~5e-9 at
+    # h = 1e-3, with the truncation error still below that; masses use 1e-3 relative.
+    for which, base, grad, hrel in (("x", x, xa.grad, 1e-6), ("v", v, va.grad, 1e-6), ("m", m, ma.grad, 1e-3)):
         flat = base.reshape(-1)
         for idx in rng.choice(flat.numel(), 6, replace=False):
             hstep = hrel * abs(float(flat[idx]))

@@ -87,3 +87,52 @@ def test_mixed_kdk_tracks_fp64(gpu):
     b.evolve(16)
     assert rel_err(b.x, a.x) < 1e-9
     assert rel_err(b.v, a.v) < 1e-6
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+def test_every_force_variant(gpu, prec):
+    """Each force-kernel variant, pinned on the handle, against the FP64 default (FP64 variants to
+    1e-13 relative, mixed ones to the mixed bar of 1e-6 RMS), on a ragged N."""
+    import ctypes as C
+
+    from gregpackagescpp_b200 import _lib
+    L = _lib.load()
+    m, x, v = plummer(3001, 23)
+    want = System(m, x, v, units_format=UNITS_G6674).accelerations()
+    p = _lib.PREC_MIXED if prec == "mixed" else _lib.PREC_F64
+    count = C.c_int()
+    _lib.check(L.gtd_direct_variant_count(p, C.byref(count)))
+    assert count.value >= 1
+    s = System(m, x, v, units_format=UNITS_G6674, precision=prec)
+    for var in range(count.value):
+        _lib.check(L.gtd_system_set_direct_variant(s._h, var))
+        got = s.accelerations()
+        rel = np.linalg.norm(got - want, axis=1) / np.linalg.norm(want, axis=1)
+        if prec == "f64":
+            assert rel.max() < 1e-13, (var, float(rel.max()))
+        else:
+            assert np.sqrt((rel ** 2).mean()) < 1e-6, (var, float(np.sqrt((rel ** 2).mean())))
+    assert L.gtd_system_set_direct_variant(s._h, count.value) == _lib.ERR_INVALID_ARGUMENT
+
+
+def test_autotune_result_reaches_other_handles(gpu):
+    """gtd_system_autotune_direct remembers its choice for the process: a new handle of the same
+    precision and size class computes bit-identically to a handle pinned to that variant, and so
+    does a pinned handle after unpinning."""
+    import ctypes as C
+
+    from gregpackagescpp_b200 import _lib
+    L = _lib.load()
+    m, x, v = plummer(5000, 24)
+    a = System(m, x, v, units_format=UNITS_G6674, precision="mixed")
+    a.accelerations()  # uploads the bodies
+    best = C.c_int()
+    _lib.check(L.gtd_system_autotune_direct(a._h, 1, C.byref(best), None))
+    pinned = System(m, x, v, units_format=UNITS_G6674, precision="mixed")
+    _lib.check(L.gtd_system_set_direct_variant(pinned._h, best.value))
+    fresh = System(m, x, v, units_format=UNITS_G6674, precision="mixed")
+    assert np.array_equal(fresh.accelerations(), pinned.accelerations())
+    other = (best.value + 1) % 9
+    _lib.check(L.gtd_system_set_direct_variant(pinned._h, other))
+    _lib.check(L.gtd_system_set_direct_variant(pinned._h, -1))  # unpinned: back to the tuned variant
+    assert np.array_equal(fresh.accelerations(), pinned.accelerations())
