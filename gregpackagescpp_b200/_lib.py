@@ -33,6 +33,10 @@ PREC_MIXED = 1
 NO_COLL, OVERLAP_COLL, MERGE_COLL = 0, 3, 4
 
 
+ERR_NSYS_LOAD = 13
+ERR_NSYS_FORMAT = 14
+
+
 class GtdError(RuntimeError):
     """A non-zero status from the C ABI; ``code`` is the GTD_ERR_* value."""
 
@@ -65,12 +69,22 @@ class IndistinguishableBodies(BarnesHutError):
     """gtd::indistinguishable_bodies (greg8tree.hpp:32-46)."""
 
 
+class NsysLoadError(NbodyError):
+    """gtd::nsys_load_error (gregsys.hpp:125-129)."""
+
+
+class NsysFormatError(NsysLoadError):
+    """gtd::nsys_format_error (gregsys.hpp:130-134)."""
+
+
 _EXC = {
     ERR_INVALID_ARGUMENT: ValueError,
     ERR_OVERLAPPING_BODIES: OverlappingBodiesError,
     ERR_TWO_BODY: TwoBodyError,
     ERR_INVALID_BODY_PLACEMENT: InvalidBodyPlacement,
     ERR_INDISTINGUISHABLE: IndistinguishableBodies,
+    ERR_NSYS_LOAD: NsysLoadError,
+    ERR_NSYS_FORMAT: NsysFormatError,
 }
 
 _lib = None
@@ -130,6 +144,10 @@ def load():
     L.gtd_bh_tree_size.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), dp]
     L.gtd_bh_tree_download.argtypes = [vp] + [dp] * 10
     L.gtd_bh_accelerations.argtypes = [vp, dp, dp]
+    L.gtd_nsys_chunk_size.argtypes = [ip, ip, ip, C.POINTER(C.c_int)]
+    L.gtd_system_to_nsys.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, dp, ip, ip, ip, C.POINTER(i64)]
+    L.gtd_system_load_nsys.argtypes = [vp, C.c_char_p, ip, ip, ip, ip, C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double), dp, C.POINTER(C.c_double)]
     for name in exported_symbols():
         if name != "gtd_last_error":
             getattr(L, name).restype = C.c_int

@@ -70,8 +70,10 @@ __device__ __forceinline__ bool cand_less(const Cand &a, const Cand &b) {
 }
 
 // One thread: heap sort of the candidates by (o, dist, i), then the sequential s_coll response.
-__global__ void restitution_kernel(Cand *cand, const int *count, int cap, const double4 *pm, const double *rest,
-                                   double4 *vel, int *status) {
+// With perm != nullptr the candidates hold Barnes-Hut slots (the order of the reference's leaf and
+// neighbour iteration) and perm maps them to bodies.
+__global__ void restitution_kernel(Cand *cand, const int *count, int cap, const int32_t *perm, const double4 *pm,
+                                   const double *rest, double4 *vel, int *status) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     int c = *count;
     if (c > cap) {
@@ -102,15 +104,17 @@ __global__ void restitution_kernel(Cand *cand, const int *count, int cap, const 
             root = child;
         }
     }
+    auto body = [&](int32_t q) { return perm ? perm[q] : q; };
     int g = 0;
     while (g < c) {
-        const int o = cand[g].o;
+        const int og = cand[g].o;
+        const int o = body(og);
         int e = g;
-        while (e < c && cand[e].o == o) ++e;
+        while (e < c && cand[e].o == og) ++e;
         // momenta along r12 snapshotted for the whole group before any update (gregsys.hpp:740-742)
         const double4 xo = pm[o];
         for (int k = g; k < e; ++k) {
-            const int i = cand[k].i;
+            const int i = body(cand[k].i);
             const double4 xi = pm[i];
             const double d = cand[k].dist;
             const double ux = (xi.x - xo.x) / d, uy = (xi.y - xo.y) / d, uz = (xi.z - xo.z) / d;
@@ -126,7 +130,7 @@ __global__ void restitution_kernel(Cand *cand, const int *count, int cap, const 
             const double d = cand[k].dist;
             if (k > g && d == prev) continue;  // std::map::emplace keeps the first equal key
             prev = d;
-            const int i = cand[k].i;
+            const int i = body(cand[k].i);
             const double4 xi = pm[i];
             const double ux = (xi.x - xo.x) / d, uy = (xi.y - xo.y) / d, uz = (xi.z - xo.z) / d;
             const double2 pp = reinterpret_cast<double2 *>(cand + cap)[k];
@@ -149,6 +153,93 @@ __global__ void restitution_kernel(Cand *cand, const int *count, int cap, const 
             }
         }
         g = e;
+    }
+}
+
+// ---- Barnes-Hut path: bh_s_coll (gregsys.hpp:631-688) ----------------------------------------
+// Bounds of every node's cell: the set_corners splits (greg8tree.hpp:81-131) of the root box along
+// the node's code prefix, in T (float trees round every midpoint to float).
+template <bool F>
+__global__ void node_box_kernel(int64_t n_nodes, const unsigned long long *codes, const int32_t *first,
+                                const int8_t *depth, const double *box, double *nbox) {
+    const int64_t nd = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (nd >= n_nodes) return;
+    const unsigned long long c = codes[first[nd]];
+    double lo[3], hi[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = box[k];
+        hi[k] = box[3 + k];
+    }
+    const int dl = depth[nd];
+    for (int l = 0; l < dl; ++l) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double mid = F ? (double)__fmul_rn(__fadd_rn((float)lo[k], (float)hi[k]), 0.5f)
+                                 : __dmul_rn(__dadd_rn(lo[k], hi[k]), 0.5);
+            if ((c >> (3 * (20 - l) + k)) & 1ull) lo[k] = mid;
+            else hi[k] = mid;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        nbox[6 * nd + k] = lo[k];
+        nbox[6 * nd + 3 + k] = hi[k];
+    }
+}
+
+// One thread per slot a: the nn_iterator neighbours of a's leaf (greg8tree.hpp:615-701: depth-first
+// from the root's children, descending only into cells that touch the leaf's cell, closed-interval
+// test of :624-628, the own leaf skipped), keeping the bodies that overlap a's body.  A depth-21
+// bucket leaf counts its other bodies as neighbours.  Candidates are (slot a, slot q, distance).
+__global__ void __launch_bounds__(kCT) bh_touch_pairs_kernel(int64_t n, int64_t n_nodes, const int32_t *own,
+                                                             const int32_t *perm, const int8_t *leaf,
+                                                             const int32_t *first, const int32_t *count,
+                                                             const int32_t *skip, const double *nbox,
+                                                             const double4 *pm, const double *rad, Cand *cand,
+                                                             int *cand_count, int cap) {
+    const int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    const int32_t L = own[a];
+    const int32_t o = perm[a];
+    const double4 po = pm[o];
+    const double ro = rad[o];
+    const double bx0 = nbox[6 * L], by0 = nbox[6 * L + 1], bz0 = nbox[6 * L + 2];
+    const double bx1 = nbox[6 * L + 3], by1 = nbox[6 * L + 4], bz1 = nbox[6 * L + 5];
+    int64_t k = 1;
+    while (k < n_nodes) {
+        bool take;
+        if (k == L) {
+            take = count[k] > 1;
+        } else {
+            const double *C = nbox + 6 * k;
+            const bool touch = !(bx1 < C[0] || bx0 > C[3] || by1 < C[1] || by0 > C[4] || bz1 < C[2] || bz0 > C[5]);
+            if (!touch) {
+                k = skip[k];
+                continue;
+            }
+            if (!leaf[k]) {
+                ++k;
+                continue;
+            }
+            take = true;
+        }
+        if (take) {
+            const int32_t q0 = first[k], q1 = first[k] + count[k];
+            for (int32_t q = q0; q < q1; ++q) {
+                if (q == a) continue;
+                const int32_t i = perm[q];
+                const double4 pi = pm[i];
+                const double dx = __dsub_rn(pi.x, po.x), dy = __dsub_rn(pi.y, po.y), dz = __dsub_rn(pi.z, po.z);
+                const double d =
+                    sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+                if (__dadd_rn(ro, rad[i]) > d) {
+                    const int slot = atomicAdd(cand_count, 1);
+                    if (slot < cap) cand[slot] = Cand{(int32_t)a, q, d};
+                }
+            }
+        }
+        k = skip[k];
     }
 }
 
@@ -259,6 +350,9 @@ void release_collide(gtd_system *s) {
     cudaFree(s->coll_buf);
     s->coll_buf = nullptr;
     s->coll_bytes = 0;
+    cudaFree(s->coll_nbox);
+    s->coll_nbox = nullptr;
+    s->coll_nbox_cap = 0;
 }
 
 static int ensure_coll(gtd_system *s) {
@@ -335,7 +429,8 @@ int run_collisions(gtd_system *s) {
     overlap_pairs_kernel<<<(unsigned)((s->n + kCT - 1) / kCT), kCT, 0, st>>>(s->n, s->pm[s->cur], s->rad, p.cand,
                                                                            p.count, kMaxCand);
     GTD_CHECK_LAUNCH();
-    restitution_kernel<<<1, 32, 0, st>>>(p.cand, p.count, kMaxCand, s->pm[s->cur], s->rest, s->vel, p.status);
+    restitution_kernel<<<1, 32, 0, st>>>(p.cand, p.count, kMaxCand, nullptr, s->pm[s->cur], s->rest, s->vel,
+                                         p.status);
     GTD_CHECK_LAUNCH();
     s->launches += 2;
     int host[2] = {0, 0};
@@ -343,6 +438,45 @@ int run_collisions(gtd_system *s) {
     GTD_CUDA(cudaStreamSynchronize(st));
     if (host[1] == GTD_ERR_CAPACITY)
         return fail(GTD_ERR_CAPACITY, "%d overlapping pairs in one step exceed the %d the collision pass holds",
+                    host[0], kMaxCand);
+    return GTD_OK;
+}
+
+// bh_s_coll after a Barnes-Hut kick, on the tree of the current positions (gregsys.hpp:2936-2938).
+int run_bh_collisions(gtd_system *s) {
+    if (s->n < 2 || !s->tree_valid) return GTD_OK;
+    int rc = ensure_coll(s);
+    if (rc) return rc;
+    const int64_t nn = s->n_nodes;
+    if (nn > s->coll_nbox_cap) {
+        cudaFree(s->coll_nbox);
+        s->coll_nbox = nullptr;
+        s->coll_nbox_cap = 0;
+        GTD_CUDA(cudaMalloc(&s->coll_nbox, sizeof(double) * 6 * (size_t)nn));
+        s->coll_nbox_cap = nn;
+    }
+    CollPtrs p = coll_ptrs(s);
+    cudaStream_t st = s->stream;
+    GTD_CUDA(cudaMemsetAsync(p.count, 0, 64, st));
+    const unsigned gn = (unsigned)((nn + kCT - 1) / kCT), gb = (unsigned)((s->n + kCT - 1) / kCT);
+    if (s->tree_float)
+        node_box_kernel<true><<<gn, kCT, 0, st>>>(nn, s->codes, s->nfirst, s->ndepth, s->box_dev, s->coll_nbox);
+    else
+        node_box_kernel<false><<<gn, kCT, 0, st>>>(nn, s->codes, s->nfirst, s->ndepth, s->box_dev, s->coll_nbox);
+    GTD_CHECK_LAUNCH();
+    bh_touch_pairs_kernel<<<gb, kCT, 0, st>>>(s->n, nn, s->own_leaf, s->perm, s->nleaf, s->nfirst, s->ncount,
+                                              s->nskip, s->coll_nbox, s->pm[s->cur], s->rad, p.cand, p.count,
+                                              kMaxCand);
+    GTD_CHECK_LAUNCH();
+    restitution_kernel<<<1, 32, 0, st>>>(p.cand, p.count, kMaxCand, s->perm, s->pm[s->cur], s->rest, s->vel,
+                                         p.status);
+    GTD_CHECK_LAUNCH();
+    s->launches += 3;
+    int host[2] = {0, 0};
+    GTD_CUDA(cudaMemcpyAsync(host, p.count, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    GTD_CUDA(cudaStreamSynchronize(st));
+    if (host[1] == GTD_ERR_CAPACITY)
+        return fail(GTD_ERR_CAPACITY, "%d overlapping neighbour pairs in one step exceed the %d the collision pass holds",
                     host[0], kMaxCand);
     return GTD_OK;
 }

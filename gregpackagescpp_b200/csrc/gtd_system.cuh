@@ -100,10 +100,32 @@ struct gtd_system {
     // collisions (collide.cu)
     void *coll_buf = nullptr;
     size_t coll_bytes = 0;
+    double *coll_nbox = nullptr;  // Barnes-Hut cell bounds, 6 per node (bh_s_coll)
+    int64_t coll_nbox_cap = 0;
+
+    // .nsys chunk staging (nsys.cu)
+    void *nsys_dev = nullptr, *nsys_host = nullptr;
+    size_t nsys_dev_bytes = 0, nsys_host_bytes = 0;
+};
+
+// Makes the handle's device current for the scope of an entry point.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        cudaGetDevice(&now);
+        if (prev >= 0 && now != prev) cudaSetDevice(prev);
+    }
 };
 
 void release_bodies(gtd_system *s);
 void release_tree(gtd_system *s);
+// bh_s_coll on the current tree (collide.cu); the tree must have been built at the current positions
+int run_bh_collisions(gtd_system *s);
 int reorder_bodies(gtd_system *s);
 int restore_upload_order(gtd_system *s);
 // row[s] = host row of device slot s: ascending upload index among the live bodies
@@ -111,5 +133,8 @@ int output_rows(gtd_system *s, std::vector<int64_t> &row);
 // device accelerations -> host triples in host row order (synchronises the stream)
 int copy_acc_out(gtd_system *s, double *a3);
 void release_collide(gtd_system *s);
+void release_nsys(gtd_system *s);
+int ensure_body_capacity(gtd_system *s, int64_t n);
+int set_loaded_bodies(gtd_system *s, int64_t n);
 int ensure_plan(gtd_system *s);
 int force_and_integrate(gtd_system *s, const double4 *src, int epi, const gtd::StepArgs &st);

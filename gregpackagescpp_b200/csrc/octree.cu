@@ -767,6 +767,10 @@ int bh_evolve_kdk(gtd_system *s, uint64_t steps) {
         if (rc) return rc;
         rc = bh_walk_impl(s, s->dt, true);
         if (rc) return rc;
+        if (s->coll != GTD_NO_COLL) {
+            rc = run_bh_collisions(s);
+            if (rc) return rc;
+        }
     }
     return GTD_OK;
 }

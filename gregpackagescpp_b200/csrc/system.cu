@@ -61,6 +61,21 @@ static int ensure_capacity(gtd_system *s, int64_t n) {
     return GTD_OK;
 }
 
+int ensure_body_capacity(gtd_system *s, int64_t n) { return ensure_capacity(s, n); }
+
+// State after n bodies were written straight into the device arrays in upload order.
+int set_loaded_bodies(gtd_system *s, int64_t n) {
+    s->n = n;
+    s->n_uploaded = n;
+    s->cur = 0;
+    s->begun = false;
+    s->synced = true;
+    s->tree_valid = false;
+    s->ordered = false;
+    s->steps_since_reorder = 0;
+    return GTD_OK;
+}
+
 void release_bodies(gtd_system *s) {
     cudaFree(s->pm[0]);
     cudaFree(s->pm[1]);
@@ -253,19 +268,6 @@ static int select_branch(int method) {
     return 0;
 }
 
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int d) {
-        cudaGetDevice(&prev);
-        if (prev != d) cudaSetDevice(d);
-    }
-    ~DeviceGuard() {
-        int now = -1;
-        cudaGetDevice(&now);
-        if (prev >= 0 && now != prev) cudaSetDevice(prev);
-    }
-};
-
 int run_collisions(gtd_system *s);  // collide.cu
 int bh_evolve_kdk(gtd_system *s, uint64_t steps);  // octree.cu
 int bh_accelerations(gtd_system *s, double *a3, uint32_t *n_inter);  // octree.cu
@@ -389,6 +391,7 @@ int gtd_system_destroy(gtd_system *s) {
     release_bodies(s);
     release_tree(s);
     release_collide(s);
+    release_nsys(s);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     cudaEventDestroy(s->ev0);
     cudaEventDestroy(s->ev1);

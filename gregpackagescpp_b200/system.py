@@ -23,6 +23,16 @@ _UNITS_RE = re.compile(
     r"(?=\d{1,18}\s*$)\d*[1-9]+\d*\s*$")
 
 
+def units_values(units: str) -> tuple:
+    """The six numbers of a units format "Ma:b,Dc:d,Tx:y" in the order the reference keeps them
+    (G_vals, gregsys.hpp:275-280) and writes them to .nsys headers: (m_num=b, m_denom=a, d_num=c,
+    d_denom=d, t_num=y, t_denom=x)."""
+    parse_units(units)
+    s = units.strip("MmDdTt ").replace(" ", "")
+    m_den, m_num, d_num, d_den, t_den, t_num = [int(x) for x in re.findall(r"\d+", s)]
+    return (m_num, m_den, d_num, d_den, t_num, t_den)
+
+
 def parse_units(units: str) -> float:
     """G for a units format "Ma:b,Dc:d,Tx:y" (gregsys.hpp:245-282): a = mass denominator,
     b = mass numerator, c/d = distance numerator/denominator, x/y = time denominator/numerator;
@@ -78,6 +88,7 @@ class System:
         self.dt = float(timestep)
         self.iterations = int(num_iterations)
         self.G = parse_units(units_format)
+        self.g_vals = units_values(units_format)
         self.eps = 0.0
         self.theta = PI / 3
         self.collisions = collisions
@@ -136,6 +147,47 @@ class System:
 
     def set_G_units(self, units_format: str) -> None:
         self.G = parse_units(units_format)
+        self.g_vals = units_values(units_format)
+
+    # ---- .nsys snapshots (gregsys.hpp:943-1400, 3214-3258) ------------------------------------
+    _SIZES = {"float": 4, "double": 8, "long double": 16}
+
+    def to_nsys(self, path: str | None, M: str = "double", R: str = "double", T: str = "double") -> int:
+        """system::to_nsys: writes the bodies as a .nsys file with the chunk layout of the given
+        M, R, T types ("float", "double" or "long double"); returns the bytes written (0 when path
+        is None or the file cannot be opened)."""
+        if path is None:
+            return 0
+        self._push()
+        nb = C.c_int64()
+        gv = np.array(self.g_vals, dtype=np.uint64)
+        check(self._L.gtd_system_to_nsys(self._h, str(path).encode(), self.time_elapsed, self.dt,
+                                         gv.ctypes.data, self._SIZES[M], self._SIZES[R], self._SIZES[T],
+                                         C.byref(nb)))
+        return nb.value
+
+    @classmethod
+    def from_nsys(cls, path: str, alloc_chunks: bool = True, check_nan_inf: bool = True,
+                  allow_overlapping_bodies: bool = True, M: str = "double", R: str = "double", T: str = "double",
+                  precision: str = "f64", device: int = 0) -> "System":
+        """The system(const char *nsys_path, alloc_chunks, check_nan_inf, allow_overlapping_bodies)
+        constructor.  alloc_chunks only chose between two host read strategies in the reference;
+        here the chunks always travel in one copy and are unpacked on the device."""
+        if path is None:
+            raise ValueError("nullptr passed as .nsys file path.\n")
+        s = cls(precision=precision, device=device)
+        te, dt, G = C.c_double(), C.c_double(), C.c_double()
+        gv = np.zeros(6, dtype=np.uint64)
+        check(s._L.gtd_system_load_nsys(s._h, str(path).encode(), 1 if check_nan_inf else 0, cls._SIZES[M],
+                                        cls._SIZES[R], cls._SIZES[T], C.byref(te), C.byref(dt), gv.ctypes.data,
+                                        C.byref(G)))
+        s.time_elapsed, s.dt, s.G = te.value, dt.value, G.value
+        s.g_vals = tuple(int(g) for g in gv)
+        s._pull()
+        s.allow_overlap = allow_overlapping_bodies
+        if not allow_overlapping_bodies:
+            s.check_overlap()
+        return s
 
     def set_softening(self, epsilon: float) -> bool:
         # the reference rejects eps < sqrt(LDBL_MIN) (~1.8e-2466): for a double that is eps <= 0

@@ -67,6 +67,17 @@ class indistinguishable_bodies : public barnes_hut_error {
 public:
     using barnes_hut_error::barnes_hut_error;
 };
+class nsys_load_error : public nbody_error {  // gregsys.hpp:125-129
+public:
+    nsys_load_error() : nbody_error{"Error loading N-body data from .nsys file.\n"} {}
+    explicit nsys_load_error(const char *msg) : nbody_error{msg} {}
+};
+class nsys_format_error : public nsys_load_error {  // gregsys.hpp:130-134
+public:
+    nsys_format_error() : nsys_load_error{"Error loading N-body data from .nsys file.\n"} {}
+    explicit nsys_format_error(const char *msg) : nsys_load_error{msg} {}
+};
+
 // a CUDA / resource failure of the engine itself (no counterpart: the reference runs on the host)
 class device_error : public std::runtime_error {
 public:
@@ -83,6 +94,8 @@ inline void throw_status(int rc) {
         case GTD_ERR_INVALID_BODY_PLACEMENT: throw invalid_body_placement{m};
         case GTD_ERR_INDISTINGUISHABLE: throw indistinguishable_bodies{m};
         case GTD_ERR_TWO_BODY: throw two_body_error{m};
+        case GTD_ERR_NSYS_LOAD: throw nsys_load_error{m};
+        case GTD_ERR_NSYS_FORMAT: throw nsys_format_error{m};
         default: throw device_error{m};
     }
 }

@@ -5,7 +5,9 @@
 //
 // Differences, all documented in the engine: no long double arithmetic on the device (FP64 is used
 // for every T); trajectory recording (memFreq), file output (fileFreq) and progress printing are
-// not performed; evolve-time merges use check_overlap's scan as that routine intends.
+// not performed; evolve-time merges use check_overlap's scan as that routine intends.  .nsys files
+// (to_nsys and the path constructor) are written and read by the engine, for floating-point M, R
+// and T.
 #ifndef GTD_B200_GREGSYS_HPP
 #define GTD_B200_GREGSYS_HPP
 
@@ -14,6 +16,8 @@
 #include <cstring>
 #include <functional>
 #include <initializer_list>
+#include <ios>
+#include <type_traits>
 #include <regex>
 #include <string>
 #include <vector>
@@ -52,6 +56,7 @@ private:
     long double eps = 0, dt = 1, bh_theta = 3.14159265358979323846L / 3;
     uint64_t iterations = 1'000;
     long double time_elapsed{};
+    uint64_t G_vals[6] = {1, 1, 1, 1, 1, 1};  // m_num, m_denom, d_num, d_denom, t_num, t_denom
     bool mixed = false;
     gtd_system *dev = nullptr;
     int device = 0;
@@ -67,6 +72,8 @@ private:
         for (std::sregex_iterator it{str.begin(), str.end(), digits}, end; it != end && k < 6; ++it)
             v[k++] = std::stoull(it->str());
         const uint64_t m_den = v[0], m_num = v[1], d_num = v[2], d_den = v[3], t_den = v[4], t_num = v[5];
+        const uint64_t gv[6] = {m_num, m_den, d_num, d_den, t_num, t_den};  // gregsys.hpp:275-280
+        std::memcpy(G_vals, gv, sizeof gv);
         G = 66'743;
         G *= m_num * d_num * d_num * d_num * t_num * t_num;
         G /= m_den * d_den * d_den * d_den * t_den * t_den;
@@ -139,8 +146,37 @@ public:
         parse_units_format(units_format);
     }
     system(const std::initializer_list<bod_t> &list) : bods{list}, G{G_SI} { check_overlap(); }
+    // gregsys.hpp:1479-1490: the bodies, time, time-step and units of a .nsys file.  alloc_chunks
+    // chose between two host read strategies in the reference; the engine always reads the chunks in
+    // one piece and unpacks them on the device.
+    explicit system(const char *nsys_path, bool alloc_chunks = true, bool check_nan_inf = true,
+                    bool allow_overlapping_bodies = true) {
+        static_assert(std::is_floating_point_v<M> && std::is_floating_point_v<R> && std::is_floating_point_v<T>,
+                      "the engine reads .nsys files with floating-point M, R and T");
+        (void)alloc_chunks;
+        if (nsys_path == nullptr) throw std::invalid_argument{"nullptr passed as .nsys file path.\n"};
+        ensure_device();
+        double t_el = 0, step = 0, g = 0;
+        throw_status(gtd_system_load_nsys(dev, nsys_path, check_nan_inf ? 1 : 0, (int)sizeof(M), (int)sizeof(R),
+                                          (int)sizeof(T), &t_el, &step, G_vals, &g));
+        time_elapsed = t_el;
+        dt = step;
+        G = g;
+        int64_t n = 0;
+        throw_status(gtd_system_num_bodies(dev, &n));
+        std::vector<double> m(n), r(n), e(n), x(3 * n), v(3 * n);
+        throw_status(gtd_system_download(dev, &n, m.data(), r.data(), e.data(), x.data(), v.data(), nullptr));
+        bods.reserve((size_t)n);
+        for (int64_t i = 0; i < n; ++i)
+            bods.emplace_back((M)m[i], (R)r[i], (T)x[3 * i], (T)x[3 * i + 1], (T)x[3 * i + 2], (T)v[3 * i],
+                              (T)v[3 * i + 1], (T)v[3 * i + 2], (long double)e[i]);
+        if (!allow_overlapping_bodies) check_overlap();
+    }
     system(const system &other) : bods{other.bods}, G{other.G}, eps{other.eps}, dt{other.dt},
-                                  bh_theta{other.bh_theta}, iterations{other.iterations}, mixed{other.mixed} {}
+                                  bh_theta{other.bh_theta}, iterations{other.iterations},
+                                  time_elapsed{other.time_elapsed}, mixed{other.mixed} {
+        std::memcpy(G_vals, other.G_vals, sizeof G_vals);
+    }
     system &operator=(const system &) = delete;
     ~system() { gtd_system_destroy(dev); }
 
@@ -151,6 +187,20 @@ public:
         int32_t pair[2] = {0, 0};
         throw_status(gtd_system_check_overlap(dev, mergeOverlappingBodies ? 1 : 0, pair));
         if constexpr (mergeOverlappingBodies) pull();
+    }
+
+    // ---- .nsys output (gregsys.hpp:3214-3258): returns the bytes written, 0 for a NULL path or a
+    // file that cannot be opened ----------------------------------------------------------------------
+    std::streamoff to_nsys(const char *path) const {
+        static_assert(std::is_floating_point_v<M> && std::is_floating_point_v<R> && std::is_floating_point_v<T>,
+                      "the engine writes .nsys files with floating-point M, R and T");
+        if (path == nullptr) return 0;
+        auto *self = const_cast<system *>(this);
+        self->push();
+        int64_t bytes = 0;
+        throw_status(gtd_system_to_nsys(dev, path, (double)time_elapsed, (double)dt, G_vals, (int)sizeof(M),
+                                        (int)sizeof(R), (int)sizeof(T), &bytes));
+        return (std::streamoff)bytes;
     }
 
     // ---- accessors and setters (gregsys.hpp:1627-1672) ------------------------------------------

@@ -40,6 +40,8 @@ extern "C" {
 #define GTD_ERR_NO_DEVICE 10
 #define GTD_ERR_CAPACITY 11               /* a size beyond what the entry point supports */
 #define GTD_ERR_UNSUPPORTED 12            /* a method the reference leaves empty (rk4, rk3_8, ...) */
+#define GTD_ERR_NSYS_LOAD 13              /* gtd::nsys_load_error (gregsys.hpp:125-129) */
+#define GTD_ERR_NSYS_FORMAT 14            /* gtd::nsys_format_error (gregsys.hpp:130-134) */
 
 /* ---- integration-method flags, identical to gtd::system's (gregsys.hpp:156-165) ------------- */
 #define GTD_TWO_BODY 1
@@ -103,6 +105,31 @@ GTD_API int gtd_system_num_bodies(const gtd_system *sys, int64_t *n);
 /* Upload indices of the current bodies in download order (ascending): after merges, which of the
  * uploaded bodies survived (their state holds the merged result). */
 GTD_API int gtd_system_survivors(gtd_system *sys, int64_t *upload_index);
+
+/* ---- .nsys snapshots -------------------------------------------------------------------------
+ * The reference's on-disk format (header gregsys.hpp:1444-1466, chunk :1467-1477): a 96-byte
+ * header, then per body { char r_coeff[16]; M mass; R radius; T x, y, z, vx, vy, vz; } with natural
+ * alignment, then zero padding to a multiple of 4 bytes.  m_size/r_size/t_size are sizeof(M),
+ * sizeof(R), sizeof(T) of the caller's floating-point types: 4 (float), 8 (double) or 16 (x86-64
+ * long double, 80-bit extended); integral M/R/T return GTD_ERR_UNSUPPORTED.  The chunks are packed
+ * and unpacked on the device; the file holds the bodies in download order.
+ * gtd_nsys_chunk_size: sizeof(nsys_chunk) for those sizes. */
+GTD_API int gtd_nsys_chunk_size(int m_size, int r_size, int t_size, int *chunk_bytes);
+/* Replaces system::to_nsys (gregsys.hpp:3214-3258).  time_elapsed and dt are stored as long
+ * double, g_vals are the six unsigned numbers of the units format (m_num, m_denom, d_num, d_denom,
+ * t_num, t_denom).  *bytes_written receives the file size, or 0 (with GTD_OK) when path is NULL or
+ * the file cannot be opened, as the reference returns 0. */
+GTD_API int gtd_system_to_nsys(gtd_system *sys, const char *path, double time_elapsed, double dt,
+                               const uint64_t *g_vals, int m_size, int r_size, int t_size, int64_t *bytes_written);
+/* Replaces the system(const char *nsys_path, ...) constructor's load_from_nsys (gregsys.hpp:947-1400):
+ * the same checks in the same order with the same messages (GTD_ERR_NSYS_LOAD / GTD_ERR_NSYS_FORMAT
+ * for nsys_load_error / nsys_format_error; GTD_ERR_INVALID_ARGUMENT for a non-positive time-step),
+ * then the bodies replace the handle's (upload order = file order).  check_nan_inf scans every field
+ * (on the device) and names the first offending chunk and field.  Long doubles are rounded to
+ * double.  Outputs (any may be NULL): the stored time and time-step, the six units numbers, and G
+ * computed from them as the reference does (gregsys.hpp:1281-1284). */
+GTD_API int gtd_system_load_nsys(gtd_system *sys, const char *path, int check_nan_inf, int m_size, int r_size,
+                                 int t_size, double *time_elapsed, double *dt, uint64_t *g_vals, double *G);
 
 /* gtd::system::evolve(method) with no callbacks (gregsys.hpp:2593-3071): `iterations` steps of
  * the method on the device, one upload/download around it done by the caller.  *elapsed_ns is

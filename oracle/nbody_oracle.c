@@ -63,7 +63,8 @@ static void axpy_ld(double *x, ld s, const double *y) {
 }
 
 typedef struct {
-    int inner;
+    int inner; /* position in the iteration order that generated the candidate (ties) */
+    int body;  /* body index */
     ld dist;
     double mom_o, mom_i;
     double ux, uy, uz;
@@ -75,6 +76,8 @@ static int cand_cmp(const void *a, const void *b) {
     if (p->dist > q->dist) return 1;
     return (p->inner > q->inner) - (p->inner < q->inner);
 }
+
+static void resolve_group(int o, coll_cand *c, int nc, const double *m, const double *rest, double *v3);
 
 /* s_coll without GREGSYS_MERGERS, gregsys.hpp:690-914.  For each outer body, the overlapping
  * later bodies are keyed by their long-double distance in a std::map (first insertion wins on an
@@ -99,6 +102,7 @@ void orc_s_coll(int n, const double *m, const double *r, const double *rest, con
                 double po = mox * ux + moy * uy + moz * uz;
                 double pi = mix * ux + miy * uy + miz * uz;
                 c[nc].inner = i;
+                c[nc].body = i;
                 c[nc].dist = dist;
                 c[nc].mom_o = po;
                 c[nc].mom_i = pi;
@@ -109,34 +113,40 @@ void orc_s_coll(int n, const double *m, const double *r, const double *rest, con
             }
         }
         if (!nc) continue;
-        qsort(c, (size_t)nc, sizeof(coll_cand), cand_cmp);
-        for (int k = 0; k < nc; ++k) {
-            if (k > 0 && c[k].dist == c[k - 1].dist) continue; /* std::map::emplace keeps the first key */
-            int i = c[k].inner;
-            double o_vel = c[k].mom_o / m[o];
-            double i_vel = c[k].mom_i / m[i];
-            double o_minus_i = o_vel - i_vel;
-            ld avg_rest = ((ld)rest[o] + (ld)rest[i]) / 2;
-            if (o_vel > 0 || i_vel < 0) {
-                if (o_vel <= 0 && i_vel < 0)
-                    if (o_vel < i_vel) continue;
-                if (o_vel > 0 && i_vel >= 0)
-                    if (o_vel < i_vel) continue;
-                double psum = c[k].mom_o + c[k].mom_i;
-                double msum = m[o] + m[i];
-                double new_o_vel = (double)(((ld)psum - (ld)m[i] * avg_rest * (ld)o_minus_i) / (ld)msum);
-                double new_i_vel = (double)(((ld)psum + (ld)m[o] * avg_rest * (ld)o_minus_i) / (ld)msum);
-                double d_o = new_o_vel - o_vel, d_i = new_i_vel - i_vel;
-                v3[3 * o] += d_o * c[k].ux;
-                v3[3 * o + 1] += d_o * c[k].uy;
-                v3[3 * o + 2] += d_o * c[k].uz;
-                v3[3 * i] += d_i * c[k].ux;
-                v3[3 * i + 1] += d_i * c[k].uy;
-                v3[3 * i + 2] += d_i * c[k].uz;
-            }
-        }
+        resolve_group(o, c, nc, m, rest, v3);
     }
     free(c);
+}
+
+/* The response of s_coll / bh_s_coll to one outer body's candidates (gregsys.hpp:810-838 and
+ * 657-681): ascending distance, first of equal keys only, impulse for approaching pairs. */
+static void resolve_group(int o, coll_cand *c, int nc, const double *m, const double *rest, double *v3) {
+    qsort(c, (size_t)nc, sizeof(coll_cand), cand_cmp);
+    for (int k = 0; k < nc; ++k) {
+        if (k > 0 && c[k].dist == c[k - 1].dist) continue; /* std::map::emplace keeps the first key */
+        int i = c[k].body;
+        double o_vel = c[k].mom_o / m[o];
+        double i_vel = c[k].mom_i / m[i];
+        double o_minus_i = o_vel - i_vel;
+        ld avg_rest = ((ld)rest[o] + (ld)rest[i]) / 2;
+        if (o_vel > 0 || i_vel < 0) {
+            if (o_vel <= 0 && i_vel < 0)
+                if (o_vel < i_vel) continue;
+            if (o_vel > 0 && i_vel >= 0)
+                if (o_vel < i_vel) continue;
+            double psum = c[k].mom_o + c[k].mom_i;
+            double msum = m[o] + m[i];
+            double new_o_vel = (double)(((ld)psum - (ld)m[i] * avg_rest * (ld)o_minus_i) / (ld)msum);
+            double new_i_vel = (double)(((ld)psum + (ld)m[o] * avg_rest * (ld)o_minus_i) / (ld)msum);
+            double d_o = new_o_vel - o_vel, d_i = new_i_vel - i_vel;
+            v3[3 * o] += d_o * c[k].ux;
+            v3[3 * o + 1] += d_o * c[k].uy;
+            v3[3 * o + 2] += d_o * c[k].uz;
+            v3[3 * i] += d_i * c[k].ux;
+            v3[3 * i + 1] += d_i * c[k].uy;
+            v3[3 * i + 2] += d_i * c[k].uz;
+        }
+    }
 }
 
 int orc_evolve(int method, int coll, int n, const double *m, const double *r, const double *rest, double *x3,
@@ -615,5 +625,90 @@ int orc_bench_kdk(int n, const double *m, const double *x3, const double *v3, lo
     for (int t = 0; t < threads; ++t) { free(jobs[t].x3); free(jobs[t].v3); free(jobs[t].a3); }
     free(jobs);
     free(tid);
+    return 0;
+}
+
+/* Cell bounds of node nd (set_corners splits of the root box, greg8tree.hpp:81-131, in T). */
+static void node_box(const orc_tree *t, int nd, int is_float, double lo[3], double hi[3]) {
+    uint64_t c = t->code[t->first[nd]];
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = t->box6[k];
+        hi[k] = t->box6[3 + k];
+    }
+    for (int l = 0; l < t->depth[nd]; ++l) {
+        for (int k = 0; k < 3; ++k) {
+            double mid = midT(lo[k], hi[k], is_float);
+            if ((c >> (3 * (20 - l) + k)) & 1u) lo[k] = mid;
+            else hi[k] = mid;
+        }
+    }
+}
+
+/* bh_s_coll (gregsys.hpp:631-688): for every leaf in DFS order (bh_cube::iterator), the bodies of
+ * the leaves whose cells touch its cell (nn_iterator, greg8tree.hpp:615-701: depth-first from the
+ * root's children in octant order, descending only into touching cells, closed-interval test of
+ * :624-628) that overlap it by radius, resolved exactly as in s_coll.  Leaves shared by bodies with
+ * equal 63-bit codes (depth-21 buckets) count their other bodies as touching neighbours. */
+int orc_bh_s_coll(const orc_tree *t, const double *m, const double *r, const double *rest, const double *x3,
+                  double *v3, int is_float) {
+    int n = t->n;
+    if (n < 2) return 0;
+    int nn = t->n_nodes;
+    double *bx = (double *)malloc(sizeof(double) * 6 * (size_t)nn);
+    int *own = (int *)malloc(sizeof(int) * (size_t)n);
+    coll_cand *c = (coll_cand *)malloc(sizeof(coll_cand) * (size_t)n);
+    if (!bx || !own || !c) { free(bx); free(own); free(c); return -3; }
+    for (int nd = 0; nd < nn; ++nd) {
+        node_box(t, nd, is_float, bx + 6 * nd, bx + 6 * nd + 3);
+        if (t->is_leaf[nd])
+            for (int q = t->first[nd]; q < t->first[nd] + t->count[nd]; ++q) own[q] = nd;
+    }
+    for (int a = 0; a < n; ++a) {
+        int L = own[a], o = t->perm[a], nc = 0;
+        const double *B = bx + 6 * L;
+        for (int k = 1; k < nn;) {
+            int take = 0;
+            if (k == L) {
+                take = t->count[k] > 1;
+            } else {
+                const double *C = bx + 6 * k;
+                int touch = !(B[3] < C[0] || B[0] > C[3] || B[4] < C[1] || B[1] > C[4] || B[5] < C[2] || B[2] > C[5]);
+                if (!touch) { k = t->skip[k]; continue; }
+                if (!t->is_leaf[k]) { ++k; continue; }
+                take = 1;
+            }
+            if (take) {
+                for (int q = t->first[k]; q < t->first[k] + t->count[k]; ++q) {
+                    if (q == a) continue;
+                    int i = t->perm[q];
+                    double rad_dist = r[o] + r[i];
+                    double ux = x3[3 * i] - x3[3 * o], uy = x3[3 * i + 1] - x3[3 * o + 1],
+                           uz = x3[3 * i + 2] - x3[3 * o + 2];
+                    ld dist = mag_ld(ux, uy, uz);
+                    ux = (double)((ld)ux / dist);
+                    uy = (double)((ld)uy / dist);
+                    uz = (double)((ld)uz / dist);
+                    if ((ld)rad_dist > dist) {
+                        double mox = m[o] * v3[3 * o], moy = m[o] * v3[3 * o + 1], moz = m[o] * v3[3 * o + 2];
+                        double mix = m[i] * v3[3 * i], miy = m[i] * v3[3 * i + 1], miz = m[i] * v3[3 * i + 2];
+                        c[nc].inner = q;
+                        c[nc].body = i;
+                        c[nc].dist = dist;
+                        c[nc].mom_o = mox * ux + moy * uy + moz * uz;
+                        c[nc].mom_i = mix * ux + miy * uy + miz * uz;
+                        c[nc].ux = ux;
+                        c[nc].uy = uy;
+                        c[nc].uz = uz;
+                        ++nc;
+                    }
+                }
+            }
+            k = t->skip[k];
+        }
+        if (nc) resolve_group(o, c, nc, m, rest, v3);
+    }
+    free(bx);
+    free(own);
+    free(c);
     return 0;
 }

@@ -103,6 +103,12 @@ void orc_bh_free(orc_tree *t);
 void orc_bh_acc(const orc_tree *t, const double *x3, const double *m, int is_float, double theta, double eps, double G,
                 double *a3, uint32_t *n_inter);
 
+/* bh_s_coll (gregsys.hpp:631-688) over tree t built at x3: restitution impulses between each leaf's
+ * body and the overlapping bodies of the leaves whose cells touch its cell (nn_iterator,
+ * greg8tree.hpp:615-701), leaves in DFS order; v3 is updated in place.  Returns 0 or -3. */
+int orc_bh_s_coll(const orc_tree *t, const double *m, const double *r, const double *rest, const double *x3,
+                  double *v3, int is_float);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,6 +82,8 @@ class Oracle:
         L.orc_bh_build.argtypes = [C.c_int, _dp, _dp, C.c_int, C.POINTER(_Tree)]
         L.orc_bh_free.argtypes = [C.POINTER(_Tree)]
         L.orc_bh_acc.argtypes = [C.POINTER(_Tree), _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _up]
+        L.orc_bh_s_coll.restype = C.c_int
+        L.orc_bh_s_coll.argtypes = [C.POINTER(_Tree), _dp, _dp, _dp, _dp, _dp, C.c_int]
         L.orc_bench_kdk.restype = C.c_int
         L.orc_bench_kdk.argtypes = [C.c_int, _dp, _dp, _dp, C.c_longdouble, C.c_uint64, C.POINTER(C.c_longdouble),
                                     C.c_int, C.POINTER(C.c_longlong)]
@@ -172,6 +174,15 @@ class Oracle:
         out["_tree"] = t
         return out
 
+    def bh_s_coll(self, tree, m, r, rest, x, v, is_float):
+        """bh_s_coll over `tree` (built at x); returns the new velocities."""
+        n = tree["n"]
+        v3 = _c3(v).copy()
+        rc = self.lib.orc_bh_s_coll(C.byref(tree["_tree"]), _c3(m), _c3(r), _c3(rest), _c3(x), v3, int(is_float))
+        if rc:
+            raise RuntimeError(f"orc_bh_s_coll failed ({rc})")
+        return v3.reshape(n, 3)
+
     def bh_free(self, tree):
         self.lib.orc_bh_free(C.byref(tree["_tree"]))
 
@@ -217,6 +228,18 @@ class RefOracle:
         L.ref_bench_kdk.restype = C.c_int
         L.ref_bench_kdk.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, C.c_uint64, C.c_char_p, C.c_int,
                                     C.POINTER(C.c_longlong)]
+        L.ref_to_nsys.restype = C.c_int
+        L.ref_to_nsys.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_uint64, C.c_char_p,
+                                  C.c_char_p, C.POINTER(C.c_longlong)]
+        L.ref_load_nsys.restype = C.c_int
+        L.ref_load_nsys.argtypes = [C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), _dp, _dp,
+                                    _dp, _dp, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double)]
+        L.ref_bh_kdk_coll.restype = C.c_int
+        L.ref_bh_kdk_coll.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_uint64, C.c_double,
+                                      C.c_char_p, _dp, _dp]
+        L.ref_bh_s_coll.restype = C.c_int
+        L.ref_bh_s_coll.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ref_bh_kdk.restype = C.c_int
         L.ref_bh_kdk.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, C.c_uint64, C.c_double, C.c_double,
                                  C.c_char_p, _dp, _dp, _dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
@@ -295,3 +318,45 @@ class RefOracle:
         self._chk(self.lib.ref_bh_kdk(n, _c3(m), _c3(x), _c3(v), dt, steps, theta, eps, units.encode(), xo, vo, ao,
                                       C.byref(tb), C.byref(tw)))
         return xo.reshape(n, 3), vo.reshape(n, 3), ao.reshape(n, 3), tb.value, tw.value
+
+    def bh_s_coll(self, m, r, rest, x, v):
+        """One reference bh_s_coll (gregsys.hpp:631-688) on a T=double tree built at x."""
+        n = len(m)
+        vo = np.zeros(3 * n)
+        self._chk(self.lib.ref_bh_s_coll(n, _c3(m), _c3(r), _c3(rest), _c3(x), _c3(v), vo))
+        return vo.reshape(n, 3)
+
+    def bh_kdk_coll(self, m, r, rest, x, v, dt, steps, theta, units="M66743:66740,D1:1,T1:1"):
+        """ref_bh_kdk with the reference's bh_s_coll after every full kick."""
+        n = len(m)
+        xo, vo = np.zeros(3 * n), np.zeros(3 * n)
+        self._chk(self.lib.ref_bh_kdk_coll(n, _c3(m), _c3(r), _c3(rest), _c3(x), _c3(v), dt, steps, theta,
+                                           units.encode(), xo, vo))
+        return xo.reshape(n, 3), vo.reshape(n, 3)
+
+    NSYS_KINDS = {"ddd": 0, "fff": 1, "lll": 2, "ffd": 3}
+
+    def to_nsys(self, kind, m, r, rest, x, v, dt, steps, path, units="M66743:66740,D1:1,T1:1"):
+        """system<M,R,T>::to_nsys after `steps` leapfrog KDK steps; kind "ddd", "fff", "lll" or
+        "ffd" names M, R, T (double, float, long double).  Returns the bytes written."""
+        nb = C.c_longlong()
+        self._chk(self.lib.ref_to_nsys(self.NSYS_KINDS[kind], len(m), _c3(m), _c3(r), _c3(rest), _c3(x), _c3(v), dt,
+                                       steps, units.encode(), str(path).encode(), C.byref(nb)))
+        return nb.value
+
+    def load_nsys(self, kind, path, check=True, max_n=1 << 20, alloc_chunks=False):
+        """The system<M,R,T>(path, alloc_chunks, check) constructor.  Returns (status, message,
+        state dict): status 0, -1 (nsys_load_error), -2 (nsys_format_error) or -3 (another
+        exception).  alloc_chunks defaults to False: with True the reference crashes on a NaN/Inf
+        chunk (it deletes its stream twice)."""
+        k = max_n
+        m, r, rest = np.zeros(k), np.zeros(k), np.zeros(k)
+        x, v = np.zeros(3 * k), np.zeros(3 * k)
+        n, te, dt, G = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+        rc = self.lib.ref_load_nsys(self.NSYS_KINDS[kind], str(path).encode(), int(alloc_chunks), int(check), k,
+                                    C.byref(n), m, r, rest, x, v, C.byref(te), C.byref(dt), C.byref(G))
+        if rc:
+            return rc, self.lib.ref_last_error().decode(), None
+        nn = n.value
+        return 0, "", dict(m=m[:nn], r=r[:nn], rest=rest[:nn], x=x[:3 * nn].reshape(nn, 3),
+                           v=v[:3 * nn].reshape(nn, 3), time=te.value, dt=dt.value, G=G.value)

@@ -28,7 +28,7 @@ public:
     using bod_f = body<float, float, float, 0>;
 
     template <typename S>
-    static std::vector<bod_d> &bodies(S &s) { return s.bods; }
+    static auto &bodies(S &s) { return s.bods; }
 
     template <typename B>
     static void set_acc(B &b, double ax, double ay, double az) { b.acc.x = ax; b.acc.y = ay; b.acc.z = az; }
@@ -46,6 +46,12 @@ public:
 
     template <typename S>
     static long double G(const S &s) { return s.G; }
+    template <typename S>
+    static long double time_elapsed(const S &s) { return s.time_elapsed; }
+    template <typename S>
+    static long double dt(const S &s) { return s.dt; }
+    template <typename B>
+    static long double rest(const B &b) { return b.rest_c; }
 
     /* DFS pre-order dump of a bh_tree, children in octant order 0..7 (greg8tree.hpp:74-76). */
     template <typename Tree, typename Bod>
@@ -132,6 +138,38 @@ public:
             walk();
             for (auto &b : v) b.curr_vel += dt * b.acc;
         }
+    }
+
+    /* The same schedule on a system with collisions != 0, so that the reference's own bh_s_coll
+     * (gregsys.hpp:631-688) runs after every full kick on the system's own btree, as in
+     * gregsys.hpp:2936-2938. */
+    template <typename S>
+    static void bh_kdk_coll(S &s, long double dt, uint64_t steps, long double theta, long double eps_sq) {
+        auto &v = s.bods;
+        const long double Gc = s.G;
+        const long double half_dt = dt / 2;
+        auto walk = [&]() {
+            s.btree.delete_tree();
+            s.btree.add_bodies(v);
+            s.btree.calc_com();
+            bh_walk(s.btree, v, theta, eps_sq, Gc, nullptr);
+        };
+        walk();
+        for (auto &b : v) b.curr_vel += half_dt * b.acc;
+        for (uint64_t k = 0; k < steps; ++k) {
+            for (auto &b : v) b.curr_pos += dt * b.curr_vel;
+            walk();
+            for (auto &b : v) b.curr_vel += dt * b.acc;
+            s.bh_s_coll();
+        }
+    }
+
+    /* One bh_s_coll on a tree built at the given state (no gravity, no drift). */
+    template <typename S>
+    static void bh_s_coll_once(S &s) {
+        s.btree.delete_tree();
+        s.btree.add_bodies(s.bods);
+        s.bh_s_coll();
     }
 
     template <typename A, typename B>
@@ -345,6 +383,128 @@ int ref_bh_kdk(int n, const double *m, const double *x3, const double *v3, doubl
             a3o[3 * i + 2] = v[i].acceleration().get_z();
         }
     }
+    return 0;
+    REF_CATCH
+}
+
+}  // extern "C"
+
+/* .nsys snapshots through the reference's own system::to_nsys (gregsys.hpp:3214-3258) and
+ * load_from_nsys constructor (gregsys.hpp:1478-1480, 947-1400), for M, R, T in {float, double,
+ * long double}: kind 0 = double x3, 1 = float x3, 2 = long double x3, 3 = <float, float, double>. */
+template <typename M, typename R, typename T>
+static int to_nsys_impl(int n, const double *m, const double *r, const double *rest, const double *x3,
+                        const double *v3, double dt, uint64_t steps, const char *units, const char *path,
+                        long long *bytes) {
+    using sys_t = gtd::system<M, R, T, false, false, 0, 0, 0, false>;
+    using bod_t = gtd::body<M, R, T, 0>;
+    std::vector<bod_t> v;
+    v.reserve(n);
+    for (int i = 0; i < n; ++i)
+        v.emplace_back((M)m[i], (R)r[i], gtd::vector3D<T>{(T)x3[3 * i], (T)x3[3 * i + 1], (T)x3[3 * i + 2]},
+                       gtd::vector3D<T>{(T)v3[3 * i], (T)v3[3 * i + 1], (T)v3[3 * i + 2]}, (long double)rest[i]);
+    sys_t s{std::move(v), (long double)dt, steps, units, true};
+    if (steps) s.evolve(16);  // leapfrog_kdk
+    *bytes = (long long)s.to_nsys(path);
+    return 0;
+}
+
+template <typename M, typename R, typename T>
+static int load_nsys_impl(const char *path, int alloc, int check, int max_n, int *n_out, double *m, double *r,
+                          double *rest, double *x3, double *v3, double *t_el, double *dt, double *G) {
+    using sys_t = gtd::system<M, R, T, false, false, 0, 0, 0, false>;
+    sys_t s{path, alloc != 0, check != 0, true};
+    auto &b = ref_access::bodies(s);
+    *n_out = (int)b.size();
+    for (int i = 0; i < (int)b.size() && i < max_n; ++i) {
+        m[i] = (double)b[i].mass();
+        r[i] = (double)b[i].rad();
+        rest[i] = (double)ref_access::rest(b[i]);
+        x3[3 * i] = (double)b[i].pos().get_x(); x3[3 * i + 1] = (double)b[i].pos().get_y();
+        x3[3 * i + 2] = (double)b[i].pos().get_z();
+        v3[3 * i] = (double)b[i].vel().get_x(); v3[3 * i + 1] = (double)b[i].vel().get_y();
+        v3[3 * i + 2] = (double)b[i].vel().get_z();
+    }
+    *t_el = (double)ref_access::time_elapsed(s);
+    *dt = (double)ref_access::dt(s);
+    *G = (double)ref_access::G(s);
+    return 0;
+}
+
+extern "C" {
+
+int ref_to_nsys(int kind, int n, const double *m, const double *r, const double *rest, const double *x3,
+                const double *v3, double dt, uint64_t steps, const char *units, const char *path, long long *bytes) {
+    REF_TRY
+    switch (kind) {
+        case 0: return to_nsys_impl<double, double, double>(n, m, r, rest, x3, v3, dt, steps, units, path, bytes);
+        case 1: return to_nsys_impl<float, float, float>(n, m, r, rest, x3, v3, dt, steps, units, path, bytes);
+        case 2:
+            return to_nsys_impl<long double, long double, long double>(n, m, r, rest, x3, v3, dt, steps, units, path,
+                                                                       bytes);
+        case 3: return to_nsys_impl<float, float, double>(n, m, r, rest, x3, v3, dt, steps, units, path, bytes);
+    }
+    std::snprintf(g_err, sizeof g_err, "unknown kind %d", kind);
+    return -1;
+    REF_CATCH
+}
+
+/* Returns 0, or -1 (nsys_load_error), -2 (nsys_format_error), -3 (other exception) with the
+ * exception's what() in ref_last_error.  alloc = the constructor's alloc_chunks; with alloc != 0 a
+ * NaN/Inf chunk makes the reference delete its input stream a second time (gregsys.hpp:1306-1308,
+ * then final_handler :950-952) and crash, so NaN/Inf cases are read with alloc = 0. */
+int ref_load_nsys(int kind, const char *path, int alloc, int check, int max_n, int *n_out, double *m, double *r,
+                  double *rest, double *x3, double *v3, double *t_el, double *dt, double *G) {
+    try {
+        switch (kind) {
+            case 0:
+                return load_nsys_impl<double, double, double>(path, alloc, check, max_n, n_out, m, r, rest, x3, v3,
+                                                              t_el, dt, G);
+            case 1:
+                return load_nsys_impl<float, float, float>(path, alloc, check, max_n, n_out, m, r, rest, x3, v3, t_el,
+                                                           dt, G);
+            case 2:
+                return load_nsys_impl<long double, long double, long double>(path, alloc, check, max_n, n_out, m, r,
+                                                                             rest, x3, v3, t_el, dt, G);
+            case 3:
+                return load_nsys_impl<float, float, double>(path, alloc, check, max_n, n_out, m, r, rest, x3, v3, t_el,
+                                                            dt, G);
+        }
+        std::snprintf(g_err, sizeof g_err, "unknown kind %d", kind);
+        return -3;
+    } catch (const gtd::nsys_format_error &e) {
+        std::snprintf(g_err, sizeof g_err, "%s", e.what());
+        return -2;
+    } catch (const gtd::nsys_load_error &e) {
+        std::snprintf(g_err, sizeof g_err, "%s", e.what());
+        return -1;
+    } catch (const std::exception &e) {
+        std::snprintf(g_err, sizeof g_err, "%s", e.what());
+        return -3;
+    }
+}
+
+/* ref_bh_kdk with the reference's bh_s_coll after every full kick: a
+ * gtd::system<double,double,double,false,false,3,0,0,false> (overlapping bodies allowed). */
+int ref_bh_kdk_coll(int n, const double *m, const double *r, const double *rest, const double *x3, const double *v3,
+                    double dt, uint64_t steps, double theta, const char *units, double *x3o, double *v3o) {
+    REF_TRY
+    using sys_t = gtd::system<double, double, double, false, false, 3, 0, 0, false>;
+    sys_t s{make_bodies(n, m, r, rest, x3, v3), (long double)dt, steps, units, true};
+    ref_access::bh_kdk_coll(s, (long double)dt, steps, (long double)theta, 0.0L);
+    read_back(s, x3o, v3o, nullptr, nullptr, nullptr);
+    return 0;
+    REF_CATCH
+}
+
+/* One reference bh_s_coll on the given state (tree built at x3); v3o receives the velocities. */
+int ref_bh_s_coll(int n, const double *m, const double *r, const double *rest, const double *x3, const double *v3,
+                  double *v3o) {
+    REF_TRY
+    using sys_t = gtd::system<double, double, double, false, false, 3, 0, 0, false>;
+    sys_t s{make_bodies(n, m, r, rest, x3, v3), 1.0L, 1, "M1:1,D1:1,T1:1", true};
+    ref_access::bh_s_coll_once(s);
+    read_back(s, nullptr, v3o, nullptr, nullptr, nullptr);
     return 0;
     REF_CATCH
 }

@@ -91,6 +91,27 @@ int main() {
         std::printf("octree leaf order matches host rebuild: %d\n", (int)same);
         fails += !same;
     }
+    {  // .nsys round trip: to_nsys, then the path constructor (gregsys.hpp:3214-3258, 1479-1490)
+        const auto ni = make(100, 15, 1.0);
+        sys_t s{ni, 3600, 3, "M66743:66740,D1:1,T1:1", true};
+        s.evolve(sys_t::leapfrog_kdk);
+        const char *path = "dropin_roundtrip.nsys";
+        const auto bytes = s.to_nsys(path);
+        sys_t t{path};
+        bool same = bytes == 96 + 100 * 80 && t.num_bodies() == s.num_bodies() && t.G_val() == s.G_val() &&
+                    t.elapsed_time() == s.elapsed_time();
+        for (size_t i = 0; same && i < s.num_bodies(); ++i)
+            same = t[i].pos().x == s[i].pos().x && t[i].vel().z == s[i].vel().z && t[i].mass() == s[i].mass();
+        bool thrown = false;
+        try {
+            gtd::system<float, float, float> bad{path};
+        } catch (const gtd::nsys_load_error &) {
+            thrown = true;  // M is float here but the file holds doubles
+        }
+        std::remove(path);
+        std::printf(".nsys round trip: %d, size mismatch threw: %d\n", (int)same, (int)thrown);
+        fails += !(same && thrown);
+    }
     std::printf(fails ? "FAIL\n" : "OK\n");
     return fails ? 1 : 0;
 }

@@ -21,6 +21,97 @@ from oracle.oracle import RefOracle, ensure_built  # noqa: E402
 METHODS = {"euler": 2, "modified_euler": 4, "midpoint": 8, "leapfrog_kdk": 16, "leapfrog_dkd": 32}
 
 
+def _mut(fn):
+    def wrap(b):
+        b = bytearray(b)
+        fn(b)
+        return bytes(b)
+    return wrap
+
+
+def _set_f64(off, val):
+    return _mut(lambda b: b.__setitem__(slice(off, off + 8), np.float64(val).tobytes()))
+
+
+def _set_x87(off, val):
+    return _mut(lambda b: b.__setitem__(slice(off, off + 16), np.array([val], dtype=np.longdouble).tobytes()))
+
+
+def nsys_fixtures(r, out):
+    """.nsys files written by the reference's to_nsys (after 3 KDK steps) for four M/R/T choices,
+    the state its loader reads back, and corrupted copies with the reference loader's verdicts
+    (read with alloc_chunks = false: with true the reference crashes on a NaN/Inf chunk)."""
+    import tempfile
+    m, x, v = plummer(37, 3)
+    rad = np.linspace(1e3, 5e3, 37)
+    rest = np.linspace(0.2, 1.0, 37)
+    out["nsys_m"], out["nsys_x"], out["nsys_v"], out["nsys_r"], out["nsys_rest"] = m, x, v, rad, rest
+    cases = {
+        "sig_both": _mut(lambda b: b.__setitem__(slice(0, 2), b"XY")),
+        "sig_first_only": _mut(lambda b: b.__setitem__(0, ord("X"))),
+        "dtypes_bit6": _mut(lambda b: b.__setitem__(2, b[2] | 0x40)),
+        "m_integral": _mut(lambda b: b.__setitem__(2, b[2] & ~0x02)),
+        "t_size": _mut(lambda b: b.__setitem__(38, 4)),
+        "rest_size_12": _mut(lambda b: b.__setitem__(39, 12)),
+        "rest_size_32": _mut(lambda b: b.__setitem__(39, 32)),
+        "rest_size_8": _mut(lambda b: b.__setitem__(39, 8)),
+        "truncated": lambda b: b[:-4],
+        "short": lambda b: b[:50],
+        "time_size_12": _mut(lambda b: b.__setitem__(3, 12)),
+        "time_integral": _mut(lambda b: (b.__setitem__(2, b[2] & ~0x01), b.__setitem__(3, 8),
+                                         b.__setitem__(slice(4, 12), np.uint64(7200).tobytes()),
+                                         b.__setitem__(slice(20, 28), np.uint64(600).tobytes()))),
+        "dt_zero": _set_x87(20, 0.0),
+        "dt_inf": _set_x87(20, np.inf),
+        "nan_zpos_5": _set_f64(96 + 5 * 80 + 48, np.nan),
+        "inf_mass_9": _set_f64(96 + 9 * 80 + 16, -np.inf),
+        "nan_rcoeff_2": _set_x87(96 + 2 * 80, np.nan),
+        "zero_bodies": lambda b: b[:88] + np.uint64(0).tobytes(),
+    }
+    with tempfile.TemporaryDirectory() as d:
+        for kind in ("ddd", "fff", "lll", "ffd"):
+            p = os.path.join(d, kind + ".nsys")
+            r.to_nsys(kind, m, rad, rest, x, v, 3600.0, 3, p, UNITS_G6674)
+            with open(p, "rb") as f:
+                out[f"nsys_{kind}_bytes"] = np.frombuffer(f.read(), dtype=np.uint8).copy()
+            rc, msg, st = r.load_nsys(kind, p)
+            assert rc == 0, msg
+            for k in ("m", "r", "rest", "x", "v"):
+                out[f"nsys_{kind}_{k}"] = st[k]
+            out[f"nsys_{kind}_meta"] = np.array([st["time"], st["dt"], st["G"]])
+        base = bytes(out["nsys_ddd_bytes"])
+        names, rcs, msgs = [], [], []
+        for name, fn in cases.items():
+            p = os.path.join(d, name + ".nsys")
+            data = fn(base)
+            with open(p, "wb") as f:
+                f.write(data)
+            rc, msg, st = r.load_nsys("ddd", p)
+            out[f"nsysbad_{name}_bytes"] = np.frombuffer(data, dtype=np.uint8).copy()
+            if rc == 0:
+                out[f"nsysbad_{name}_meta"] = np.array([st["time"], st["dt"], st["G"], len(st["m"])])
+                for k in ("m", "r", "rest", "x", "v"):
+                    out[f"nsysbad_{name}_{k}"] = st[k]
+            names.append(name)
+            rcs.append(rc)
+            msgs.append(msg)
+        out["nsysbad_names"] = np.array(names)
+        out["nsysbad_rc"] = np.array(rcs)
+        out["nsysbad_msg"] = np.array(msgs)
+
+
+def overlap_cluster(n: int, seed: int):
+    """n bodies uniform in a 0.05 AU cube with radii of the order of their spacing (many overlaps),
+    log-uniform masses 1e24..1e28 kg, Gaussian velocities of 3 km/s and restitution in [0.3, 1]."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-1.0, 1.0, (n, 3)) * 0.05 * AU
+    v = rng.normal(0.0, 3e3, (n, 3))
+    m = np.exp(rng.uniform(np.log(1e24), np.log(1e28), n))
+    r = 0.02 * AU * n ** (-1.0 / 3.0) * rng.uniform(0.5, 3.0, n)
+    rest = rng.uniform(0.3, 1.0, n)
+    return m, r, rest, x, v
+
+
 def main():
     ensure_built(ref=True)
     r = RefOracle()
@@ -93,6 +184,15 @@ def main():
     out["bhk_m"], out["bhk_x"], out["bhk_v"] = m6, x6, v6
     xo, vo, ao, _, _ = r.bh_kdk(m6, x6, v6, 3600.0, 5, 0.5, 0.0, UNITS_G6674)
     out["bhk_xo"], out["bhk_vo"], out["bhk_ao"] = xo, vo, ao
+    # bh_s_coll: a tight cluster of overlapping bodies; one collision pass on a T=double tree, then
+    # a Barnes-Hut KDK with the pass after every full kick (collisions != 0)
+    mc, rc, ec, xc, vc = overlap_cluster(400, 9)
+    out["bhc_m"], out["bhc_r"], out["bhc_rest"], out["bhc_x"], out["bhc_v"] = mc, rc, ec, xc, vc
+    out["bhc_v_out"] = r.bh_s_coll(mc, rc, ec, xc, vc)
+    mk, rk, ek, xk, vk = overlap_cluster(300, 10)
+    out["bhck_m"], out["bhck_r"], out["bhck_rest"], out["bhck_x"], out["bhck_v"] = mk, rk, ek, xk, vk
+    out["bhck_xo"], out["bhck_vo"] = r.bh_kdk_coll(mk, rk, ek, xk, vk, 3600.0, 5, 0.5, UNITS_G6674)
+    nsys_fixtures(r, out)
     path = os.path.join(HERE, "reference_golden.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes,", len(out), "arrays")

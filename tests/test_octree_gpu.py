@@ -141,3 +141,69 @@ def test_nonfinite_position_rejected(gpu):
     s = System(m, x, np.zeros_like(x))
     with pytest.raises(InvalidBodyPlacement):
         s.bh_build(True)
+
+
+def _bh_coll_kdk_oracle(oracle, m, r, rest, x, v, dt, steps, theta, G, is_float):
+    """The reference's Barnes-Hut KDK schedule with bh_s_coll after each full kick, from the
+    oracle's tree, walk and collision pass."""
+    x, v = x.copy(), v.copy()
+
+    def walk():
+        t = oracle.bh_tree(x, m, is_float)
+        a, _ = oracle.bh_acc(t, x, m, is_float, theta, 0.0, G)
+        return t, a
+
+    t, a = walk()
+    oracle.bh_free(t)
+    v = v + 0.5 * dt * a
+    for _ in range(steps):
+        x = x + dt * v
+        t, a = walk()
+        v = v + dt * a
+        v = oracle.bh_s_coll(t, m, r, rest, x, v, is_float)
+        oracle.bh_free(t)
+    return x, v
+
+
+def test_bh_collisions_vs_reference_golden(gpu, golden):
+    """Barnes-Hut KDK with collisions on (bh_s_coll after every full kick) against the reference
+    run on the same overlapping cluster, T=double tree."""
+    g = golden
+    s = System(g["bhck_m"], g["bhck_x"], g["bhck_v"], r=g["bhck_r"], rest=g["bhck_rest"], timestep=3600.0,
+               num_iterations=5, units_format=UNITS_G6674, collisions=System.overlap_coll_check)
+    s.set_bh_opening_angle(0.5)
+    s.bh_tree_float(False)
+    s.evolve(System.leapfrog_kdk | System.barnes_hut)
+    no = System(g["bhck_m"], g["bhck_x"], g["bhck_v"], r=g["bhck_r"], rest=g["bhck_rest"], timestep=3600.0,
+                num_iterations=5, units_format=UNITS_G6674)
+    no.set_bh_opening_angle(0.5)
+    no.bh_tree_float(False)
+    no.evolve(System.leapfrog_kdk | System.barnes_hut)
+    vmax = np.abs(g["bhck_vo"]).max()
+    assert np.abs(s.x - g["bhck_xo"]).max() / np.abs(g["bhck_xo"]).max() < 1e-12
+    assert np.abs(s.v - g["bhck_vo"]).max() / vmax < 1e-10
+    assert np.abs(no.v - g["bhck_vo"]).max() / vmax > 1e-3  # the collisions changed the run
+
+
+@pytest.mark.parametrize("tree_float", [False, True])
+def test_bh_collisions_vs_oracle(gpu, oracle, tree_float):
+    """The same on a denser cluster, float and double trees, against the oracle's composition.
+    Masses of 1e-3..10 kg make gravity negligible, so the float tree's FP32 forces between
+    near-coincident bodies (no softening) do not mask what is checked here: the float tree's cells,
+    the neighbour order and the FP64 impulses."""
+    rng = np.random.default_rng(31)
+    n = 1500
+    x = rng.uniform(-1.0, 1.0, (n, 3)) * 0.05 * AU
+    v = rng.normal(0.0, 3e3, (n, 3))
+    m = np.exp(rng.uniform(np.log(1e-3), np.log(10.0), n))
+    r = 0.02 * AU * n ** (-1.0 / 3.0) * rng.uniform(0.5, 3.0, n)
+    rest = rng.uniform(0.3, 1.0, n)
+    s = System(m, x, v, r=r, rest=rest, timestep=3600.0, num_iterations=3, units_format=UNITS_G6674,
+               collisions=System.overlap_coll_check)
+    s.set_bh_opening_angle(0.5)
+    s.bh_tree_float(tree_float)
+    s.evolve(System.leapfrog_kdk | System.barnes_hut)
+    xo, vo = _bh_coll_kdk_oracle(oracle, m, r, rest, x, v, 3600.0, 3, 0.5, 6.674e-11, tree_float)
+    assert np.abs(s.x - xo).max() / np.abs(xo).max() < 1e-12
+    assert np.abs(s.v - vo).max() / np.abs(vo).max() < 1e-10
+    assert np.abs(vo - v).max() > 1.0  # the collisions changed the velocities

@@ -98,3 +98,16 @@ def test_barnes_hut_acc_matches_reference_walk(oracle, golden):
     assert int(cnt.sum()) == int(g["bh_count"])
     rel = np.linalg.norm(a - g["bh_acc"], axis=1) / np.linalg.norm(g["bh_acc"], axis=1)
     assert rel.max() < 1e-12
+
+
+def test_bh_s_coll_bit_exact(oracle, golden):
+    """bh_s_coll (gregsys.hpp:631-688): leaf-cube neighbours, ascending distance, restitution
+    impulses; the oracle on its own T=double tree against the reference's pass."""
+    g = golden
+    t = oracle.bh_tree(g["bhc_x"], g["bhc_m"], 0)
+    try:
+        v = oracle.bh_s_coll(t, g["bhc_m"], g["bhc_r"], g["bhc_rest"], g["bhc_x"], g["bhc_v"], 0)
+    finally:
+        oracle.bh_free(t)
+    assert np.array_equal(v, g["bhc_v_out"])
+    assert (np.abs(g["bhc_v_out"] - g["bhc_v"]).max(1) > 0).sum() > 50  # the fixture really collides
