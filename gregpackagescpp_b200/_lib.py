@@ -145,6 +145,8 @@ def load():
     L.gtd_bh_tree_download.argtypes = [vp] + [dp] * 10
     L.gtd_bh_accelerations.argtypes = [vp, dp, dp]
     L.gtd_nsys_chunk_size.argtypes = [ip, ip, ip, C.POINTER(C.c_int)]
+    L.gtd_system_set_recording.argtypes = [vp, u64]
+    L.gtd_system_recording.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), dp, dp]
     L.gtd_system_to_nsys.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, dp, ip, ip, ip, C.POINTER(i64)]
     L.gtd_system_load_nsys.argtypes = [vp, C.c_char_p, ip, ip, ip, ip, C.POINTER(C.c_double),
                                        C.POINTER(C.c_double), dp, C.POINTER(C.c_double)]

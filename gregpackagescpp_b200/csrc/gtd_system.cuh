@@ -106,6 +106,15 @@ struct gtd_system {
     // .nsys chunk staging (nsys.cu)
     void *nsys_dev = nullptr, *nsys_host = nullptr;
     size_t nsys_dev_bytes = 0, nsys_host_bytes = 0;
+
+    // trajectory frames (record.cu): every rec_every-th state of a direct-summation evolve
+    uint64_t rec_every = 0;
+    uint64_t rec_step = 0;               // steps since evolve_begin
+    std::vector<double> rec_frames;      // [frames][rec_n][8]: x y z vx vy vz ke pe
+    std::vector<int64_t> rec_states;     // step index of each frame
+    int64_t rec_n = 0;
+    double *rec_dev = nullptr;
+    int64_t rec_dev_n = 0;
 };
 
 // Makes the handle's device current for the scope of an entry point.
@@ -134,6 +143,8 @@ int output_rows(gtd_system *s, std::vector<int64_t> &row);
 int copy_acc_out(gtd_system *s, double *a3);
 void release_collide(gtd_system *s);
 void release_nsys(gtd_system *s);
+void release_record(gtd_system *s);
+int record_frame(gtd_system *s, uint64_t state);
 int ensure_body_capacity(gtd_system *s, int64_t n);
 int set_loaded_bodies(gtd_system *s, int64_t n);
 int ensure_plan(gtd_system *s);

@@ -307,9 +307,18 @@ static int evolve_begin(gtd_system *s, int method) {
     s->method = method;
     s->begun = true;
     s->synced = true;
+    s->rec_step = 0;
+    s->rec_frames.clear();
+    s->rec_states.clear();
     if (s->n == 0) return GTD_OK;
+    if (s->rec_every && s->coll == GTD_MERGE_COLL)
+        return fail(GTD_ERR_UNSUPPORTED, "trajectory recording with merging collisions is not supported");
     int rc = maybe_reorder(s, true);
     if (rc) return rc;
+    if (s->rec_every) {
+        rc = record_frame(s, 0);
+        if (rc) return rc;
+    }
     if (method == GTD_LEAPFROG_KDK) {
         StepArgs a = step_args(s, s->pm[s->cur], true);
         return force_and_integrate(s, s->pm[s->cur], EPI_ACC, a);
@@ -321,14 +330,20 @@ static int evolve_steps(gtd_system *s, uint64_t k) {
     if (!s->begun) return fail(GTD_ERR_INVALID_ARGUMENT, "gtd_system_evolve_steps before gtd_system_evolve_begin");
     if (s->n == 0 || k == 0) return GTD_OK;
     for (uint64_t i = 0; i < k; ++i) {
-        const bool last = (i + 1 == k) || s->coll != GTD_NO_COLL;
+        const bool rec = s->rec_every && (s->rec_step + 1) % s->rec_every == 0;
+        const bool last = (i + 1 == k) || s->coll != GTD_NO_COLL || rec;
         int rc = maybe_reorder(s, false);
         if (rc) return rc;
         rc = direct_step(s, s->method, last);
         if (rc) return rc;
         s->steps_since_reorder += 1;
+        s->rec_step += 1;
         if (s->coll != GTD_NO_COLL) {
             rc = run_collisions(s);
+            if (rc) return rc;
+        }
+        if (rec) {
+            rc = record_frame(s, s->rec_step);
             if (rc) return rc;
         }
     }
@@ -392,6 +407,7 @@ int gtd_system_destroy(gtd_system *s) {
     release_tree(s);
     release_collide(s);
     release_nsys(s);
+    release_record(s);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     cudaEventDestroy(s->ev0);
     cudaEventDestroy(s->ev1);
@@ -573,6 +589,8 @@ int gtd_system_evolve(gtd_system *s, int method, int64_t *elapsed_ns) {
     GTD_CUDA(cudaEventRecord(s->ev0, s->stream));
     int rc;
     if (bh) {
+        s->rec_frames.clear();  // the reference records nothing in its Barnes-Hut branches
+        s->rec_states.clear();
         rc = bh_evolve_kdk(s, s->iterations);
     } else {
         rc = evolve_begin(s, branch);

@@ -23,6 +23,17 @@ _UNITS_RE = re.compile(
     r"(?=\d{1,18}\s*$)\d*[1-9]+\d*\s*$")
 
 
+def _ke(m, v):
+    """body::set_ke (gregbod.hpp:325-328): 0.5 * m * |v| * |v|."""
+    mag = np.sqrt(v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1] + v[:, 2] * v[:, 2]) if len(m) else np.zeros(0)
+    return 0.5 * m * mag * mag
+
+
+def _seq_sum(a):
+    """Left-to-right sum, the order of the reference's accumulation loops."""
+    return float(np.add.accumulate(a)[-1]) if len(a) else 0.0
+
+
 def units_values(units: str) -> tuple:
     """The six numbers of a units format "Ma:b,Dc:d,Tx:y" in the order the reference keeps them
     (G_vals, gregsys.hpp:275-280) and writes them to .nsys headers: (m_num=b, m_denom=a, d_num=c,
@@ -81,7 +92,7 @@ class System:
     def __init__(self, m=None, x=None, v=None, r=None, rest=None, timestep: float = 1.0,
                  num_iterations: int = 1000, units_format: str = "M1:1,D1:1,T1:1",
                  allow_overlapping_bodies: bool = True, precision: str = "f64", collisions: int = 0,
-                 merge_overlapping: bool = False, device: int = 0):
+                 merge_overlapping: bool = False, device: int = 0, mem_freq: int = 0):
         L = _lib.load()
         if timestep <= 0:
             raise ValueError("Time-step cannot be zero or negative.\n")  # check_dt, gregsys.hpp:1401-1405
@@ -108,6 +119,12 @@ class System:
         self._h = h
         self._L = L
         self.time_elapsed = 0.0
+        # memFreq recordings (gregbod.hpp:304-320, gregsys.hpp:219-227); curr_ke is each body's
+        # kinetic energy as last recorded (set at construction, gregbod.hpp:325-328)
+        self.mem_freq = int(mem_freq)
+        check(L.gtd_system_set_recording(h, self.mem_freq))
+        self.curr_ke = _ke(self.m, self.v)
+        self._clear_recordings()
         self.allow_overlap = allow_overlapping_bodies
         if not allow_overlapping_bodies:
             self.check_overlap()
@@ -184,6 +201,8 @@ class System:
         s.time_elapsed, s.dt, s.G = te.value, dt.value, G.value
         s.g_vals = tuple(int(g) for g in gv)
         s._pull()
+        s.curr_ke = _ke(s.m, s.v)
+        s._clear_recordings()
         s.allow_overlap = allow_overlapping_bodies
         if not allow_overlapping_bodies:
             s.check_overlap()
@@ -221,6 +240,8 @@ class System:
         x, v, a = np.zeros((k, 3)), np.zeros((k, 3)), np.zeros((k, 3))
         check(L.gtd_system_download(self._h, C.byref(n), ptr(m), ptr(r), ptr(rest), ptr(x), ptr(v), ptr(a)))
         self.m, self.r, self.rest, self.x, self.v, self.a = m, r, rest, x, v, a
+        if len(getattr(self, "curr_ke", ())) != k:
+            self.curr_ke = _ke(m, v)
 
     def evolve(self, integration_method: int = 16, continue_ev_if=None, for_each_bod=None,
                for_all_bods=None) -> int:
@@ -230,10 +251,17 @@ class System:
         self._push()
         ns = C.c_int64()
         if continue_ev_if is None and for_each_bod is None and for_all_bods is None:
+            x0, v0 = self.x.copy(), self.v.copy()
             check(self._L.gtd_system_evolve(self._h, integration_method, C.byref(ns)))
             self._pull()
+            if self.mem_freq and len(self.m):
+                self.x, self.v, cur = x0, v0, (self.x, self.v)
+                self._collect_recordings(integration_method)
+                self.x, self.v = cur
             self.time_elapsed = self.iterations * self.dt
             return ns.value
+        if self.mem_freq:
+            raise NotImplementedError("memFreq recordings with evolve callbacks are not supported")
         check(self._L.gtd_system_evolve_begin(self._h, integration_method))
         steps = 0
         while (continue_ev_if() if continue_ev_if is not None else steps < self.iterations):
@@ -251,6 +279,52 @@ class System:
         self._pull()
         self.time_elapsed = steps * self.dt
         return 0
+
+    # ---- memFreq recordings ------------------------------------------------------------------
+    def _clear_recordings(self) -> None:
+        """clear_evolution (gregsys.hpp:2569-2586) / body::clear (gregbod.hpp:621-628): one frame,
+        the current state with the last recorded kinetic energy; no energy records."""
+        n = len(self.m)
+        self.positions = self.x.reshape(1, n, 3).copy()
+        self.velocities = self.v.reshape(1, n, 3).copy()
+        self.kinetic_energies = self.curr_ke.reshape(1, n).copy()
+        self.pe = np.zeros((0, n))
+        self.energies = np.zeros((0, n))
+        self.tot_pe, self.tot_ke, self.tot_e = np.zeros(0), np.zeros(0), np.zeros(0)
+
+    def _collect_recordings(self, method: int) -> None:
+        """The records the reference keeps (fileFreq = 0, the only setting with which its evolve
+        compiles): FUNC_TEMPL_SELECT (gregsys.hpp:15-105) never takes its recording branch, so
+        trajectories beyond the first frame come only from the collision pass (s_coll<true>, with
+        collisions on); energies come from calc_acc_and_e / calc_energy (every frame of Euler,
+        modified Euler and midpoint; only the first for the leapfrogs without collisions, whose
+        per-step energy records sit behind that branch) and from the leapfrogs' collision path.
+        Energies use each body's last recorded kinetic energy.  Barnes-Hut branches record nothing."""
+        self._clear_recordings()
+        f = C.c_int64()
+        nb = C.c_int64()
+        check(self._L.gtd_system_recording(self._h, C.byref(f), C.byref(nb), None, None))
+        if f.value == 0 or method & self.barnes_hut:
+            return
+        n = nb.value
+        states = np.zeros(f.value, np.int64)
+        fr = np.zeros((f.value, n, 8))
+        check(self._L.gtd_system_recording(self._h, None, None, ptr(states), ptr(fr)))
+        branch = next((b for b in (1, 2, 4, 8, 16, 32, 64, 128) if method & b == b), 0)
+        coll = self.collisions != 0
+        if coll and f.value > 1:
+            self.positions = np.concatenate([self.positions, fr[1:, :, 0:3]])
+            self.velocities = np.concatenate([self.velocities, fr[1:, :, 3:6]])
+            self.kinetic_energies = np.concatenate([self.kinetic_energies, fr[1:, :, 6]])
+        n_e = 1 if (branch in (self.leapfrog_kdk, self.leapfrog_dkd) and not coll) else f.value
+        ke_at = [self.curr_ke if (k == 0 or not coll) else fr[k, :, 6] for k in range(n_e)]
+        self.pe = fr[:n_e, :, 7].copy()
+        self.energies = np.array([ke_at[k] + self.pe[k] for k in range(n_e)]).reshape(n_e, n)
+        self.tot_pe = np.array([_seq_sum(self.pe[k]) for k in range(n_e)])
+        self.tot_ke = np.array([_seq_sum(ke_at[k]) for k in range(n_e)])
+        self.tot_e = self.tot_pe + self.tot_ke
+        if coll and f.value > 1:
+            self.curr_ke = fr[-1, :, 6].copy()
 
     def accelerations(self, method: int = 0) -> np.ndarray:
         self._push()

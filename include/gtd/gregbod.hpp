@@ -12,6 +12,7 @@
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "../gtd_b200.h"
 
@@ -187,27 +188,60 @@ class bh_tree;
 template <isNumWrapper M = long double, isNumWrapper R = long double, isNumWrapper T = long double,
           uint64_t recFreq = 0>
 class body : public body_counter {
+public:
+    using K = decltype(M{} * T{} * T{});  // kinetic energy type
+
+private:
     M mass_{1};
     R radius{1};
     vector3D<T> curr_pos{}, curr_vel{}, acc{};
     long double rest_c{1};
+    K curr_ke{};  // kinetic energy as last recorded (gregbod.hpp:299, 325-328)
+    // trajectory (recFreq != 0; gregbod.hpp:304-306): the first element is the state at construction
+    std::vector<vector3D<T>> positions, velocities;
+    std::vector<K> energies;
     void check() const {
         if (mass_ < M{0}) throw negative_mass_error{};
         if (radius < R{0}) throw negative_radius_error{};
     }
+    void set_ke() {
+        const auto mag = curr_vel.magnitude();
+        curr_ke = 0.5 * mass_ * mag * mag;
+    }
+    void add_pos_vel_ke() {
+        if constexpr (recFreq != 0) {
+            set_ke();
+            positions.push_back(curr_pos);
+            velocities.push_back(curr_vel);
+            energies.push_back(curr_ke);
+        }
+    }
+    void clear_trajectory() {  // body::clear (gregbod.hpp:621-628): the current state, ke not recomputed
+        positions.assign(1, curr_pos);
+        velocities.assign(1, curr_vel);
+        energies.assign(1, curr_ke);
+    }
 
 public:
-    body() = default;
-    body(const M &m, const R &r) : mass_{m}, radius{r} { check(); }
+    body() { add_pos_vel_ke(); }
+    body(const M &m, const R &r) : mass_{m}, radius{r} {
+        check();
+        add_pos_vel_ke();
+    }
     body(const M &m, const R &r, const vector3D<T> &pos, const vector3D<T> &vel, long double restitution = 1)
         : mass_{m}, radius{r}, curr_pos{pos}, curr_vel{vel}, rest_c{restitution} {
         check();
+        add_pos_vel_ke();
     }
     body(const M &m, const R &r, const T &x, const T &y, const T &z, const T &vx, const T &vy, const T &vz,
          long double restitution = 1)
         : mass_{m}, radius{r}, curr_pos{x, y, z}, curr_vel{vx, vy, vz}, rest_c{restitution} {
         check();
+        add_pos_vel_ke();
     }
+    const std::vector<vector3D<T>> &get_positions() const { return positions; }
+    const std::vector<vector3D<T>> &get_velocities() const { return velocities; }
+    const std::vector<K> &get_kinetic_energies() const { return energies; }
     const M &mass() const noexcept { return mass_; }
     const R &rad() const noexcept { return radius; }
     const vector3D<T> &pos() const noexcept { return curr_pos; }

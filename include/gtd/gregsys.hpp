@@ -57,6 +57,9 @@ private:
     uint64_t iterations = 1'000;
     long double time_elapsed{};
     uint64_t G_vals[6] = {1, 1, 1, 1, 1, 1};  // m_num, m_denom, d_num, d_denom, t_num, t_denom
+    // memFreq energy records of the last evolve (gregsys.hpp:219-227), per body in body order
+    std::vector<std::vector<T>> pe_rec, energy_rec;
+    std::vector<T> tot_pe, tot_ke, tot_e;
     bool mixed = false;
     gtd_system *dev = nullptr;
     int device = 0;
@@ -80,7 +83,60 @@ private:
         G /= 1'000'000'000'000'000;
     }
     void ensure_device() {
-        if (!dev) throw_status(gtd_system_create(&dev, device, mixed ? GTD_PREC_MIXED : GTD_PREC_F64));
+        if (!dev) {
+            throw_status(gtd_system_create(&dev, device, mixed ? GTD_PREC_MIXED : GTD_PREC_F64));
+            throw_status(gtd_system_set_recording(dev, memFreq));
+        }
+    }
+    // The records the reference keeps (fileFreq = 0 is the only setting with which its evolve
+    // compiles): FUNC_TEMPL_SELECT (gregsys.hpp:15-105) never takes its recording branch, so the
+    // trajectories grow past their first element only through the collision pass (s_coll<true>);
+    // energies come from calc_acc_and_e / calc_energy (every frame for Euler, modified Euler and
+    // midpoint, the first only for the leapfrogs without collisions) and from the leapfrogs'
+    // collision path, with each body's last recorded kinetic energy.  Barnes-Hut records nothing.
+    void collect_recordings(int method) {
+        pe_rec.clear();
+        energy_rec.clear();
+        tot_pe.clear();
+        tot_ke.clear();
+        tot_e.clear();
+        int64_t frames = 0, n = 0;
+        throw_status(gtd_system_recording(dev, &frames, &n, nullptr, nullptr));
+        if (!frames || (method & barnes_hut) == barnes_hut || (size_t)n != bods.size()) return;
+        std::vector<int64_t> states((size_t)frames);
+        std::vector<double> fr((size_t)frames * (size_t)n * 8);
+        throw_status(gtd_system_recording(dev, nullptr, nullptr, states.data(), fr.data()));
+        int branch = 0;
+        for (int b : {1, 2, 4, 8, 16, 32, 64, 128})
+            if ((method & b) == b) { branch = b; break; }
+        constexpr bool coll = collisions != 0;
+        const int64_t n_e = (!coll && (branch == leapfrog_kdk || branch == leapfrog_dkd)) ? 1 : frames;
+        pe_rec.assign((size_t)n, {});
+        energy_rec.assign((size_t)n, {});
+        for (int64_t k = 0; k < frames; ++k) {
+            T tpe{}, tke{};
+            for (int64_t i = 0; i < n; ++i) {
+                const double *f = &fr[((size_t)k * n + i) * 8];
+                bod_t &b = bods[(size_t)i];
+                if (coll && k > 0) {
+                    b.positions.push_back(vector3D<T>{(T)f[0], (T)f[1], (T)f[2]});
+                    b.velocities.push_back(vector3D<T>{(T)f[3], (T)f[4], (T)f[5]});
+                    b.curr_ke = f[6];
+                    b.energies.push_back(b.curr_ke);
+                }
+                if (k < n_e) {
+                    pe_rec[(size_t)i].push_back((T)f[7]);
+                    energy_rec[(size_t)i].push_back((T)(b.curr_ke + f[7]));
+                    tpe += (T)f[7];
+                    tke += (T)b.curr_ke;
+                }
+            }
+            if (k < n_e) {
+                tot_pe.push_back(tpe);
+                tot_ke.push_back(tke);
+                tot_e.push_back(tpe + tke);
+            }
+        }
     }
     int coll_mode() const {
         if constexpr (collisions == overlap_coll_check) return mergeOverlappingBodies ? GTD_MERGE_COLL : GTD_OVERLAP_COLL;
@@ -159,9 +215,14 @@ public:
         double t_el = 0, step = 0, g = 0;
         throw_status(gtd_system_load_nsys(dev, nsys_path, check_nan_inf ? 1 : 0, (int)sizeof(M), (int)sizeof(R),
                                           (int)sizeof(T), &t_el, &step, G_vals, &g));
+        (void)g;
         time_elapsed = t_el;
         dt = step;
-        G = g;
+        // G from the stored units in long double, as load_from_nsys does (gregsys.hpp:1281-1284)
+        G = 66'743;
+        G *= G_vals[0] * G_vals[2] * G_vals[2] * G_vals[2] * G_vals[4] * G_vals[4];
+        G /= G_vals[1] * G_vals[3] * G_vals[3] * G_vals[3] * G_vals[5] * G_vals[5];
+        G /= 1'000'000'000'000'000;
         int64_t n = 0;
         throw_status(gtd_system_num_bodies(dev, &n));
         std::vector<double> m(n), r(n), e(n), x(3 * n), v(3 * n);
@@ -188,6 +249,14 @@ public:
         throw_status(gtd_system_check_overlap(dev, mergeOverlappingBodies ? 1 : 0, pair));
         if constexpr (mergeOverlappingBodies) pull();
     }
+
+    // ---- memFreq energy records of the last evolve (private in the reference; read here for
+    // checks): per body (body order) potential and total energies, and the system totals -------------
+    const std::vector<std::vector<T>> &recorded_pe() const noexcept { return pe_rec; }
+    const std::vector<std::vector<T>> &recorded_energy() const noexcept { return energy_rec; }
+    const std::vector<T> &recorded_total_pe() const noexcept { return tot_pe; }
+    const std::vector<T> &recorded_total_ke() const noexcept { return tot_ke; }
+    const std::vector<T> &recorded_total_e() const noexcept { return tot_e; }
 
     // ---- .nsys output (gregsys.hpp:3214-3258): returns the bytes written, 0 for a NULL path or a
     // file that cannot be opened ----------------------------------------------------------------------
@@ -297,15 +366,19 @@ public:
                                           const bodFuncT &for_each_bod = nullptr,
                                           const bodsFuncT &for_all_bods = nullptr) {
         if (bods.empty()) return std::chrono::nanoseconds::zero();
+        if constexpr (memFreq != 0)
+            for (bod_t &b : bods) b.clear_trajectory();  // clear_evolution (gregsys.hpp:2569-2586)
         push();
         if constexpr (std::same_as<evFuncT, std::nullptr_t> && std::same_as<bodFuncT, std::nullptr_t> &&
                       std::same_as<bodsFuncT, std::nullptr_t>) {
             int64_t ns = 0;
             throw_status(gtd_system_evolve(dev, integration_method, &ns));
             pull();
+            if constexpr (memFreq != 0) collect_recordings(integration_method);
             time_elapsed = iterations * dt;
             return std::chrono::nanoseconds{ns};
         } else {
+            static_assert(memFreq == 0, "memFreq recordings with evolve callbacks are not supported by the engine");
             // callbacks see the bodies every step: the state makes a host round trip per step
             const auto start = std::chrono::steady_clock::now();
             throw_status(gtd_system_evolve_begin(dev, integration_method));

@@ -106,6 +106,20 @@ GTD_API int gtd_system_num_bodies(const gtd_system *sys, int64_t *n);
  * uploaded bodies survived (their state holds the merged result). */
 GTD_API int gtd_system_survivors(gtd_system *sys, int64_t *upload_index);
 
+/* ---- trajectory frames (memFreq) -------------------------------------------------------------
+ * Replaces the recording of gtd::system<..., memFreq, ...> (body trajectories gregbod.hpp:304-320,
+ * per-body and total energies gregsys.hpp:219-227, 343-363, 439-476, 608-630).  With every != 0,
+ * each direct-summation evolve records a frame at its start and after every every-th step (after
+ * that step's collision pass); a frame holds, per body in download order, x, y, z, vx, vy, vz,
+ * ke = 0.5 m |v| |v| and pe = 0.5 sum_{j != i} -G m_i m_j / r_ij, computed on the device in FP64.
+ * Each evolve starts a new recording; Barnes-Hut evolves record nothing (as the reference).  Which
+ * of these values the reference keeps depends on the method and collision mode; the C++ and Python
+ * front ends apply its rules.  Merging collisions with recording return GTD_ERR_UNSUPPORTED.
+ * gtd_system_recording: frame count, bodies per frame, the step index of each frame (states,
+ * [frames]) and the frames (frame8, [frames][n][8]); pass NULL arrays to query the counts. */
+GTD_API int gtd_system_set_recording(gtd_system *sys, uint64_t every);
+GTD_API int gtd_system_recording(gtd_system *sys, int64_t *frames, int64_t *n, int64_t *states, double *frame8);
+
 /* ---- .nsys snapshots -------------------------------------------------------------------------
  * The reference's on-disk format (header gregsys.hpp:1444-1466, chunk :1467-1477): a 96-byte
  * header, then per body { char r_coeff[16]; M mass; R radius; T x, y, z, vx, vy, vz; } with natural

@@ -235,6 +235,10 @@ class RefOracle:
         L.ref_load_nsys.argtypes = [C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), _dp, _dp,
                                     _dp, _dp, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]
+        L.ref_evolve_record.restype = C.c_int
+        L.ref_evolve_record.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_uint64, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double,
+                                        C.c_uint64, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int), _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ref_bh_kdk_coll.restype = C.c_int
         L.ref_bh_kdk_coll.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_uint64, C.c_double,
                                       C.c_char_p, _dp, _dp]
@@ -360,3 +364,25 @@ class RefOracle:
         nn = n.value
         return 0, "", dict(m=m[:nn], r=r[:nn], rest=rest[:nn], x=x[:3 * nn].reshape(nn, 3),
                            v=v[:3 * nn].reshape(nn, 3), time=te.value, dt=dt.value, G=G.value)
+
+    def evolve_record(self, method, m, x, v, dt, steps, mem_freq, calls=1, r=None, rest=None, coll=0,
+                      units="M66743:66740,D1:1,T1:1", file_freq=0):
+        """evolve(method) of a system with memFreq = mem_freq (1, 2 or 3), `calls` times; returns the
+        last call's recordings: pos/vel [frames, n, 3], ke [frames, n], pe/energy [pe_frames, n],
+        totals [pe_frames, 3] (pe, ke, e), and the final x, v."""
+        n = len(m)
+        F = steps + 2
+        pos, vel = np.zeros(F * n * 3), np.zeros(F * n * 3)
+        ke, pe, en, tot = np.zeros(F * n), np.zeros(F * n), np.zeros(F * n), np.zeros(F * 3)
+        xo, vo = np.zeros(3 * n), np.zeros(3 * n)
+        pf, ef = C.c_int(), C.c_int()
+        r = np.zeros(n) if r is None else r
+        rest = np.ones(n) if rest is None else rest
+        self._chk(self.lib.ref_evolve_record(method, coll, mem_freq, file_freq, n, _c3(m), _c3(r), _c3(rest), _c3(x), _c3(v), dt,
+                                             steps,
+                                             units.encode(), calls, F, C.byref(pf), C.byref(ef), pos, vel, ke, pe, en,
+                                             tot, xo, vo))
+        p, e = pf.value, ef.value
+        return dict(pos=pos[:p * n * 3].reshape(p, n, 3), vel=vel[:p * n * 3].reshape(p, n, 3),
+                    ke=ke[:p * n].reshape(p, n), pe=pe[:e * n].reshape(e, n), energy=en[:e * n].reshape(e, n),
+                    tot=tot[:e * 3].reshape(e, 3), x=xo.reshape(n, 3), v=vo.reshape(n, 3))

@@ -53,6 +53,40 @@ public:
     template <typename B>
     static long double rest(const B &b) { return b.rest_c; }
 
+    /* The recordings of a system with memFreq != 0 (gregsys.hpp:219-227; gregbod.hpp:304-306):
+     * every body's positions/velocities/kinetic energies, the per-body pe and energy maps (keyed by
+     * body id) and the system totals.  Capacities in frames; returns the frame counts. */
+    template <typename S>
+    static void recordings(S &s, int max_frames, int *pos_frames, int *pe_frames, double *pos3, double *vel3,
+                           double *ke, double *pe, double *energy, double *tot3) {
+        const int n = (int)s.bods.size();
+        *pos_frames = n ? (int)s.bods[0].get_positions().size() : 0;
+        *pe_frames = (int)s.tot_pe.size();
+        for (int i = 0; i < n; ++i) {
+            const auto &b = s.bods[i];
+            const auto &P = b.get_positions();
+            const auto &V = b.get_velocities();
+            const auto &K = b.get_kinetic_energies();
+            for (int f = 0; f < (int)P.size() && f < max_frames; ++f) {
+                const size_t o = ((size_t)f * n + i);
+                pos3[3 * o] = (double)P[f].x; pos3[3 * o + 1] = (double)P[f].y; pos3[3 * o + 2] = (double)P[f].z;
+                vel3[3 * o] = (double)V[f].x; vel3[3 * o + 1] = (double)V[f].y; vel3[3 * o + 2] = (double)V[f].z;
+                ke[o] = (double)K[f];
+            }
+            const auto &PE = s.pe[b.id];
+            const auto &E = s.energy[b.id];
+            for (int f = 0; f < (int)PE.size() && f < max_frames; ++f) {
+                pe[(size_t)f * n + i] = (double)PE[f];
+                energy[(size_t)f * n + i] = (double)E[f];
+            }
+        }
+        for (int f = 0; f < *pe_frames && f < max_frames; ++f) {
+            tot3[3 * f] = (double)s.tot_pe[f];
+            tot3[3 * f + 1] = (double)s.tot_ke[f];
+            tot3[3 * f + 2] = (double)s.tot_e[f];
+        }
+    }
+
     /* DFS pre-order dump of a bh_tree, children in octant order 0..7 (greg8tree.hpp:74-76). */
     template <typename Tree, typename Bod>
     static long dump_tree(Tree &tree, const Bod *base, long max_nodes, int *depth, int *leaf_body,
@@ -482,6 +516,54 @@ int ref_load_nsys(int kind, const char *path, int alloc, int check, int max_n, i
         std::snprintf(g_err, sizeof g_err, "%s", e.what());
         return -3;
     }
+}
+
+}  // extern "C"
+
+/* evolve with trajectory recording: gtd::system<double,double,double,false,false,coll,MF,FF,false>,
+ * evolve(method) called `calls` times (a second call clears the first one's recordings,
+ * gregsys.hpp:2615-2619, 2569-2586); the recordings of the last call and the final state. */
+template <int coll, uint64_t MF, uint64_t FF>
+static int evolve_rec_impl(int method, int n, const double *m, const double *r, const double *rest, const double *x3,
+                           const double *v3, double dt, uint64_t steps, const char *units, int calls, int max_frames,
+                           int *pos_frames, int *pe_frames, double *pos3, double *vel3, double *ke, double *pe,
+                           double *energy, double *tot3, double *x3o, double *v3o) {
+    using sys_t = gtd::system<double, double, double, false, false, coll, MF, FF, false>;
+    using bod_t = gtd::body<double, double, double, MF>;
+    std::vector<bod_t> v;
+    v.reserve(n);
+    for (int i = 0; i < n; ++i)
+        v.emplace_back(m[i], r ? r[i] : 0.0, gtd::vector3D<double>{x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]},
+                       gtd::vector3D<double>{v3[3 * i], v3[3 * i + 1], v3[3 * i + 2]},
+                       rest ? (long double)rest[i] : 1.0L);
+    sys_t s{std::move(v), (long double)dt, steps, units, true};
+    for (int c = 0; c < calls; ++c) s.evolve(method);
+    ref_access::recordings(s, max_frames, pos_frames, pe_frames, pos3, vel3, ke, pe, energy, tot3);
+    read_back(s, x3o, v3o, nullptr, nullptr, nullptr);
+    return 0;
+}
+
+extern "C" {
+
+/* mem_freq 1, 2 or 3; coll 0 or 3; file_freq must be 0.  With memFreq and fileFreq both non-zero,
+ * evolve() does not compile (its Barnes-Hut Euler branch, gregsys.hpp:2640-2646, names members that
+ * do not exist); with fileFreq == 0, FUNC_TEMPL_SELECT (gregsys.hpp:15-16) always takes its
+ * non-recording branch, so only the energies of calc_acc_and_e / calc_energy are recorded. */
+int ref_evolve_record(int method, int coll, uint64_t mem_freq, uint64_t file_freq, int n, const double *m, const double *r,
+                      const double *rest, const double *x3, const double *v3, double dt, uint64_t steps,
+                      const char *units, int calls, int max_frames, int *pos_frames, int *pe_frames, double *pos3,
+                      double *vel3, double *ke, double *pe, double *energy, double *tot3, double *x3o, double *v3o) {
+    REF_TRY
+#define REC_CASE(C, F, FF)                                                                                      \
+    if (coll == C && mem_freq == F && file_freq == FF)                                                         \
+        return evolve_rec_impl<C, F, FF>(method, n, m, r, rest, x3, v3, dt, steps, units, calls, max_frames,   \
+                                         pos_frames, pe_frames, pos3, vel3, ke, pe, energy, tot3, x3o, v3o);
+    REC_CASE(0, 1, 0) REC_CASE(0, 2, 0) REC_CASE(0, 3, 0) REC_CASE(3, 1, 0) REC_CASE(3, 2, 0) REC_CASE(3, 3, 0)
+#undef REC_CASE
+    std::snprintf(g_err, sizeof g_err, "unsupported coll %d / mem_freq %llu / file_freq %llu", coll,
+                  (unsigned long long)mem_freq, (unsigned long long)file_freq);
+    return -1;
+    REF_CATCH
 }
 
 /* ref_bh_kdk with the reference's bh_s_coll after every full kick: a

@@ -91,6 +91,19 @@ int main() {
         std::printf("octree leaf order matches host rebuild: %d\n", (int)same);
         fails += !same;
     }
+    {  // memFreq recordings (collisions on: the reference records trajectories through s_coll)
+        using rsys_t = gtd::system<double, double, double, false, false, 3, 2, 0, false>;
+        const auto ci = make(64, 17, 1.5e10);
+        std::vector<rsys_t::bod_t> rb;
+        for (const auto &b : ci) rb.emplace_back(b.mass(), b.rad(), b.pos(), b.vel(), b.restitution());
+        rsys_t s{rb, 3600, 6, "M66743:66740,D1:1,T1:1", true};
+        s.evolve(rsys_t::leapfrog_kdk);
+        const auto &P = s[0].get_positions();
+        bool ok = P.size() == 4 && s[0].get_kinetic_energies().size() == 4 && s.recorded_total_e().size() == 4 &&
+                  s.recorded_pe().size() == 64 && P.back().x == s[0].pos().x && P.front().x == ci[0].pos().x;
+        std::printf("memFreq recordings: %d\n", (int)ok);
+        fails += !ok;
+    }
     {  // .nsys round trip: to_nsys, then the path constructor (gregsys.hpp:3214-3258, 1479-1490)
         const auto ni = make(100, 15, 1.0);
         sys_t s{ni, 3600, 3, "M66743:66740,D1:1,T1:1", true};

@@ -37,6 +37,27 @@ def _set_x87(off, val):
     return _mut(lambda b: b.__setitem__(slice(off, off + 16), np.array([val], dtype=np.longdouble).tobytes()))
 
 
+def record_fixtures(r, out):
+    """memFreq recordings of the reference (fileFreq = 0, the only setting with which its evolve
+    compiles): every direct method, memFreq 1, 2 and 3, collisions off (Plummer sphere) and on (the
+    colliding "coll" cluster), one evolve call or two (the second clears the first's recordings);
+    7 steps of one hour."""
+    for meth_name, meth in METHODS.items():
+        for f in (1, 2, 3):
+            for coll in (0, 3):
+                for calls in (1, 2):
+                    if coll:
+                        args = dict(r=out["coll_r"], rest=out["coll_rest"], coll=3)
+                        m, x, v = out["coll_m"], out["coll_x"], out["coll_v"]
+                    else:
+                        args = {}
+                        m, x, v = out["direct_m"], out["direct_x"], out["direct_v"]
+                    d = r.evolve_record(meth, m, x, v, 3600.0, 7, f, calls, units=UNITS_G6674, **args)
+                    key = f"rec_{meth_name}_{f}_{coll}_{calls}"
+                    for k in ("pos", "vel", "ke", "pe", "energy", "tot", "x", "v"):
+                        out[f"{key}_{k}"] = d[k]
+
+
 def nsys_fixtures(r, out):
     """.nsys files written by the reference's to_nsys (after 3 KDK steps) for four M/R/T choices,
     the state its loader reads back, and corrupted copies with the reference loader's verdicts
@@ -193,6 +214,7 @@ def main():
     out["bhck_m"], out["bhck_r"], out["bhck_rest"], out["bhck_x"], out["bhck_v"] = mk, rk, ek, xk, vk
     out["bhck_xo"], out["bhck_vo"] = r.bh_kdk_coll(mk, rk, ek, xk, vk, 3600.0, 5, 0.5, UNITS_G6674)
     nsys_fixtures(r, out)
+    record_fixtures(r, out)
     path = os.path.join(HERE, "reference_golden.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes,", len(out), "arrays")
