@@ -607,6 +607,7 @@ def run_ensemble(args, local):
             "unit": "ensemble steps/s", "value": (len(off) - 1) * K / secs, "system_steps_per_s": (len(off) - 1) * K / secs,
             "steps": K, "ms_per_step": 1e3 * secs / K, "pair_interactions_per_s": inter * K / secs,
             "bodies": int(off[-1]), "merges_during_timed": int(merges - merges0), "autotuned_threads": threads,
+            "bodies_per_thread": e.config()[1],
             "gpu_launches": int(l1 - l0), "launch": "one persistent launch per step, replayed from a CUDA graph"}
     try:
         from oracle.oracle import RefOracle

@@ -134,6 +134,8 @@ def load():
     L.gtd_ensemble_counts.argtypes = [vp, dp, C.POINTER(u64), C.POINTER(u64)]
     L.gtd_ensemble_download.argtypes = [vp, dp, dp, dp, dp, dp, dp]
     L.gtd_ensemble_set_threads.argtypes = [vp, ip]
+    L.gtd_ensemble_set_bodies_per_thread.argtypes = [vp, ip]
+    L.gtd_ensemble_config.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.gtd_ensemble_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.gtd_direct_variant_count.argtypes = [ip, C.POINTER(C.c_int)]
     L.gtd_direct_variant_info.argtypes = [ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int)]

@@ -31,6 +31,7 @@ struct gtd_ensemble {
     double G = 6.6743e-11, dt = 1.0;
     int merge = 1;
     int threads = 256;   // CTA size (autotuned)
+    int ib = 1;          // bodies per thread in the force loop (autotuned; 2 needs threads <= 256)
     int blocks_per_sm = 0;
     int64_t n_sys = 0, n_bodies = 0;
     int max_n = 0;
@@ -156,8 +157,86 @@ __device__ int ens_merge_scan(int n, double4 *pos, double4 *vel, double4 *acc, d
     return out;
 }
 
-// One launch = one KDK step (or the initial force) for every system.
-__global__ void __launch_bounds__(512) ensemble_step_kernel(EnsArgs a) {
+// Forces on the IB bodies i0, i0 + T, ... (those below nc) of a staged system: each staged j pair is
+// read from shared memory once for all IB bodies.  Returns whether any of them may overlap another.
+template <int IB>
+__device__ __forceinline__ int ens_force_rows(int i0, int T, int nc, int npad, const float *sx, const float *sy,
+                                              const float *sz, const float *sm, double4 *pos, double4 *vel,
+                                              double4 *acc, const double *rad, float rmx, bool kick, double h2) {
+    const float2 *X2 = reinterpret_cast<const float2 *>(sx);
+    const float2 *Y2 = reinterpret_cast<const float2 *>(sy);
+    const float2 *Z2 = reinterpret_cast<const float2 *>(sz);
+    const float2 *M2 = reinterpret_cast<const float2 *>(sm);
+    float2 nx[IB], ny[IB], nz[IB];
+    double ax[IB], ay[IB], az[IB];
+    unsigned mnr[IB];
+#pragma unroll
+    for (int b = 0; b < IB; ++b) {
+        const int i = i0 + b * T;
+        const int ic = i < nc ? i : i0;  // a missing second body repeats the first; its result is dropped
+        nx[b] = make_float2(-sx[ic], -sx[ic]);
+        ny[b] = make_float2(-sy[ic], -sy[ic]);
+        nz[b] = make_float2(-sz[ic], -sz[ic]);
+        ax[b] = ay[b] = az[b] = 0.0;
+        mnr[b] = 0xffffffffu;  // min over j != i of r2 bits, the self pair (r2 = 0) excluded
+    }
+    for (int q0 = 0; q0 < npad / 2; q0 += kEnsFold / 2) {
+        const int q1 = min(q0 + kEnsFold / 2, npad / 2);
+        float2 fx[IB], fy[IB], fz[IB];
+#pragma unroll
+        for (int b = 0; b < IB; ++b) fx[b] = fy[b] = fz[b] = make_float2(0.f, 0.f);
+#pragma unroll 4
+        for (int q = q0; q < q1; ++q) {
+            const float2 X = X2[q], Y = Y2[q], Z = Z2[q], M = M2[q];
+#pragma unroll
+            for (int b = 0; b < IB; ++b) {
+                const float2 dx = __fadd2_rn(X, nx[b]), dy = __fadd2_rn(Y, ny[b]), dz = __fadd2_rn(Z, nz[b]);
+                float2 r2 = __fmul2_rn(dx, dx);
+                r2 = __ffma2_rn(dy, dy, r2);
+                r2 = __ffma2_rn(dz, dz, r2);
+                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.x) - 1u);
+                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.y) - 1u);
+                // the self pair has r2 == 0: clamping to 1 mm^2 makes its term exactly 0
+                const float2 inv = make_float2(ens_rsqrt(fmaxf(r2.x, 1e-6f)), ens_rsqrt(fmaxf(r2.y, 1e-6f)));
+                const float2 inv2 = __fmul2_rn(inv, inv);
+                float2 sc = __fmul2_rn(M, inv);
+                sc = __fmul2_rn(sc, inv2);
+                fx[b] = __ffma2_rn(dx, sc, fx[b]);
+                fy[b] = __ffma2_rn(dy, sc, fy[b]);
+                fz[b] = __ffma2_rn(dz, sc, fz[b]);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < IB; ++b) {
+            ax[b] += (double)fx[b].x + (double)fx[b].y;
+            ay[b] += (double)fy[b].x + (double)fy[b].y;
+            az[b] += (double)fz[b].x + (double)fz[b].y;
+        }
+    }
+    int flagged = 0;
+#pragma unroll
+    for (int b = 0; b < IB; ++b) {
+        const int i = i0 + b * T;
+        if (i >= nc) continue;
+        if (mnr[b] != 0xffffffffu) {  // some other body exists
+            const float mind2 = __int_as_float((int)(mnr[b] + 1u));
+            const float reach = (float)rad[i] + rmx;
+            if (mind2 < reach * reach * 1.0001f) flagged = 1;
+        }
+        if (kick) {
+            double4 v = vel[i];
+            v.x = fma(h2, ax[b], v.x); v.y = fma(h2, ay[b], v.y); v.z = fma(h2, az[b], v.z);
+            vel[i] = v;
+        }
+        acc[i] = make_double4(ax[b], ay[b], az[b], 0.0);
+    }
+    return flagged;
+}
+
+// One launch = one KDK step (or the initial force) for every system.  IB bodies per thread (1 or 2;
+// with 2 each staged j pair feeds two bodies, halving the shared-memory reads per interaction).
+template <int IB>
+__global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *sx = reinterpret_cast<float *>(smem_raw);
     float *sy = sx + a.stride;
@@ -235,52 +314,10 @@ __global__ void __launch_bounds__(512) ensemble_step_kernel(EnsArgs a) {
                 }
             }
             __syncthreads();
-            const float2 *X2 = reinterpret_cast<const float2 *>(sx);
-            const float2 *Y2 = reinterpret_cast<const float2 *>(sy);
-            const float2 *Z2 = reinterpret_cast<const float2 *>(sz);
-            const float2 *M2 = reinterpret_cast<const float2 *>(sm);
             int flagged = 0;
-            for (int i = t; i < nc; i += T) {
-                const float xi = sx[i], yi = sy[i], zi = sz[i];
-                const float2 nx = make_float2(-xi, -xi), ny = make_float2(-yi, -yi), nz = make_float2(-zi, -zi);
-                double ax = 0.0, ay = 0.0, az = 0.0;
-                unsigned mnr = 0xffffffffu;  // min over j != i of r2 bits, the self pair (r2 = 0) excluded
-                for (int q0 = 0; q0 < npad / 2; q0 += kEnsFold / 2) {
-                    const int q1 = min(q0 + kEnsFold / 2, npad / 2);
-                    float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
-#pragma unroll 4
-                    for (int q = q0; q < q1; ++q) {
-                        const float2 dx = __fadd2_rn(X2[q], nx), dy = __fadd2_rn(Y2[q], ny), dz = __fadd2_rn(Z2[q], nz);
-                        float2 r2 = __fmul2_rn(dx, dx);
-                        r2 = __ffma2_rn(dy, dy, r2);
-                        r2 = __ffma2_rn(dz, dz, r2);
-                        mnr = min(mnr, (unsigned)__float_as_int(r2.x) - 1u);
-                        mnr = min(mnr, (unsigned)__float_as_int(r2.y) - 1u);
-                        // the self pair has r2 == 0: clamping to 1 mm^2 makes its term exactly 0
-                        const float2 inv = make_float2(ens_rsqrt(fmaxf(r2.x, 1e-6f)), ens_rsqrt(fmaxf(r2.y, 1e-6f)));
-                        const float2 inv2 = __fmul2_rn(inv, inv);
-                        float2 sc = __fmul2_rn(M2[q], inv);
-                        sc = __fmul2_rn(sc, inv2);
-                        fx = __ffma2_rn(dx, sc, fx);
-                        fy = __ffma2_rn(dy, sc, fy);
-                        fz = __ffma2_rn(dz, sc, fz);
-                    }
-                    ax += (double)fx.x + (double)fx.y;
-                    ay += (double)fy.x + (double)fy.y;
-                    az += (double)fz.x + (double)fz.y;
-                }
-                if (mnr != 0xffffffffu) {  // some other body exists
-                    const float mind2 = __int_as_float((int)(mnr + 1u));
-                    const float reach = (float)rad[i] + rmx;
-                    if (mind2 < reach * reach * 1.0001f) flagged = 1;
-                }
-                if (a.kdk && first) {
-                    double4 v = vel[i];
-                    v.x = fma(h2, ax, v.x); v.y = fma(h2, ay, v.y); v.z = fma(h2, az, v.z);
-                    vel[i] = v;
-                }
-                acc[i] = make_double4(ax, ay, az, 0.0);
-            }
+            for (int i0 = t; i0 < nc; i0 += IB * T)
+                flagged |= ens_force_rows<IB>(i0, T, nc, npad, sx, sy, sz, sm, pos, vel, acc, rad, rmx, a.kdk && first,
+                                              h2);
             flagged = __syncthreads_or(flagged);
             if (!first || !flagged || !a.merge) break;
             const int nn = ens_merge_scan(nc, pos, vel, acc, rad, a.rest + b0, a.ids + b0, sh);
@@ -319,11 +356,17 @@ static int ens_launch(gtd_ensemble *e, int kdk) {
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e->device);
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_step_kernel, e->threads, smem);
+    if (e->ib == 2)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_step_kernel<2>, e->threads, smem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_step_kernel<1>, e->threads, smem);
     if (per_sm < 1) per_sm = 1;
     const int grid = (int)std::min<int64_t>((int64_t)dev_sms * per_sm, std::max<int64_t>(e->n_sys, 1));
     GTD_CUDA(cudaMemsetAsync(e->work, 0, sizeof(unsigned), e->stream));
-    ensemble_step_kernel<<<grid, e->threads, smem, e->stream>>>(a);
+    if (e->ib == 2)
+        ensemble_step_kernel<2><<<grid, e->threads, smem, e->stream>>>(a);
+    else
+        ensemble_step_kernel<1><<<grid, e->threads, smem, e->stream>>>(a);
     GTD_CHECK_LAUNCH();
     e->launches += 1;
     return GTD_OK;
@@ -348,7 +391,7 @@ static int ens_build_graph(gtd_ensemble *e, int steps) {
     cudaGraphDestroy(g);
     if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate", __FILE__, __LINE__);
     e->graph_steps = steps;
-    e->graph_threads = e->threads;
+    e->graph_threads = e->threads * 4 + e->ib;
     return GTD_OK;
 }
 
@@ -360,7 +403,7 @@ static int ens_steps(gtd_ensemble *e, uint64_t steps) {
     }
     const int chunk = 16;
     if (steps >= (uint64_t)chunk) {
-        if (!e->graph || e->graph_steps != chunk || e->graph_threads != e->threads) {
+        if (!e->graph || e->graph_steps != chunk || e->graph_threads != e->threads * 4 + e->ib) {
             int rc = ens_build_graph(e, chunk);
             if (rc) return rc;
         }
@@ -395,7 +438,9 @@ int gtd_ensemble_create(gtd_ensemble **out, int device) {
     GTD_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     GTD_CUDA(cudaEventCreate(&e->ev0));
     GTD_CUDA(cudaEventCreate(&e->ev1));
-    GTD_CUDA(cudaFuncSetAttribute(ensemble_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    GTD_CUDA(cudaFuncSetAttribute(ensemble_step_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  ens_smem_bytes(kEnsMaxN)));
+    GTD_CUDA(cudaFuncSetAttribute(ensemble_step_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   ens_smem_bytes(kEnsMaxN)));
     *out = e;
     return GTD_OK;
@@ -555,7 +600,24 @@ int gtd_ensemble_set_threads(gtd_ensemble *e, int threads) {
     if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
     if (threads != 64 && threads != 128 && threads != 256 && threads != 512)
         return fail(GTD_ERR_INVALID_ARGUMENT, "threads must be 64, 128, 256 or 512");
+    if (e->ib == 2 && threads > 256) e->ib = 1;
     e->threads = threads;
+    return GTD_OK;
+}
+
+int gtd_ensemble_set_bodies_per_thread(gtd_ensemble *e, int bodies) {
+    if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
+    if (bodies != 1 && bodies != 2) return fail(GTD_ERR_INVALID_ARGUMENT, "bodies per thread must be 1 or 2");
+    if (bodies == 2 && e->threads > 256)
+        return fail(GTD_ERR_INVALID_ARGUMENT, "2 bodies per thread need a CTA of at most 256 threads");
+    e->ib = bodies;
+    return GTD_OK;
+}
+
+int gtd_ensemble_config(const gtd_ensemble *e, int *threads, int *bodies_per_thread) {
+    if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
+    if (threads) *threads = e->threads;
+    if (bodies_per_thread) *bodies_per_thread = e->ib;
     return GTD_OK;
 }
 
@@ -589,12 +651,14 @@ int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
     };
     int rc = save(false);
     const bool was_begun = e->begun;
-    const int cands[] = {128, 256, 512};
-    int best = e->threads;
+    const int cands[][2] = {{128, 1}, {256, 1}, {512, 1}, {128, 2}, {256, 2}};
+    int best = e->threads, best_ib = e->ib;
     double bestv = 1e300;
-    for (int c : cands) {
+    for (const auto &cf : cands) {
         if (rc) break;
+        const int c = cf[0];
         e->threads = c;
+        e->ib = cf[1];
         for (int rep = 0; rep < 3 && !rc; ++rep) {
             if ((rc = cudaEventRecord(e->ev0, e->stream) ? GTD_ERR_CUDA : GTD_OK)) break;
             rc = ens_launch(e, 1);
@@ -606,11 +670,13 @@ int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
             if (rep > 0 && ms < bestv) {
                 bestv = ms;
                 best = c;
+                best_ib = cf[1];
             }
             if (!rc) rc = save(true);
         }
     }
     e->threads = best;
+    e->ib = best_ib;
     e->begun = was_begun;
     cudaStreamSynchronize(e->stream);
     cudaFree(sp); cudaFree(sv); cudaFree(sa); cudaFree(sr); cudaFree(se); cudaFree(si); cudaFree(sc);

@@ -49,6 +49,15 @@ class Ensemble:
     def set_threads(self, threads: int) -> None:
         check(self._L.gtd_ensemble_set_threads(self._h, int(threads)))
 
+    def set_bodies_per_thread(self, bodies: int) -> None:
+        check(self._L.gtd_ensemble_set_bodies_per_thread(self._h, int(bodies)))
+
+    def config(self) -> tuple:
+        """(CTA threads, bodies per thread) of the step kernel."""
+        t, b = C.c_int(), C.c_int()
+        check(self._L.gtd_ensemble_config(self._h, C.byref(t), C.byref(b)))
+        return t.value, b.value
+
     def counts(self):
         c = np.zeros(self.n_systems, np.int64)
         merges, launches = C.c_uint64(), C.c_uint64()

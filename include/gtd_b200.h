@@ -255,9 +255,12 @@ GTD_API int gtd_ensemble_counts(gtd_ensemble *ens, int64_t *counts, uint64_t *me
  * in upload order. */
 GTD_API int gtd_ensemble_download(gtd_ensemble *ens, double *m, double *r, double *rest, double *x3, double *v3,
                                   double *a3);
-/* CTA size of the step kernel (64, 128, 256 or 512), or let the autotuner time 128/256/512 on the
- * current state (restored afterwards) and keep the fastest. */
+/* CTA size of the step kernel (64, 128, 256 or 512) and bodies per thread in its force loop (1, or
+ * 2 with at most 256 threads), or let the autotuner time (128|256|512, 1) and (128|256, 2) on the
+ * current state (restored afterwards) and keep the fastest; gtd_ensemble_config reads the choice. */
 GTD_API int gtd_ensemble_set_threads(gtd_ensemble *ens, int threads);
+GTD_API int gtd_ensemble_set_bodies_per_thread(gtd_ensemble *ens, int bodies);
+GTD_API int gtd_ensemble_config(const gtd_ensemble *ens, int *threads, int *bodies_per_thread);
 GTD_API int gtd_ensemble_autotune(gtd_ensemble *ens, int *best_threads, double *best_ms);
 
 /* ---- adjoint of the FP64 leapfrog KDK evolve (no counterpart in the reference) ---------------

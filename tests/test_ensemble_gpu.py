@@ -86,9 +86,32 @@ def test_autotune_restores_state(gpu):
     a.evolve(3)
     b = Ensemble(off, m, x, v, r, merge=True, dt=DT)
     b.set_threads(t)
+    b.set_bodies_per_thread(a.config()[1])
     b.evolve(3)
     sa, sb = a.state(), b.state()
     assert all(np.array_equal(sa[s]["x"], sb[s]["x"]) for s in range(64))
+
+
+def test_two_bodies_per_thread_is_bit_identical(gpu):
+    """The force loop with 2 bodies per thread performs, per body, the same operations in the same
+    order as with 1: the trajectories (merges included) are bit-identical."""
+    off, m, r, x, v = ensemble(48, 75, n_min=3, n_max=1500)
+    runs = []
+    for threads, ib in ((256, 1), (256, 2), (128, 2)):
+        e = Ensemble(off, m, x, v, r, merge=True, dt=DT)
+        e.set_threads(threads)
+        e.set_bodies_per_thread(ib)
+        assert e.config() == (threads, ib)
+        e.evolve(20)
+        runs.append((e.state(), e.counts()[0]))
+    for st, cnt in runs[1:]:
+        assert np.array_equal(cnt, runs[0][1])
+        for s in range(48):
+            assert np.array_equal(st[s]["x"], runs[0][0][s]["x"]) and np.array_equal(st[s]["v"], runs[0][0][s]["v"])
+    e = Ensemble(off, m, x, v, r, merge=True, dt=DT)
+    e.set_threads(512)
+    with pytest.raises(ValueError):
+        e.set_bodies_per_thread(2)
 
 
 def test_capacity_limit(gpu):
