@@ -107,6 +107,10 @@ struct gtd_system {
     void *nsys_dev = nullptr, *nsys_host = nullptr;
     size_t nsys_dev_bytes = 0, nsys_host_bytes = 0;
 
+    // host-array staging on the device (io.cu)
+    void *io_dev = nullptr;
+    size_t io_bytes = 0;
+
     // trajectory frames (record.cu): every rec_every-th state of a direct-summation evolve
     uint64_t rec_every = 0;
     uint64_t rec_step = 0;               // steps since evolve_begin
@@ -144,6 +148,11 @@ int copy_acc_out(gtd_system *s, double *a3);
 void release_collide(gtd_system *s);
 void release_nsys(gtd_system *s);
 void release_record(gtd_system *s);
+void release_io(gtd_system *s);
+// caller's arrays (upload order) <-> device bodies, converted on the device (io.cu)
+int device_upload(gtd_system *s, int64_t n, const double *m, const double *r, const double *rest, const double *x3,
+                  const double *v3);
+int device_download(gtd_system *s, double *m, double *r, double *rest, double *x3, double *v3, double *a3);
 int record_frame(gtd_system *s, uint64_t state);
 int ensure_body_capacity(gtd_system *s, int64_t n);
 int set_loaded_bodies(gtd_system *s, int64_t n);

@@ -408,6 +408,7 @@ int gtd_system_destroy(gtd_system *s) {
     release_collide(s);
     release_nsys(s);
     release_record(s);
+    release_io(s);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     cudaEventDestroy(s->ev0);
     cudaEventDestroy(s->ev1);
@@ -458,28 +459,11 @@ int gtd_system_upload(gtd_system *s, int64_t n, const double *m, const double *r
     s->ordered = false;
     s->steps_since_reorder = 0;
     if (n == 0) return GTD_OK;
-    for (int64_t i = 0; i < n; ++i) {
-        if (m[i] < 0) return fail(GTD_ERR_INVALID_ARGUMENT, "negative mass at body %lld", (long long)i);
-        if (r && r[i] < 0) return fail(GTD_ERR_INVALID_ARGUMENT, "negative radius at body %lld", (long long)i);
+    rc = device_upload(s, n, m, r, rest, x3, v3);
+    if (rc) {  // a negative mass or radius: leave the handle empty
+        s->n = s->n_uploaded = 0;
+        return rc;
     }
-    double4 *hp = s->stage, *hv = s->stage + n;
-    double *hr = reinterpret_cast<double *>(s->stage + 2 * n), *he = hr + n;
-    int32_t *hid = reinterpret_cast<int32_t *>(s->stage + 3 * n);
-    for (int64_t i = 0; i < n; ++i) {
-        hp[i] = make_double4(x3[3 * i], x3[3 * i + 1], x3[3 * i + 2], m[i]);
-        hv[i] = v3 ? make_double4(v3[3 * i], v3[3 * i + 1], v3[3 * i + 2], 0.0) : make_double4(0, 0, 0, 0);
-        hr[i] = r ? r[i] : 0.0;
-        he[i] = rest ? rest[i] : 1.0;
-        hid[i] = (int32_t)i;
-    }
-    const size_t b4 = sizeof(double4) * (size_t)n;
-    GTD_CUDA(cudaMemcpyAsync(s->pm[0], hp, b4, cudaMemcpyHostToDevice, s->stream));
-    GTD_CUDA(cudaMemcpyAsync(s->vel, hv, b4, cudaMemcpyHostToDevice, s->stream));
-    GTD_CUDA(cudaMemcpyAsync(s->rad, hr, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s->stream));
-    GTD_CUDA(cudaMemcpyAsync(s->rest, he, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s->stream));
-    GTD_CUDA(cudaMemcpyAsync(s->ids, hid, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, s->stream));
-    GTD_CUDA(cudaMemsetAsync(s->acc, 0, b4, s->stream));
-    GTD_CUDA(cudaStreamSynchronize(s->stream));
     return GTD_OK;
 }
 
@@ -509,49 +493,13 @@ int gtd_system_download(gtd_system *s, int64_t *n_out, double *m, double *r, dou
     const int64_t n = s->n;
     if (n_out) *n_out = n;
     if (n == 0) return GTD_OK;
-    double4 *hp = s->stage, *hv = s->stage + n, *ha = s->stage + 2 * n;
-    double *hr = reinterpret_cast<double *>(s->stage + 3 * n), *he = hr + n;
-    const size_t b4 = sizeof(double4) * (size_t)n;
-    GTD_CUDA(cudaMemcpyAsync(hp, s->pm[s->cur], b4, cudaMemcpyDeviceToHost, s->stream));
-    if (v3) GTD_CUDA(cudaMemcpyAsync(hv, s->vel, b4, cudaMemcpyDeviceToHost, s->stream));
-    if (a3) GTD_CUDA(cudaMemcpyAsync(ha, s->acc, b4, cudaMemcpyDeviceToHost, s->stream));
-    if (r) GTD_CUDA(cudaMemcpyAsync(hr, s->rad, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
-    if (rest) GTD_CUDA(cudaMemcpyAsync(he, s->rest, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
-    GTD_CUDA(cudaStreamSynchronize(s->stream));
-    std::vector<int64_t> row;
-    int rc = output_rows(s, row);
-    if (rc) return rc;
-    for (int64_t i = 0; i < n; ++i) {
-        const int64_t o = row[(size_t)i];
-        if (m) m[o] = hp[i].w;
-        if (x3) { x3[3 * o] = hp[i].x; x3[3 * o + 1] = hp[i].y; x3[3 * o + 2] = hp[i].z; }
-        if (v3) { v3[3 * o] = hv[i].x; v3[3 * o + 1] = hv[i].y; v3[3 * o + 2] = hv[i].z; }
-        if (a3) { a3[3 * o] = ha[i].x; a3[3 * o + 1] = ha[i].y; a3[3 * o + 2] = ha[i].z; }
-        if (r) r[o] = hr[i];
-        if (rest) rest[o] = he[i];
-    }
-    return GTD_OK;
+    return device_download(s, m, r, rest, x3, v3, a3);
 }
 
 }  // extern "C"
 
 // Device acceleration array -> host triples in host row order.
-int copy_acc_out(gtd_system *s, double *a3) {
-    const int64_t n = s->n;
-    std::vector<double4> h((size_t)n);
-    GTD_CUDA(cudaMemcpyAsync(h.data(), s->acc, sizeof(double4) * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
-    GTD_CUDA(cudaStreamSynchronize(s->stream));
-    std::vector<int64_t> row;
-    int rc = output_rows(s, row);
-    if (rc) return rc;
-    for (int64_t i = 0; i < n; ++i) {
-        const int64_t o = row[(size_t)i];
-        a3[3 * o] = h[i].x;
-        a3[3 * o + 1] = h[i].y;
-        a3[3 * o + 2] = h[i].z;
-    }
-    return GTD_OK;
-}
+int copy_acc_out(gtd_system *s, double *a3) { return device_download(s, nullptr, nullptr, nullptr, nullptr, nullptr, a3); }
 
 extern "C" {
 
