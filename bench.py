@@ -67,6 +67,8 @@ def parse_args():
     p.add_argument("--bh-n", type=int, default=4194304)
     p.add_argument("--bh-cpu-n", type=int, default=10000)
     p.add_argument("--ens-systems", type=int, default=4096)
+    p.add_argument("--ens-config", type=str, default="",
+                   help="THREADS,BODIES_PER_THREAD for the ensemble kernel instead of the autotuner's choice")
     p.add_argument("--adj-n", type=int, default=16384)
     p.add_argument("--adj-steps", type=int, default=2000)
     p.add_argument("--adj-every", type=int, default=45)
@@ -595,7 +597,12 @@ def run_ensemble(args, local):
     from gregpackagescpp_b200.ics import ensemble
     off, m, r, x, v = ensemble(args.ens_systems, 4)
     e = Ensemble(off, m, x, v, r, merge=True, dt=600.0, device=local)
-    threads, tune_ms = e.autotune()
+    if args.ens_config:
+        threads, ib = (int(t) for t in args.ens_config.split(","))
+        e.set_threads(threads)
+        e.set_bodies_per_thread(ib)
+    else:
+        threads, tune_ms = e.autotune()
     e.evolve(args.warmup)
     counts0, merges0, l0 = e.counts()
     K = max(args.steps, 16)
