@@ -207,3 +207,17 @@ def test_bh_collisions_vs_oracle(gpu, oracle, tree_float):
     assert np.abs(s.x - xo).max() / np.abs(xo).max() < 1e-12
     assert np.abs(s.v - vo).max() / np.abs(vo).max() < 1e-10
     assert np.abs(vo - v).max() > 1.0  # the collisions changed the velocities
+
+
+def test_topology_full_size(gpu, oracle):
+    """The Barnes-Hut workload's size: two Plummer spheres of 2^21 bodies.  Codes, order, depths,
+    skips, widths and FP64 moments bit-exact against the host rebuild, and every body in exactly
+    one leaf (counts of the leaves sum to N)."""
+    m, x, _ = two_plummer(1 << 21, 1)
+    s, t = gpu_tree(m, x, 1)
+    o = oracle.bh_tree(x, m, 1)
+    try:
+        compare_tree(t, o)
+        assert int(t["count"][t["is_leaf"] == 1].sum()) == len(m)
+    finally:
+        oracle.bh_free(o)
