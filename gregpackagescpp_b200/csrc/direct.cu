@@ -38,9 +38,12 @@ __device__ __forceinline__ void cta_range(const ForceKArgs &a, int g, int64_t &s
 // FP64: a_i = sum_j G m_j (x_j - x_i) / |x_j - x_i|^3, no softening (the reference's direct path
 // ignores eps).  The i == j term has r2 == 0 and is dropped by the select on inv.
 // -------------------------------------------------------------------------------------------
-template <int I>
+// BJ: j-bodies per work unit (a row of bi = 256 I bodies against BJ j-bodies).  Narrow units (BJ 32
+// or 64) let a small system spread over every SM: at N = 1024 the 256-wide units give 8 CTAs.
+template <int I, int BJ = kThreads>
 __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
-    __shared__ double4 tile[2][kThreads];
+    static_assert(BJ <= kThreads && kThreads % BJ == 0, "BJ divides the CTA size");
+    __shared__ double4 tile[2][BJ];
     const int t = threadIdx.x;
     int64_t s, e;
     cta_range(a, blockIdx.x, s, e);
@@ -58,8 +61,8 @@ __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
             xi[k] = p.x; yi[k] = p.y; zi[k] = p.z;
             ax[k] = 0.0; ay[k] = 0.0; az[k] = 0.0;
         }
-        {
-            const int64_t j = jt0 * kThreads + t;
+        if (t < BJ) {
+            const int64_t j = jt0 * BJ + t;
             double4 q = j < a.n ? a.src[j] : zero;
             q.w *= a.G;
             tile[0][t] = q;
@@ -69,12 +72,12 @@ __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
         for (int64_t jt = jt0; jt < jt1; ++jt) {
             const bool more = jt + 1 < jt1;
             double4 qn = zero;
-            if (more) {
-                const int64_t j = (jt + 1) * kThreads + t;
+            if (more && t < BJ) {
+                const int64_t j = (jt + 1) * BJ + t;
                 if (j < a.n) qn = a.src[j];
             }
 #pragma unroll 4
-            for (int jj = 0; jj < kThreads; ++jj) {
+            for (int jj = 0; jj < BJ; ++jj) {
                 const double4 q = tile[cur][jj];
 #pragma unroll
                 for (int k = 0; k < I; ++k) {
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
                     az[k] = fma(sc, dz, az[k]);
                 }
             }
-            if (more) {
+            if (more && t < BJ) {
                 qn.w *= a.G;
                 tile[cur ^ 1][t] = qn;
             }
@@ -350,11 +353,12 @@ __global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs 
 // times them all on the caller's bodies and keeps the fastest.
 struct VariantInfo {
     int i, fold;
+    int bj = kThreads;  // j-bodies per work unit
 };
 // mixed: {I, FOLD}; the launch bound (blocks per SM) and where the Kahan sums live are in with_mixed
 static const VariantInfo kMixedVariants[] = {{2, 64}, {4, 128}, {2, 64}, {2, 128}, {2, 64},
                                              {2, 128}, {1, 64},  {2, 64},  {4, 128}};
-static const VariantInfo kF64Variants[] = {{2, 0}, {1, 0}, {4, 0}};
+static const VariantInfo kF64Variants[] = {{2, 0}, {1, 0}, {4, 0}, {1, 0, 64}, {1, 0, 32}};
 constexpr int kNumMixed = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
 constexpr int kNumF64 = sizeof(kF64Variants) / sizeof(kF64Variants[0]);
 
@@ -362,9 +366,11 @@ int variant_count(int precision) { return precision == GTD_PREC_MIXED ? kNumMixe
 
 // Variant for a handle nobody tuned.  From N ~ 32768 up the mixed kernel is fastest with 4 i-bodies
 // per thread at 1 CTA/SM (<4,128,1,regs,U4>, variant 8: 27.4 ms against 29.1 ms for variant 0 at
-// N = 262144 on B200); below that the 2-per-thread variants keep more CTAs busy.
+// N = 262144 on B200); below that the 2-per-thread variants keep more CTAs busy.  Small FP64
+// systems take the 32-wide work units so that every SM has work.
 int default_variant(int precision, int64_t n) {
-    return (precision == GTD_PREC_MIXED && n >= 32768) ? 8 : 0;
+    if (precision == GTD_PREC_MIXED) return n >= 32768 ? 8 : 0;
+    return n <= 4096 ? 4 : 0;  // FP64: 32-wide units up to N = 4096 (at least 512 units on 148 SMs)
 }
 
 namespace {
@@ -416,6 +422,8 @@ static void with_f64(int v, F &&f) {
     switch (v) {
         case 1: f(force_f64_kernel<1>); break;
         case 2: f(force_f64_kernel<4>); break;
+        case 3: f(force_f64_kernel<1, 64>); break;
+        case 4: f(force_f64_kernel<1, 32>); break;
         default: f(force_f64_kernel<2>); break;
     }
 }
@@ -426,7 +434,7 @@ ForcePlan make_plan(int64_t n, int precision, int device, int variant) {
     p.variant = (variant >= 0 && variant < variant_count(precision)) ? variant : 0;
     const VariantInfo &vi = precision == GTD_PREC_MIXED ? kMixedVariants[p.variant] : kF64Variants[p.variant];
     p.bi = kThreads * vi.i;
-    p.bj = kThreads;
+    p.bj = vi.bj;
     p.rows = (n + p.bi - 1) / p.bi;
     p.tiles = (n + p.bj - 1) / p.bj;
     p.total = p.rows * p.tiles;

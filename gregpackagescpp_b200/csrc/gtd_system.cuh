@@ -8,6 +8,19 @@
 
 #include "gtd_internal.cuh"
 
+// What a captured step graph depends on.
+struct GraphKey {
+    int method = 0, cur = 0;
+    int64_t n = 0;
+    int variant = 0;
+    double G = 0, dt = 0;
+    const void *p0 = nullptr, *p1 = nullptr, *part = nullptr, *pred = nullptr;
+    bool operator==(const GraphKey &o) const {
+        return method == o.method && cur == o.cur && n == o.n && variant == o.variant && G == o.G && dt == o.dt &&
+               p0 == o.p0 && p1 == o.p1 && part == o.part && pred == o.pred;
+    }
+};
+
 struct gtd_system {
     int device = 0;
     int precision = GTD_PREC_F64;
@@ -107,6 +120,11 @@ struct gtd_system {
     void *nsys_dev = nullptr, *nsys_host = nullptr;
     size_t nsys_dev_bytes = 0, nsys_host_bytes = 0;
 
+    // captured steady-state steps (system.cu)
+    cudaGraphExec_t graph = nullptr;
+    GraphKey graph_key;
+    uint64_t graph_launches = 0;
+
     // host-array staging on the device (io.cu)
     void *io_dev = nullptr;
     size_t io_bytes = 0;
@@ -149,6 +167,7 @@ void release_collide(gtd_system *s);
 void release_nsys(gtd_system *s);
 void release_record(gtd_system *s);
 void release_io(gtd_system *s);
+void release_graph(gtd_system *s);
 // caller's arrays (upload order) <-> device bodies, converted on the device (io.cu)
 int device_upload(gtd_system *s, int64_t n, const double *m, const double *r, const double *rest, const double *x3,
                   const double *v3);

@@ -326,10 +326,77 @@ static int evolve_begin(gtd_system *s, int method) {
     return GTD_OK;
 }
 
+// Steady-state steps with no host logic between them (FP64, no collisions, recording or force
+// timing) are replayed from a CUDA graph of kGraphSteps steps: at small N the launches, not the
+// arithmetic, set the step time.  kGraphSteps is even, so the position double buffer ends where it
+// started and one graph per (method, buffer parity, parameters) serves every replay.
+constexpr int kGraphSteps = 16;
+
+static bool graph_eligible(const gtd_system *s) {
+    if (s->precision != GTD_PREC_F64 || s->coll != GTD_NO_COLL || s->rec_every || s->time_force) return false;
+    if ((s->method == GTD_LEAPFROG_KDK || s->method == GTD_LEAPFROG_DKD) && s->synced) return false;
+    return true;
+}
+
+void release_graph(gtd_system *s) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+}
+
+static int run_graph_chunk(gtd_system *s) {
+    int rc = ensure_plan(s);  // no allocation inside the capture
+    if (rc) return rc;
+    if (s->method == GTD_MODIFIED_EULER || s->method == GTD_MIDPOINT) {
+        rc = ensure_pred(s);
+        if (rc) return rc;
+    }
+    const GraphKey key{s->method, s->cur, s->n, s->variant, s->G, s->dt, s->pm[0], s->pm[1], s->partials,
+                       s->pred_pos};
+    if (!s->graph || !(key == s->graph_key)) {
+        release_graph(s);
+        const int cur0 = s->cur;
+        const bool synced0 = s->synced;
+        const uint64_t launches0 = s->launches;
+        GTD_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        for (int c = 0; c < kGraphSteps && !rc; ++c) rc = direct_step(s, s->method, false);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
+        s->graph_launches = s->launches - launches0;
+        s->launches = launches0;  // captured, not yet run
+        s->cur = cur0;
+        s->synced = synced0;
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+        const cudaError_t ie = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            s->graph = nullptr;
+            return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+        }
+        s->graph_key = key;
+    }
+    GTD_CUDA(cudaGraphLaunch(s->graph, s->stream));
+    s->launches += s->graph_launches;
+    // the state after kGraphSteps steps: same buffer parity, still unsynchronised
+    return GTD_OK;
+}
+
 static int evolve_steps(gtd_system *s, uint64_t k) {
     if (!s->begun) return fail(GTD_ERR_INVALID_ARGUMENT, "gtd_system_evolve_steps before gtd_system_evolve_begin");
     if (s->n == 0 || k == 0) return GTD_OK;
     for (uint64_t i = 0; i < k; ++i) {
+        // whole graph chunks while more than one chunk's worth of steps remains (the final step
+        // runs on its own, with `last` set)
+        while (k - i > (uint64_t)kGraphSteps && graph_eligible(s)) {
+            int rc = run_graph_chunk(s);
+            if (rc) return rc;
+            i += kGraphSteps;
+            s->rec_step += kGraphSteps;
+            s->steps_since_reorder += kGraphSteps;
+        }
         const bool rec = s->rec_every && (s->rec_step + 1) % s->rec_every == 0;
         const bool last = (i + 1 == k) || s->coll != GTD_NO_COLL || rec;
         int rc = maybe_reorder(s, false);
@@ -409,6 +476,7 @@ int gtd_system_destroy(gtd_system *s) {
     release_nsys(s);
     release_record(s);
     release_io(s);
+    release_graph(s);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     cudaEventDestroy(s->ev0);
     cudaEventDestroy(s->ev1);
@@ -458,6 +526,8 @@ int gtd_system_upload(gtd_system *s, int64_t n, const double *m, const double *r
     s->tree_valid = false;
     s->ordered = false;
     s->steps_since_reorder = 0;
+    s->rec_frames.clear();  // recordings belong to the bodies they were made from
+    s->rec_states.clear();
     if (n == 0) return GTD_OK;
     rc = device_upload(s, n, m, r, rest, x3, v3);
     if (rc) {  // a negative mass or radius: leave the handle empty

@@ -136,3 +136,29 @@ def test_autotune_result_reaches_other_handles(gpu):
     _lib.check(L.gtd_system_set_direct_variant(pinned._h, other))
     _lib.check(L.gtd_system_set_direct_variant(pinned._h, -1))  # unpinned: back to the tuned variant
     assert np.array_equal(fresh.accelerations(), pinned.accelerations())
+
+
+def test_full_size_mixed_accuracy_and_fp64_momentum(gpu):
+    """The headline size, N = 262144: the mixed force within the 1e-6 RMS bar of the FP64 one, and
+    the FP64 forces' momentum balance sum m_i a_i ~ 0 (pairwise antisymmetry) to 1e-12 of sum m|a|."""
+    m, x, v = plummer(262144, 1)
+    a64 = System(m, x, v, units_format=UNITS_G6674).accelerations()
+    amx = System(m, x, v, units_format=UNITS_G6674, precision="mixed").accelerations()
+    rel = np.linalg.norm(amx - a64, axis=1) / np.linalg.norm(a64, axis=1)
+    assert np.sqrt((rel ** 2).mean()) < 1e-6
+    p = (m[:, None] * a64).sum(0)
+    assert np.abs(p).max() / (m * np.linalg.norm(a64, axis=1)).sum() < 1e-12
+
+
+@pytest.mark.parametrize("name", list(METHODS))
+def test_graph_replayed_steps_are_bit_identical(gpu, name):
+    """FP64 steady-state steps run from a captured CUDA graph; with force-kernel timing on, the same
+    steps are launched one by one.  Both give bit-identical states (and match the oracle)."""
+    from gregpackagescpp_b200 import _lib
+    m, x, v = plummer(1024, 61)
+    a = System(m, x, v, timestep=3600.0, num_iterations=50, units_format=UNITS_G6674)
+    b = System(m, x, v, timestep=3600.0, num_iterations=50, units_format=UNITS_G6674)
+    _lib.check(b._L.gtd_system_time_force_kernels(b._h, 1))
+    a.evolve(METHODS[name])
+    b.evolve(METHODS[name])
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.v, b.v)
