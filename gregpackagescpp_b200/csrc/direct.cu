@@ -480,20 +480,8 @@ __device__ __forceinline__ int64_t cta_of(int64_t pos, int grid, int64_t total) 
     return ((pos + 1) * (int64_t)grid - 1) / total;
 }
 
-__global__ void integrate_kernel(IntArgs a) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    const int64_t r = i / a.bi;
-    const int l = (int)(i - r * a.bi);
-    const int64_t g0 = cta_of(r * a.tiles, a.grid, a.total);
-    const int64_t g1 = cta_of((r + 1) * a.tiles - 1, a.grid, a.total);
-    double ax = 0.0, ay = 0.0, az = 0.0;
-    for (int64_t g = g0; g <= g1; ++g) {
-        const double *slot = a.part + (size_t)(g + r) * 3 * a.bi;
-        ax += slot[l];
-        ay += slot[a.bi + l];
-        az += slot[2 * a.bi + l];
-    }
+// The method's update of body i from its summed force (ax, ay, az), in FP64.
+__device__ __forceinline__ void apply_epilogue(const IntArgs &a, int64_t i, double ax, double ay, double az) {
     const StepArgs &st = a.st;
     const double h = st.h, h2 = 0.5 * st.h;
     if (a.epi == EPI_ACC) {  // the force alone: position and velocity are not read
@@ -556,11 +544,58 @@ __global__ void integrate_kernel(IntArgs a) {
     }
 }
 
+// Thread per body: the partial sums of body i in CTA order, one after another.
+__global__ void integrate_kernel(IntArgs a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int64_t r = i / a.bi;
+    const int l = (int)(i - r * a.bi);
+    const int64_t g0 = cta_of(r * a.tiles, a.grid, a.total);
+    const int64_t g1 = cta_of((r + 1) * a.tiles - 1, a.grid, a.total);
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int64_t g = g0; g <= g1; ++g) {
+        const double *slot = a.part + (size_t)(g + r) * 3 * a.bi;
+        ax += slot[l];
+        ay += slot[a.bi + l];
+        az += slot[2 * a.bi + l];
+    }
+    apply_epilogue(a, i, ax, ay, az);
+}
+
+// Warp per body, for rows spread over many CTAs (small N with narrow work units): the lanes load
+// the partial sums in parallel and reduce them with shuffles, lane 0 applies the update.
+__global__ void integrate_warp_kernel(IntArgs a) {
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= a.n) return;  // whole warps leave together
+    const int64_t r = i / a.bi;
+    const int l = (int)(i - r * a.bi);
+    const int64_t g0 = cta_of(r * a.tiles, a.grid, a.total);
+    const int64_t g1 = cta_of((r + 1) * a.tiles - 1, a.grid, a.total);
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int64_t g = g0 + lane; g <= g1; g += 32) {
+        const double *slot = a.part + (size_t)(g + r) * 3 * a.bi;
+        ax += slot[l];
+        ay += slot[a.bi + l];
+        az += slot[2 * a.bi + l];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    if (lane == 0) apply_epilogue(a, i, ax, ay, az);
+}
+
 int launch_integrate(const ForcePlan &p, const double *partials, int epi, const StepArgs &st, cudaStream_t s) {
     if (p.n == 0) return GTD_OK;
     IntArgs a{p.n, p.tiles, p.total, p.grid, p.bi, epi, partials, st};
     const int threads = 256;
-    integrate_kernel<<<(unsigned)((p.n + threads - 1) / threads), threads, 0, s>>>(a);
+    if ((int64_t)p.grid > 4 * p.rows)  // a row's force is spread over more than ~4 CTAs
+        integrate_warp_kernel<<<(unsigned)((p.n * 32 + threads - 1) / threads), threads, 0, s>>>(a);
+    else
+        integrate_kernel<<<(unsigned)((p.n + threads - 1) / threads), threads, 0, s>>>(a);
     GTD_CHECK_LAUNCH();
     return GTD_OK;
 }
