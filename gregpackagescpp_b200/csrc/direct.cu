@@ -588,6 +588,59 @@ __global__ void integrate_warp_kernel(IntArgs a) {
     if (lane == 0) apply_epilogue(a, i, ax, ay, az);
 }
 
+// Small FP64 systems, one launch per force evaluation: a warp per body sums its whole row (lanes
+// strided over j, the bodies staged in shared-memory tiles), reduces with shuffles, and lane 0
+// applies the method's update.  No partial sums, no second kernel.
+constexpr int kFusedWarps = 4;
+constexpr int kFusedTile = 512;
+
+__global__ void __launch_bounds__(kFusedWarps * 32) fused_small_kernel(IntArgs a, const double4 *src, double G) {
+    __shared__ double4 tile[kFusedTile];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t i = (int64_t)blockIdx.x * kFusedWarps + w;
+    const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+    const double4 p = i < a.n ? src[i] : zero;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int64_t j0 = 0; j0 < a.n; j0 += kFusedTile) {
+        for (int k = threadIdx.x; k < kFusedTile; k += blockDim.x) {
+            const int64_t j = j0 + k;
+            double4 q = j < a.n ? src[j] : zero;
+            q.w *= G;
+            tile[k] = q;
+        }
+        __syncthreads();
+        const int lim = (int)min((int64_t)kFusedTile, a.n - j0);
+#pragma unroll 4
+        for (int jj = lane; jj < lim; jj += 32) {
+            const double4 q = tile[jj];
+            const double dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+            const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+            double inv = rsqrt(r2);
+            inv = r2 > 0.0 ? inv : 0.0;
+            const double sc = (q.w * inv) * (inv * inv);
+            ax = fma(sc, dx, ax);
+            ay = fma(sc, dy, ay);
+            az = fma(sc, dz, az);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    if (lane == 0 && i < a.n) apply_epilogue(a, i, ax, ay, az);
+}
+
+int launch_fused_small(int64_t n, const double4 *src, double G, int epi, const StepArgs &st, cudaStream_t s) {
+    if (n == 0) return GTD_OK;
+    IntArgs a{n, 0, 0, 0, 0, epi, nullptr, st};
+    fused_small_kernel<<<(unsigned)((n + kFusedWarps - 1) / kFusedWarps), kFusedWarps * 32, 0, s>>>(a, src, G);
+    GTD_CHECK_LAUNCH();
+    return GTD_OK;
+}
+
 int launch_integrate(const ForcePlan &p, const double *partials, int epi, const StepArgs &st, cudaStream_t s) {
     if (p.n == 0) return GTD_OK;
     IntArgs a{p.n, p.tiles, p.total, p.grid, p.bi, epi, partials, st};

@@ -72,6 +72,9 @@ int variant_info(int precision, int variant, int *i_per_thread, int *fold);
 // Process-wide autotune results: a handle without a pinned variant takes the variant last tuned on
 // its device for its precision and size class (the bit length of N), else default_variant.
 int default_variant(int precision, int64_t n);
+// Up to this many bodies an FP64 force evaluation and its update run as one fused launch.
+constexpr int64_t kFusedMaxN = 4096;
+int launch_fused_small(int64_t n, const double4 *src, double G, int epi, const StepArgs &st, cudaStream_t s);
 void remember_variant(int device, int precision, int64_t n, int variant);
 int tuned_variant(int device, int precision, int64_t n);
 size_t partial_bytes(const ForcePlan &p);

@@ -161,7 +161,16 @@ static int timed_event(gtd_system *s) {
 }
 
 int force_and_integrate(gtd_system *s, const double4 *src, int epi, const StepArgs &st) {
-    int rc = ensure_plan(s);
+    int rc;
+    if (s->precision == GTD_PREC_F64 && s->n <= kFusedMaxN) {
+        if (s->time_force && (rc = timed_event(s))) return rc;
+        rc = launch_fused_small(s->n, src, s->G, epi, st, s->stream);
+        if (rc) return rc;
+        if (s->time_force && (rc = timed_event(s))) return rc;
+        s->launches += 1;
+        return GTD_OK;
+    }
+    rc = ensure_plan(s);
     if (rc) return rc;
     if (s->time_force && (rc = timed_event(s))) return rc;
     rc = launch_force(s->precision, s->plan, src, s->G, s->partials, s->stream);

@@ -92,12 +92,13 @@ def test_mixed_kdk_tracks_fp64(gpu):
 @pytest.mark.parametrize("prec", ["f64", "mixed"])
 def test_every_force_variant(gpu, prec):
     """Each force-kernel variant, pinned on the handle, against the FP64 default (FP64 variants to
-    1e-13 relative, mixed ones to the mixed bar of 1e-6 RMS), on a ragged N."""
+    1e-13 relative, mixed ones to the mixed bar of 1e-6 RMS), on a ragged N (above the size up to
+    which FP64 evaluations take the fused single-launch kernel instead of the variants)."""
     import ctypes as C
 
     from gregpackagescpp_b200 import _lib
     L = _lib.load()
-    m, x, v = plummer(3001, 23)
+    m, x, v = plummer(5001, 23)
     want = System(m, x, v, units_format=UNITS_G6674).accelerations()
     p = _lib.PREC_MIXED if prec == "mixed" else _lib.PREC_F64
     count = C.c_int()
@@ -162,3 +163,16 @@ def test_graph_replayed_steps_are_bit_identical(gpu, name):
     a.evolve(METHODS[name])
     b.evolve(METHODS[name])
     assert np.array_equal(a.x, b.x) and np.array_equal(a.v, b.v)
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 1024, 4096, 4097])
+def test_fused_small_path_vs_oracle(gpu, oracle, n):
+    """FP64 systems up to 4096 bodies evaluate each force with its update in one launch (a warp per
+    body); at 4097 the stream-K kernels take over.  Both against the oracle at the FP64 bar."""
+    m, x, v = plummer(n, 300 + n)
+    s = System(m, x, v, timestep=3600.0, num_iterations=10, units_format=UNITS_G6674)
+    s.evolve(METHODS["leapfrog_kdk"])
+    xo, vo, _ = oracle.evolve(METHODS["leapfrog_kdk"], m, x, v, 3600.0, 10, oracle.G(UNITS_G6674))
+    assert rel_err(s.x, xo) < RTOL
+    if n > 1:  # a lone body has no velocity to compare against
+        assert rel_err(s.v, vo) < RTOL
