@@ -17,6 +17,7 @@
 #include <functional>
 #include <initializer_list>
 #include <ios>
+#include <iostream>  // the reference's headers provide it to the drivers
 #include <type_traits>
 #include <regex>
 #include <string>

@@ -33,3 +33,21 @@ def test_dropin_program_runs_on_gpu(gpu, tmp_path):
     run = subprocess.run([exe], capture_output=True, text=True, timeout=600)
     print(run.stdout)
     assert run.returncode == 0, run.stdout + run.stderr
+
+
+REF_DRIVER = "/root/reference/nrg.cpp"
+
+
+@pytest.mark.skipif(not os.path.exists(REF_DRIVER), reason="the reference tree is not mounted here")
+def test_reference_driver_compiles_unchanged(tmp_path):
+    """nrg.cpp, one of the reference's own drivers (it loads .nsys files into
+    gtd::system<T,T,T,true,false,3,0,0,false> for three T and sums their energies through body and
+    vector3D accessors), compiles unchanged against include/gtd and links the engine.  The source is
+    copied to a scratch directory first, so that its own directory's headers do not shadow these."""
+    import shutil
+    src = tmp_path / "nrg.cpp"
+    shutil.copy(REF_DRIVER, src)
+    cmd = ["g++", "-std=c++20", "-O1", "-I", os.path.join(ROOT, "include", "gtd"), "-I", os.path.join(ROOT, "include"),
+           str(src), "-o", str(tmp_path / "nrg"), "-L", PKG, "-l:libgtd_b200.so", f"-Wl,-rpath,{PKG}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-4000:]
