@@ -150,6 +150,8 @@ def load():
     L.gtd_system_set_recording.argtypes = [vp, u64]
     L.gtd_system_recording.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), dp, dp]
     L.gtd_system_to_nsys.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, dp, ip, ip, ip, C.POINTER(i64)]
+    L.gtd_system_to_nsys_async.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, dp, ip, ip, ip]
+    L.gtd_system_nsys_wait.argtypes = [vp, C.POINTER(i64)]
     L.gtd_system_load_nsys.argtypes = [vp, C.c_char_p, ip, ip, ip, ip, C.POINTER(C.c_double),
                                        C.POINTER(C.c_double), dp, C.POINTER(C.c_double)]
     for name in exported_symbols():

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <future>
+#include <string>
 #include <vector>
 
 #include "gtd_internal.cuh"
@@ -119,6 +121,15 @@ struct gtd_system {
     // .nsys chunk staging (nsys.cu)
     void *nsys_dev = nullptr, *nsys_host = nullptr;
     size_t nsys_dev_bytes = 0, nsys_host_bytes = 0;
+    // snapshot writes in flight: pinned buffer, copy-done event and host writer per slot
+    struct NsysWrite {
+        void *buf = nullptr;
+        size_t bytes = 0;
+        cudaEvent_t done = nullptr;
+        std::future<std::pair<int, std::string>> job;  // status, message (bytes written on success)
+        int64_t written = 0;
+    } nsys_w[2];
+    int nsys_next = 0, nsys_last = -1;
 
     // captured steady-state steps (system.cu)
     cudaGraphExec_t graph = nullptr;

@@ -20,6 +20,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <future>
+#include <string>
+#include <utility>
 #include <vector>
 
 #include "gtd_internal.cuh"
@@ -252,21 +255,73 @@ static uint64_t nsys_file_size(uint64_t n, int chunk_bytes) {  // gregsys.hpp:94
     return kNsysHeader + body + (rem ? 4 - rem : 0);
 }
 
-// Packs the chunks of the live bodies (in output order) into s->nsys_host.
-static int pack_to_host(gtd_system *s, const NsysLayout &L) {
+// Enqueues the packing of the live bodies (in output order) and its copy into pinned buffer w,
+// then the event that marks the copy done.  Nothing waits here.
+static int pack_async(gtd_system *s, const NsysLayout &L, gtd_system::NsysWrite &w) {
     const int64_t n = s->n;
     int rc = restore_upload_order(s);  // output row order
     if (rc) return rc;
     const size_t bytes = (size_t)n * L.bytes;
-    rc = ensure_nsys_buffers(s, bytes);
-    if (rc) return rc;
+    if (bytes > s->nsys_dev_bytes) {
+        cudaFree(s->nsys_dev);
+        s->nsys_dev = nullptr;
+        s->nsys_dev_bytes = 0;
+        GTD_CUDA(cudaMalloc(&s->nsys_dev, bytes));
+        s->nsys_dev_bytes = bytes;
+    }
+    if (bytes > w.bytes) {
+        cudaFreeHost(w.buf);
+        w.buf = nullptr;
+        w.bytes = 0;
+        GTD_CUDA(cudaMallocHost(&w.buf, bytes));
+        w.bytes = bytes;
+    }
+    if (!w.done) GTD_CUDA(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming));
     const unsigned blocks = (unsigned)((n + kPackThreads - 1) / kPackThreads);
     nsys_pack_kernel<<<blocks, kPackThreads, (size_t)kPackThreads * L.bytes, s->stream>>>(
         n, L, s->pm[s->cur], s->vel, s->rad, s->rest, static_cast<unsigned char *>(s->nsys_dev));
     GTD_CHECK_LAUNCH();
     s->launches += 1;
-    GTD_CUDA(cudaMemcpyAsync(s->nsys_host, s->nsys_dev, bytes, cudaMemcpyDeviceToHost, s->stream));
-    GTD_CUDA(cudaStreamSynchronize(s->stream));
+    GTD_CUDA(cudaMemcpyAsync(w.buf, s->nsys_dev, bytes, cudaMemcpyDeviceToHost, s->stream));
+    GTD_CUDA(cudaEventRecord(w.done, s->stream));
+    return GTD_OK;
+}
+
+// The host side of one write: the header, the chunks once their copy is done, the padding.
+static std::pair<int, std::string> write_file(int device, cudaEvent_t done, std::string path,
+                                              std::vector<unsigned char> header, const void *body, size_t body_bytes,
+                                              int64_t *written) {
+    *written = 0;
+    if (body_bytes) {
+        cudaSetDevice(device);
+        const cudaError_t e = cudaEventSynchronize(done);
+        if (e != cudaSuccess) return {GTD_ERR_CUDA, std::string("snapshot copy: ") + cudaGetErrorString(e)};
+    }
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) return {GTD_OK, ""};  // the reference returns 0 when the stream does not open
+    bool ok = std::fwrite(header.data(), 1, header.size(), f) == header.size();
+    int64_t tell = (int64_t)header.size();
+    if (ok && body_bytes) {
+        ok = std::fwrite(body, 1, body_bytes, f) == body_bytes;
+        tell += (int64_t)body_bytes;
+        if (const int rem = (int)(tell % 4); ok && rem) {
+            static const unsigned char zeros[4] = {0, 0, 0, 0};
+            ok = std::fwrite(zeros, 1, (size_t)(4 - rem), f) == (size_t)(4 - rem);
+            tell += 4 - rem;
+        }
+    }
+    if (std::fclose(f) != 0) ok = false;
+    if (!ok) return {GTD_ERR_INVALID_ARGUMENT, "error writing " + path};
+    *written = tell;
+    return {GTD_OK, ""};
+}
+
+// Waits for the write in slot k (if any); its status, with the message set for the caller's thread.
+static int finish_write(gtd_system *s, int k) {
+    gtd_system::NsysWrite &w = s->nsys_w[k];
+    if (!w.job.valid()) return GTD_OK;
+    const std::pair<int, std::string> r = w.job.get();
+    if (r.first) return fail(r.first, "%s", r.second.c_str());
     return GTD_OK;
 }
 
@@ -275,6 +330,14 @@ static int pack_to_host(gtd_system *s, const NsysLayout &L) {
 using namespace gtd;
 
 void release_nsys(gtd_system *s) {
+    for (auto &w : s->nsys_w) {
+        if (w.job.valid()) w.job.wait();
+        cudaFreeHost(w.buf);
+        if (w.done) cudaEventDestroy(w.done);
+        w.buf = nullptr;
+        w.bytes = 0;
+        w.done = nullptr;
+    }
     cudaFree(s->nsys_dev);
     cudaFreeHost(s->nsys_host);
     s->nsys_dev = nullptr;
@@ -292,53 +355,64 @@ int gtd_nsys_chunk_size(int m_size, int r_size, int t_size, int *chunk_bytes) {
     return GTD_OK;
 }
 
-int gtd_system_to_nsys(gtd_system *s, const char *path, double time_elapsed, double dt, const uint64_t *g_vals,
-                       int m_size, int r_size, int t_size, int64_t *bytes_written) {
+int gtd_system_to_nsys_async(gtd_system *s, const char *path, double time_elapsed, double dt, const uint64_t *g_vals,
+                             int m_size, int r_size, int t_size) {
     if (!s || !g_vals) return fail(GTD_ERR_INVALID_ARGUMENT, "NULL argument");
     if (!valid_size(m_size) || !valid_size(r_size) || !valid_size(t_size))
         return fail(GTD_ERR_UNSUPPORTED, "M, R and T must be float, double or long double (sizes 4, 8, 16)");
-    if (bytes_written) *bytes_written = 0;
     if (!path) return GTD_OK;  // gregsys.hpp:3220-3221
     DeviceGuard g(s->device);
+    const int k = s->nsys_next;
+    int rc = finish_write(s, k);  // the slot's previous write must release its buffer first
+    if (rc) return rc;
+    gtd_system::NsysWrite &w = s->nsys_w[k];
     const NsysLayout L = nsys_layout(m_size, r_size, t_size);
     const int64_t n = s->n;
     if (n > 0) {
-        int rc = pack_to_host(s, L);
+        rc = pack_async(s, L, w);
         if (rc) return rc;
     }
-    FILE *f = std::fopen(path, "wb");
-    if (!f) return GTD_OK;  // the reference returns 0 when the stream does not open
-    unsigned char h[kNsysHeader];
-    std::memset(h, 0, sizeof h);
+    std::vector<unsigned char> h(kNsysHeader, 0);
     h[0] = 'N';
     h[1] = 'S';
     h[2] = (unsigned char)(1 + (1 << 1) + (1 << 2) + (1 << 3));  // floating time, M, R and T
     h[3] = 16;                                                  // sizeof(long double)
-    f64_to_x87(time_elapsed, h + 4);
-    f64_to_x87(dt, h + 20);
+    f64_to_x87(time_elapsed, h.data() + 4);
+    f64_to_x87(dt, h.data() + 20);
     h[36] = (unsigned char)m_size;
     h[37] = (unsigned char)r_size;
     h[38] = (unsigned char)t_size;
     h[39] = 16;
-    std::memcpy(h + 40, g_vals, 6 * sizeof(uint64_t));
+    std::memcpy(h.data() + 40, g_vals, 6 * sizeof(uint64_t));
     const uint64_t nb = (uint64_t)n;
-    std::memcpy(h + 88, &nb, 8);
-    bool ok = std::fwrite(h, 1, sizeof h, f) == sizeof h;
-    int64_t tell = kNsysHeader;
-    if (ok && n > 0) {
-        const size_t body = (size_t)n * L.bytes;
-        ok = std::fwrite(s->nsys_host, 1, body, f) == body;
-        tell += (int64_t)body;
-        if (const int rem = (int)(tell % 4); ok && rem) {
-            static const unsigned char zeros[4] = {0, 0, 0, 0};
-            ok = std::fwrite(zeros, 1, (size_t)(4 - rem), f) == (size_t)(4 - rem);
-            tell += 4 - rem;
-        }
-    }
-    if (std::fclose(f) != 0) ok = false;
-    if (!ok) return fail(GTD_ERR_INVALID_ARGUMENT, "error writing %s", path);
-    if (bytes_written) *bytes_written = tell;
+    std::memcpy(h.data() + 88, &nb, 8);
+    const size_t body = (size_t)n * L.bytes;
+    w.job = std::async(std::launch::async, write_file, s->device, w.done, std::string(path), std::move(h), w.buf, body,
+                       &w.written);
+    s->nsys_last = k;
+    s->nsys_next = k ^ 1;
     return GTD_OK;
+}
+
+int gtd_system_nsys_wait(gtd_system *s, int64_t *bytes_written) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (bytes_written) *bytes_written = 0;
+    const int last = s->nsys_last;
+    const int first = last < 0 ? 0 : last ^ 1;  // the older write first
+    int rc = finish_write(s, first);
+    const int rc2 = finish_write(s, first ^ 1);
+    if (!rc) rc = rc2;
+    if (rc) return rc;
+    if (bytes_written && last >= 0) *bytes_written = s->nsys_w[last].written;
+    return GTD_OK;
+}
+
+int gtd_system_to_nsys(gtd_system *s, const char *path, double time_elapsed, double dt, const uint64_t *g_vals,
+                       int m_size, int r_size, int t_size, int64_t *bytes_written) {
+    if (bytes_written) *bytes_written = 0;
+    const int rc = gtd_system_to_nsys_async(s, path, time_elapsed, dt, g_vals, m_size, r_size, t_size);
+    if (rc || !path) return rc;  // a NULL path writes nothing, as in the reference
+    return gtd_system_nsys_wait(s, bytes_written);
 }
 
 int gtd_system_load_nsys(gtd_system *s, const char *path, int check_nan_inf, int m_size, int r_size, int t_size,

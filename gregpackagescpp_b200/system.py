@@ -169,18 +169,29 @@ class System:
     # ---- .nsys snapshots (gregsys.hpp:943-1400, 3214-3258) ------------------------------------
     _SIZES = {"float": 4, "double": 8, "long double": 16}
 
-    def to_nsys(self, path: str | None, M: str = "double", R: str = "double", T: str = "double") -> int:
+    def to_nsys(self, path: str | None, M: str = "double", R: str = "double", T: str = "double",
+                wait: bool = True) -> int | None:
         """system::to_nsys: writes the bodies as a .nsys file with the chunk layout of the given
         M, R, T types ("float", "double" or "long double"); returns the bytes written (0 when path
-        is None or the file cannot be opened)."""
+        is None or the file cannot be opened).  wait=False returns once the snapshot is taken on
+        the device; a host thread writes the file (nsys_wait() collects the result)."""
         if path is None:
             return 0
         self._push()
-        nb = C.c_int64()
         gv = np.array(self.g_vals, dtype=np.uint64)
-        check(self._L.gtd_system_to_nsys(self._h, str(path).encode(), self.time_elapsed, self.dt,
-                                         gv.ctypes.data, self._SIZES[M], self._SIZES[R], self._SIZES[T],
-                                         C.byref(nb)))
+        args = (self._h, str(path).encode(), self.time_elapsed, self.dt, gv.ctypes.data, self._SIZES[M],
+                self._SIZES[R], self._SIZES[T])
+        if not wait:
+            check(self._L.gtd_system_to_nsys_async(*args))
+            return None
+        nb = C.c_int64()
+        check(self._L.gtd_system_to_nsys(*args, C.byref(nb)))
+        return nb.value
+
+    def nsys_wait(self) -> int:
+        """Waits for the snapshot writes started with to_nsys(wait=False); the size of the last."""
+        nb = C.c_int64()
+        check(self._L.gtd_system_nsys_wait(self._h, C.byref(nb)))
         return nb.value
 
     @classmethod

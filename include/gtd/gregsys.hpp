@@ -272,6 +272,22 @@ public:
                                         (int)sizeof(R), (int)sizeof(T), &bytes));
         return (std::streamoff)bytes;
     }
+    // Extension: the snapshot is taken on the device now and written to the file by a host thread,
+    // so the next evolve() overlaps the write; nsys_wait() returns the last file's size.
+    void to_nsys_async(const char *path) const {
+        static_assert(std::is_floating_point_v<M> && std::is_floating_point_v<R> && std::is_floating_point_v<T>,
+                      "the engine writes .nsys files with floating-point M, R and T");
+        if (path == nullptr) return;
+        auto *self = const_cast<system *>(this);
+        self->push();
+        throw_status(gtd_system_to_nsys_async(dev, path, (double)time_elapsed, (double)dt, G_vals, (int)sizeof(M),
+                                              (int)sizeof(R), (int)sizeof(T)));
+    }
+    std::streamoff nsys_wait() const {
+        int64_t bytes = 0;
+        if (dev) throw_status(gtd_system_nsys_wait(dev, &bytes));
+        return (std::streamoff)bytes;
+    }
 
     // ---- accessors and setters (gregsys.hpp:1627-1672) ------------------------------------------
     typename std::vector<bod_t>::size_type num_bodies() const noexcept { return bods.size(); }

@@ -135,6 +135,14 @@ GTD_API int gtd_nsys_chunk_size(int m_size, int r_size, int t_size, int *chunk_b
  * the file cannot be opened, as the reference returns 0. */
 GTD_API int gtd_system_to_nsys(gtd_system *sys, const char *path, double time_elapsed, double dt,
                                const uint64_t *g_vals, int m_size, int r_size, int t_size, int64_t *bytes_written);
+/* The same, returning once the packing and its device-to-host copy are enqueued on the handle's
+ * stream: a host thread writes the file when the copy is done, so the next evolve can run meanwhile
+ * (the snapshot is of the state at the call).  Two writes can be in flight per handle; a third
+ * call waits for the oldest.  gtd_system_nsys_wait waits for every pending write and returns the
+ * first failure, or GTD_OK and the size of the most recent file. */
+GTD_API int gtd_system_to_nsys_async(gtd_system *sys, const char *path, double time_elapsed, double dt,
+                                     const uint64_t *g_vals, int m_size, int r_size, int t_size);
+GTD_API int gtd_system_nsys_wait(gtd_system *sys, int64_t *bytes_written);
 /* Replaces the system(const char *nsys_path, ...) constructor's load_from_nsys (gregsys.hpp:947-1400):
  * the same checks in the same order with the same messages (GTD_ERR_NSYS_LOAD / GTD_ERR_NSYS_FORMAT
  * for nsys_load_error / nsys_format_error; GTD_ERR_INVALID_ARGUMENT for a non-positive time-step),

@@ -118,3 +118,25 @@ def test_missing_file_and_null_path(gpu, tmp_path):
     s = System(*plummer(10, 1))
     assert s.to_nsys(None) == 0
     assert s.to_nsys(str(tmp_path / "no_such_dir" / "f.nsys")) == 0
+
+
+def test_async_frames_overlap_evolve(gpu, tmp_path):
+    """A frame loop with asynchronous snapshots (evolve, to_nsys(wait=False), evolve, ...): every
+    file holds the state at its call, bit-identical to a synchronous write of that state."""
+    m, x, v = plummer(5000, 71)
+    s = System(m, x, v, timestep=3600.0, num_iterations=4, units_format=UNITS_G6674)
+    states = []
+    for k in range(5):
+        s.evolve(System.leapfrog_kdk)
+        s.to_nsys(str(tmp_path / f"frame{k}.nsys"), wait=False)
+        states.append((s.x.copy(), s.v.copy()))
+    assert s.nsys_wait() == 96 + 5000 * 80
+    for k, (xk, vk) in enumerate(states):
+        t = System.from_nsys(str(tmp_path / f"frame{k}.nsys"))
+        assert np.array_equal(t.x, xk) and np.array_equal(t.v, vk)
+        ref = System(t.m, xk, vk, units_format=UNITS_G6674)
+        p = str(tmp_path / "sync.nsys")
+        ref.to_nsys(p)
+        a = open(p, "rb").read()
+        b = open(str(tmp_path / f"frame{k}.nsys"), "rb").read()
+        assert a[96:] == b[96:]
