@@ -8,8 +8,9 @@
 from . import ics  # noqa: F401
 from ._lib import GtdError, NbodyError, OverlappingBodiesError, TwoBodyError, BarnesHutError  # noqa: F401
 from ._lib import InvalidBodyPlacement, IndistinguishableBodies, NsysLoadError, NsysFormatError  # noqa: F401
-from .system import System, Body, parse_units  # noqa: F401
+from ._lib import CallbackError  # noqa: F401
+from .system import System, Body, parse_units, RestFromCom, WhileRestBelow, DeviceHook  # noqa: F401
 
 __all__ = ["System", "Body", "parse_units", "ics", "GtdError", "NbodyError", "OverlappingBodiesError",
            "TwoBodyError", "BarnesHutError", "InvalidBodyPlacement", "IndistinguishableBodies", "NsysLoadError",
-           "NsysFormatError"]
+           "NsysFormatError", "CallbackError", "RestFromCom", "WhileRestBelow", "DeviceHook"]

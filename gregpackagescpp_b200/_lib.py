@@ -35,6 +35,10 @@ NO_COLL, OVERLAP_COLL, MERGE_COLL = 0, 3, 4
 
 ERR_NSYS_LOAD = 13
 ERR_NSYS_FORMAT = 14
+ERR_CALLBACK = 15
+
+# gtd_step_hook: int (*)(void *user)
+STEP_HOOK = C.CFUNCTYPE(C.c_int, C.c_void_p)
 
 
 class GtdError(RuntimeError):
@@ -77,6 +81,10 @@ class NsysFormatError(NsysLoadError):
     """gtd::nsys_format_error (gregsys.hpp:130-134)."""
 
 
+class CallbackError(GtdError):
+    """An evolve callback (host step hook or device hook) reported a failure."""
+
+
 _EXC = {
     ERR_INVALID_ARGUMENT: ValueError,
     ERR_OVERLAPPING_BODIES: OverlappingBodiesError,
@@ -85,6 +93,7 @@ _EXC = {
     ERR_INDISTINGUISHABLE: IndistinguishableBodies,
     ERR_NSYS_LOAD: NsysLoadError,
     ERR_NSYS_FORMAT: NsysFormatError,
+    ERR_CALLBACK: CallbackError,
 }
 
 _lib = None
@@ -154,6 +163,14 @@ def load():
     L.gtd_system_nsys_wait.argtypes = [vp, C.POINTER(i64)]
     L.gtd_system_load_nsys.argtypes = [vp, C.c_char_p, ip, ip, ip, ip, C.POINTER(C.c_double),
                                        C.POINTER(C.c_double), dp, C.POINTER(C.c_double)]
+    L.gtd_system_set_step_hook.argtypes = [vp, vp, vp]
+    L.gtd_system_update_bodies.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.gtd_system_set_device_callbacks.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    L.gtd_system_set_rest_from_com.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, dp, ip]
+    L.gtd_system_rest_from_com_centre.argtypes = [vp, dp]
+    L.gtd_system_set_continue_while_rest_below.argtypes = [vp, C.c_double, u64]
+    L.gtd_system_evolve_callbacks.argtypes = [vp, ip, u64, C.POINTER(u64), C.POINTER(i64)]
+    L.gtd_system_callback_stats.argtypes = [vp, C.POINTER(u64), C.POINTER(C.c_int)]
     for name in exported_symbols():
         if name != "gtd_last_error":
             getattr(L, name).restype = C.c_int

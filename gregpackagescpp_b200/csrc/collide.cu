@@ -416,13 +416,21 @@ static int merge_scan(gtd_system *s, bool only_check, int32_t *pair_out) {
     return GTD_OK;
 }
 
-int run_collisions(gtd_system *s) {
-    if (s->n < 2) return GTD_OK;
-    if (s->coll == GTD_MERGE_COLL) return merge_scan(s, false, nullptr);
+// Upload order and the candidate buffer for overlap passes; *status: the pass's device error word
+// (GTD_ERR_CAPACITY when the candidates overflowed), cleared by every pass.
+int prepare_collisions(gtd_system *s, int **status) {
     int rc = restore_upload_order(s);
     if (rc) return rc;
     rc = ensure_coll(s);
     if (rc) return rc;
+    if (status) *status = coll_ptrs(s).status;
+    return GTD_OK;
+}
+
+// One s_coll pass (overlap restitution) enqueued on the stream, without reading its status back;
+// prepare_collisions must have run since the last reorder.  Capturable.
+int enqueue_collisions(gtd_system *s) {
+    if (s->n < 2) return GTD_OK;
     CollPtrs p = coll_ptrs(s);
     cudaStream_t st = s->stream;
     GTD_CUDA(cudaMemsetAsync(p.count, 0, 64, st));
@@ -433,6 +441,18 @@ int run_collisions(gtd_system *s) {
                                          p.status);
     GTD_CHECK_LAUNCH();
     s->launches += 2;
+    return GTD_OK;
+}
+
+int run_collisions(gtd_system *s) {
+    if (s->n < 2) return GTD_OK;
+    if (s->coll == GTD_MERGE_COLL) return merge_scan(s, false, nullptr);
+    int rc = prepare_collisions(s, nullptr);
+    if (rc) return rc;
+    rc = enqueue_collisions(s);
+    if (rc) return rc;
+    CollPtrs p = coll_ptrs(s);
+    cudaStream_t st = s->stream;
     int host[2] = {0, 0};
     GTD_CUDA(cudaMemcpyAsync(host, p.count, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     GTD_CUDA(cudaStreamSynchronize(st));

@@ -140,6 +140,29 @@ struct gtd_system {
     void *io_dev = nullptr;
     size_t io_bytes = 0;
 
+    // evolve callbacks (callbacks.cu).  Host: a hook called inside every step of evolve_steps at
+    // for_all_bods' place.  Device: continue_ev_if / for_each_bod / for_all_bods as GPU work.
+    gtd_step_hook step_hook = nullptr;
+    void *step_hook_user = nullptr;
+    struct DeviceCallbacks {
+        int cont_kind = 0;  // 0 none (run `iterations` steps), 1 user hook, 2 rest below a bound
+        gtd_device_hook cont_fn = nullptr;
+        void *cont_user = nullptr;
+        double min_max_cor = 0.0;
+        uint64_t probing_iters = 0;
+        int all_kind = 0;   // 0 none, 1 user hook, 2 restitution from the distance to the carried COM
+        gtd_device_hook all_fn = nullptr;
+        void *all_user = nullptr;
+        double min_cor = 0.0, max_cor = 1.0, scale_factor = 1.0, n_exp = 1.0;
+        int mass_weighted = 0;
+        gtd_device_hook each_fn = nullptr;
+        void *each_user = nullptr;
+    } cb;
+    void *cb_ctl = nullptr;   // device control block of the device-driven loop
+    void *cb_host = nullptr;  // pinned mirror of it
+    uint64_t cb_waits = 0;    // host waits of the last callback-driven evolve
+    bool cb_graph = false;    // whether it ran as graph chunks
+
     // trajectory frames (record.cu): every rec_every-th state of a direct-summation evolve
     uint64_t rec_every = 0;
     uint64_t rec_step = 0;               // steps since evolve_begin
@@ -179,6 +202,20 @@ void release_nsys(gtd_system *s);
 void release_record(gtd_system *s);
 void release_io(gtd_system *s);
 void release_graph(gtd_system *s);
+void release_callbacks(gtd_system *s);
+// overwrite live bodies in download order, keeping accelerations and the evolve state (io.cu)
+int device_update(gtd_system *s, const double *m, const double *r, const double *rest, const double *x3,
+                  const double *v3);
+// overlap collision pass split for capture (collide.cu)
+int prepare_collisions(gtd_system *s, int **status);
+int enqueue_collisions(gtd_system *s);
+int run_collisions(gtd_system *s);
+// pieces of evolve for the callback-driven loop (system.cu)
+int cb_evolve_begin(gtd_system *s, int method);
+int cb_direct_step(gtd_system *s);
+int cb_maybe_reorder(gtd_system *s);
+int cb_select_branch(int method);
+int cb_prepare_steps(gtd_system *s);
 // caller's arrays (upload order) <-> device bodies, converted on the device (io.cu)
 int device_upload(gtd_system *s, int64_t n, const double *m, const double *r, const double *rest, const double *x3,
                   const double *v3);

@@ -87,6 +87,25 @@ __global__ void unpack_bodies_kernel(int64_t n, const double4 *pm, const double4
     if (want & 32) o.rest[w] = rest[i];
 }
 
+// Slot i takes row rows[i] (or ids[i], or i) of each given input; acceleration and order untouched.
+__global__ void update_bodies_kernel(int64_t n, double4 *pm, double4 *vel, double *rad, double *rest,
+                                     const int32_t *map, IoView in, unsigned have) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t w = map ? map[i] : i;
+    double4 p = pm[i];
+    if (have & 1) { p.x = in.x3[3 * w]; p.y = in.x3[3 * w + 1]; p.z = in.x3[3 * w + 2]; }
+    if (have & 8) p.w = in.m[w];
+    pm[i] = p;
+    if (have & 2) {
+        double4 v = vel[i];
+        v.x = in.v3[3 * w]; v.y = in.v3[3 * w + 1]; v.z = in.v3[3 * w + 2];
+        vel[i] = v;
+    }
+    if (have & 16) rad[i] = in.r[w];
+    if (have & 32) rest[i] = in.rest[w];
+}
+
 }  // namespace gtd
 
 using namespace gtd;
@@ -127,6 +146,24 @@ int device_upload(gtd_system *s, int64_t n, const double *m, const double *r, co
     return GTD_OK;
 }
 
+// Device slot -> host row map for the live bodies (NULL: identity), staged in io.rows when needed.
+static int row_map(gtd_system *s, const IoView &io, const int32_t **map) {
+    *map = nullptr;
+    if (s->n != s->n_uploaded) {  // after merges: ranks of the surviving upload indices (host sort)
+        std::vector<int64_t> row;
+        int rc = output_rows(s, row);
+        if (rc) return rc;
+        std::vector<int32_t> r32(row.begin(), row.end());
+        GTD_CUDA(cudaMemcpyAsync(io.rows, r32.data(), sizeof(int32_t) * (size_t)s->n, cudaMemcpyHostToDevice,
+                                 s->stream));
+        GTD_CUDA(cudaStreamSynchronize(s->stream));
+        *map = io.rows;
+    } else if (s->ordered) {
+        *map = s->ids;
+    }
+    return GTD_OK;
+}
+
 // Writes the requested arrays (any may be NULL) in download order: upload order among the live bodies.
 int device_download(gtd_system *s, double *m, double *r, double *rest, double *x3, double *v3, double *a3) {
     const int64_t n = s->n;
@@ -135,17 +172,8 @@ int device_download(gtd_system *s, double *m, double *r, double *rest, double *x
     IoView io = io_view(static_cast<double *>(s->io_dev), n);
     cudaStream_t st = s->stream;
     const int32_t *map = nullptr;
-    if (n != s->n_uploaded) {  // after merges: ranks of the surviving upload indices (host sort)
-        std::vector<int64_t> row;
-        rc = output_rows(s, row);
-        if (rc) return rc;
-        std::vector<int32_t> r32(row.begin(), row.end());
-        GTD_CUDA(cudaMemcpyAsync(io.rows, r32.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
-        GTD_CUDA(cudaStreamSynchronize(st));
-        map = io.rows;
-    } else if (s->ordered) {
-        map = s->ids;
-    }
+    rc = row_map(s, io, &map);
+    if (rc) return rc;
     const unsigned want = (x3 ? 1u : 0u) | (v3 ? 2u : 0u) | (a3 ? 4u : 0u) | (m ? 8u : 0u) | (r ? 16u : 0u) |
                           (rest ? 32u : 0u);
     if (!want) return GTD_OK;
@@ -161,5 +189,34 @@ int device_download(gtd_system *s, double *m, double *r, double *rest, double *x
     if (r) GTD_CUDA(cudaMemcpyAsync(r, io.r, d * (size_t)n, cudaMemcpyDeviceToHost, st));
     if (rest) GTD_CUDA(cudaMemcpyAsync(rest, io.rest, d * (size_t)n, cudaMemcpyDeviceToHost, st));
     GTD_CUDA(cudaStreamSynchronize(st));
+    return GTD_OK;
+}
+
+// Overwrites the given arrays (any may be NULL) of the live bodies, in download order, leaving the
+// accelerations, the body order and the evolve state as they are.
+int device_update(gtd_system *s, const double *m, const double *r, const double *rest, const double *x3,
+                  const double *v3) {
+    const int64_t n = s->n;
+    const unsigned have = (x3 ? 1u : 0u) | (v3 ? 2u : 0u) | (m ? 8u : 0u) | (r ? 16u : 0u) | (rest ? 32u : 0u);
+    if (n == 0 || !have) return GTD_OK;
+    int rc = ensure_io(s, n);
+    if (rc) return rc;
+    IoView io = io_view(static_cast<double *>(s->io_dev), n);
+    cudaStream_t st = s->stream;
+    const int32_t *map = nullptr;
+    rc = row_map(s, io, &map);
+    if (rc) return rc;
+    const size_t d = sizeof(double);
+    if (x3) GTD_CUDA(cudaMemcpyAsync(io.x3, x3, 3 * d * (size_t)n, cudaMemcpyHostToDevice, st));
+    if (v3) GTD_CUDA(cudaMemcpyAsync(io.v3, v3, 3 * d * (size_t)n, cudaMemcpyHostToDevice, st));
+    if (m) GTD_CUDA(cudaMemcpyAsync(io.m, m, d * (size_t)n, cudaMemcpyHostToDevice, st));
+    if (r) GTD_CUDA(cudaMemcpyAsync(io.r, r, d * (size_t)n, cudaMemcpyHostToDevice, st));
+    if (rest) GTD_CUDA(cudaMemcpyAsync(io.rest, rest, d * (size_t)n, cudaMemcpyHostToDevice, st));
+    update_bodies_kernel<<<(unsigned)((n + kIT - 1) / kIT), kIT, 0, st>>>(n, s->pm[s->cur], s->vel, s->rad, s->rest,
+                                                                        map, io, have);
+    GTD_CHECK_LAUNCH();
+    s->launches += 1;
+    GTD_CUDA(cudaStreamSynchronize(st));  // the caller's arrays may change as soon as this returns
+    if (x3 || m) s->tree_valid = false;
     return GTD_OK;
 }

@@ -342,7 +342,8 @@ static int evolve_begin(gtd_system *s, int method) {
 constexpr int kGraphSteps = 16;
 
 static bool graph_eligible(const gtd_system *s) {
-    if (s->precision != GTD_PREC_F64 || s->coll != GTD_NO_COLL || s->rec_every || s->time_force) return false;
+    if (s->precision != GTD_PREC_F64 || s->coll != GTD_NO_COLL || s->rec_every || s->time_force || s->step_hook)
+        return false;
     if ((s->method == GTD_LEAPFROG_KDK || s->method == GTD_LEAPFROG_DKD) && s->synced) return false;
     return true;
 }
@@ -407,13 +408,17 @@ static int evolve_steps(gtd_system *s, uint64_t k) {
             s->steps_since_reorder += kGraphSteps;
         }
         const bool rec = s->rec_every && (s->rec_step + 1) % s->rec_every == 0;
-        const bool last = (i + 1 == k) || s->coll != GTD_NO_COLL || rec;
+        const bool last = (i + 1 == k) || s->coll != GTD_NO_COLL || rec || s->step_hook;
         int rc = maybe_reorder(s, false);
         if (rc) return rc;
         rc = direct_step(s, s->method, last);
         if (rc) return rc;
         s->steps_since_reorder += 1;
         s->rec_step += 1;
+        if (s->step_hook) {  // for_all_bods' place: after the update, before the collision pass
+            rc = s->step_hook(s->step_hook_user);
+            if (rc) return rc < 0 ? fail(GTD_ERR_INVALID_ARGUMENT, "step hook returned %d", rc) : rc;
+        }
         if (s->coll != GTD_NO_COLL) {
             rc = run_collisions(s);
             if (rc) return rc;
@@ -424,6 +429,23 @@ static int evolve_steps(gtd_system *s, uint64_t k) {
         }
     }
     return GTD_OK;
+}
+
+// Entry points for the callback-driven evolve (callbacks.cu).
+int cb_evolve_begin(gtd_system *s, int method) { return evolve_begin(s, method); }
+int cb_direct_step(gtd_system *s) { return direct_step(s, s->method, true); }
+int cb_maybe_reorder(gtd_system *s) {
+    const int rc = maybe_reorder(s, false);
+    s->steps_since_reorder += 1;
+    return rc;
+}
+int cb_select_branch(int method) { return check_option(method) ? select_branch(method) : 0; }
+// Allocates what the steps of s->method use, so that they can be captured.
+int cb_prepare_steps(gtd_system *s) {
+    int rc = GTD_OK;
+    if (!(s->precision == GTD_PREC_F64 && s->n <= kFusedMaxN)) rc = ensure_plan(s);
+    if (!rc && (s->method == GTD_MODIFIED_EULER || s->method == GTD_MIDPOINT)) rc = ensure_pred(s);
+    return rc;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -486,6 +508,7 @@ int gtd_system_destroy(gtd_system *s) {
     release_record(s);
     release_io(s);
     release_graph(s);
+    release_callbacks(s);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     cudaEventDestroy(s->ev0);
     cudaEventDestroy(s->ev1);

@@ -59,6 +59,41 @@ def parse_units(units: str) -> float:
     return float(g)
 
 
+class _DeviceCallback:
+    """An evolve callback that runs on the GPU."""
+
+
+class RestFromCom(_DeviceCallback):
+    """random_comet's for_all_bods (gregsys.hpp:1966-1984) as device work: every step the carried
+    centre becomes (com + sum of positions) / N -- or (com + sum m x) / M with mass_weighted (the
+    GREGSYS_MERGERS form) -- with N and M taken at evolve() entry, then every body gets
+    rest = max_cor - (max_cor - min_cor) d^n_exp / (d^n_exp + scale_factor), d its distance to the
+    centre.  ``com`` holds the carried centre after evolve(), as the reference's lambda leaves its
+    captured _com."""
+
+    def __init__(self, min_cor, max_cor, scale_factor, n_exp, com, mass_weighted=False):
+        self.min_cor, self.max_cor, self.scale_factor, self.n_exp = min_cor, max_cor, scale_factor, n_exp
+        self.com = np.asarray(com, dtype=np.float64).reshape(3).copy()
+        self.mass_weighted = mass_weighted
+
+
+class WhileRestBelow(_DeviceCallback):
+    """random_comet's continue_ev_if (gregsys.hpp:1936-1963) on the device: true while some body
+    has rest < min_max_cor (resetting a counter), then for probing_iters more evaluations."""
+
+    def __init__(self, min_max_cor, probing_iters):
+        self.min_max_cor, self.probing_iters = min_max_cor, probing_iters
+
+
+class DeviceHook(_DeviceCallback):
+    """A caller's own device callback: ``fn`` is the address of a C function
+    ``int fn(void *user, const gtd_device_bodies *bodies)`` that enqueues GPU work on
+    ``bodies->stream`` (include/gtd_b200.h); ``user`` is passed back to it."""
+
+    def __init__(self, fn: int, user: int = 0):
+        self.fn, self.user = int(fn), int(user)
+
+
 @dataclass
 class Body:
     """gtd::body<M,R,T,0> fields that the force-and-step path reads and writes."""
@@ -255,13 +290,24 @@ class System:
             self.curr_ke = _ke(m, v)
 
     def evolve(self, integration_method: int = 16, continue_ev_if=None, for_each_bod=None,
-               for_all_bods=None) -> int:
+               for_all_bods=None, max_steps: int = 0) -> int:
         """gtd::system::evolve (gregsys.hpp:2593-3071).  Returns the elapsed device time in ns.
-        With callbacks, the state is brought back to the host every step for them (the
-        reference's contract), the stepping itself stays on the GPU."""
+
+        Callbacks are host callables -- continue_ev_if(), for_each_bod(system, i),
+        for_all_bods(system) -- which see the state every step (the reference's contract; the state
+        makes a host round trip for them), or device callbacks (RestFromCom, WhileRestBelow,
+        DeviceHook) that run on the GPU, with the bodies and the predicate kept on the device.  The
+        two kinds cannot be mixed.  max_steps (device callbacks only) stops a loop whose predicate
+        never turns false.  Per step, as in the reference (gregsys.hpp:16-106, 2970-2987):
+        continue_ev_if, the update, for_all_bods, the collision pass, for_each_bod."""
+        cbs = [c for c in (continue_ev_if, for_each_bod, for_all_bods) if c is not None]
+        if cbs and any(isinstance(c, _DeviceCallback) for c in cbs):
+            if not all(isinstance(c, _DeviceCallback) for c in cbs):
+                raise TypeError("device callbacks and host callables cannot be mixed in one evolve")
+            return self._evolve_device(integration_method, continue_ev_if, for_each_bod, for_all_bods, max_steps)
         self._push()
         ns = C.c_int64()
-        if continue_ev_if is None and for_each_bod is None and for_all_bods is None:
+        if not cbs:
             x0, v0 = self.x.copy(), self.v.copy()
             check(self._L.gtd_system_evolve(self._h, integration_method, C.byref(ns)))
             self._pull()
@@ -273,23 +319,101 @@ class System:
             return ns.value
         if self.mem_freq:
             raise NotImplementedError("memFreq recordings with evolve callbacks are not supported")
-        check(self._L.gtd_system_evolve_begin(self._h, integration_method))
-        steps = 0
-        while (continue_ev_if() if continue_ev_if is not None else steps < self.iterations):
-            check(self._L.gtd_system_evolve_steps(self._h, 1))
-            steps += 1
-            if for_all_bods is not None or for_each_bod is not None:
+        if (integration_method & System.barnes_hut) == System.barnes_hut:
+            # the Barnes-Hut branch calls no callback (gregsys.hpp:2893-2945)
+            check(self._L.gtd_system_evolve(self._h, integration_method, C.byref(ns)))
+            self._pull()
+            self.time_elapsed = self.iterations * self.dt
+            return ns.value
+        err = []
+
+        def step_hook(_user):
+            try:
                 self._pull()
-                if for_all_bods is not None:
-                    for_all_bods(self)
+                for_all_bods(self)
+                self._update()
+                return 0
+            except BaseException as e:  # re-raised below, after the engine unwinds
+                err.append(e)
+                return _lib.ERR_CALLBACK
+
+        hook = _lib.STEP_HOOK(step_hook) if for_all_bods is not None else None
+        L = self._L
+        try:
+            if hook is not None:
+                check(L.gtd_system_set_step_hook(self._h, C.cast(hook, C.c_void_p), None))
+            check(L.gtd_system_evolve_begin(self._h, integration_method))
+            steps = 0
+            while (continue_ev_if() if continue_ev_if is not None else steps < self.iterations):
+                rc = L.gtd_system_evolve_steps(self._h, 1)
+                if err:
+                    raise err[0]
+                check(rc)
+                steps += 1
                 if for_each_bod is not None:
+                    self._pull()
                     for i in range(len(self.m)):
                         for_each_bod(self, i)
-                self._push()
-                check(self._L.gtd_system_evolve_begin(self._h, integration_method))
+                    self._update()
+        finally:
+            if hook is not None:
+                L.gtd_system_set_step_hook(self._h, None, None)
         self._pull()
-        self.time_elapsed = steps * self.dt
+        self.time_elapsed = self.iterations * self.dt  # gregsys.hpp:3069, whatever the steps taken
+        self.steps_taken = steps
         return 0
+
+    def _update(self) -> None:
+        """A callback's writes, sent back without restarting the evolve in progress (the body count
+        cannot change inside a callback)."""
+        n = C.c_int64()
+        check(self._L.gtd_system_num_bodies(self._h, C.byref(n)))
+        if len(self.m) != n.value:
+            raise ValueError("an evolve callback changed the number of bodies")
+        self.m, self.r, self.rest = (np.ascontiguousarray(a, dtype=np.float64) for a in (self.m, self.r, self.rest))
+        self.x, self.v = (np.ascontiguousarray(a, dtype=np.float64).reshape(-1, 3) for a in (self.x, self.v))
+        check(self._L.gtd_system_update_bodies(self._h, ptr(self.m), ptr(self.r), ptr(self.rest), ptr(self.x),
+                                               ptr(self.v)))
+
+    def _evolve_device(self, method, cont, each, all_, max_steps) -> int:
+        L, h = self._L, self._h
+        self._push()
+        hooks = []
+        for cb in (cont, each, all_):
+            if isinstance(cb, DeviceHook):
+                hooks += [C.c_void_p(cb.fn), C.c_void_p(cb.user)]
+            else:
+                hooks += [None, None]
+        check(L.gtd_system_set_device_callbacks(h, *hooks))
+        if isinstance(cont, WhileRestBelow):
+            check(L.gtd_system_set_continue_while_rest_below(h, float(cont.min_max_cor), int(cont.probing_iters)))
+        if isinstance(all_, RestFromCom):
+            com = np.ascontiguousarray(all_.com, dtype=np.float64).reshape(3)
+            check(L.gtd_system_set_rest_from_com(h, float(all_.min_cor), float(all_.max_cor), float(all_.scale_factor),
+                                                 float(all_.n_exp), ptr(com), 1 if all_.mass_weighted else 0))
+        if isinstance(each, (WhileRestBelow, RestFromCom)) or isinstance(cont, RestFromCom) or \
+                isinstance(all_, WhileRestBelow):
+            raise TypeError("a built-in device callback was passed in the wrong position")
+        steps, ns = C.c_uint64(), C.c_int64()
+        try:
+            check(L.gtd_system_evolve_callbacks(h, method, int(max_steps), C.byref(steps), C.byref(ns)))
+        finally:
+            L.gtd_system_set_device_callbacks(h, None, None, None, None, None, None)
+        self._pull()
+        if isinstance(all_, RestFromCom):
+            c = np.zeros(3)
+            check(L.gtd_system_rest_from_com_centre(h, ptr(c)))
+            all_.com = c
+        self.time_elapsed = self.iterations * self.dt  # gregsys.hpp:3069, whatever the steps taken
+        self.steps_taken = steps.value
+        return ns.value
+
+    def callback_stats(self) -> dict:
+        """How the last device-callback evolve ran: host waits (one per 64-step graph chunk, or per
+        step in the eager form) and whether the CUDA-graph loop ran."""
+        w, g = C.c_uint64(), C.c_int()
+        check(self._L.gtd_system_callback_stats(self._h, C.byref(w), C.byref(g)))
+        return {"host_waits": w.value, "graph_loop": bool(g.value)}
 
     # ---- memFreq recordings ------------------------------------------------------------------
     def _clear_recordings(self) -> None:

@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <exception>
 #include <functional>
 #include <initializer_list>
 #include <ios>
@@ -27,6 +28,39 @@
 #include "gregbod.hpp"
 
 namespace gtd {
+
+// Device callbacks for evolve(): GPU work in place of the host callables (gtd_b200.h).
+namespace device {
+// random_comet's for_all_bods (gregsys.hpp:1966-1984): the carried centre *com becomes
+// (*com + sum of positions) / N (or (*com + sum m x) / M, the GREGSYS_MERGERS form), then every body
+// takes rest_c = max_cor - (max_cor - min_cor) d^n_exp / (d^n_exp + scale_factor), d its distance
+// to the centre.  *com is read at evolve() entry and written back at exit, as the reference's lambda
+// leaves its captured _com.
+template <typename T>
+struct rest_from_com {
+    long double min_cor, max_cor, scale_factor, n_exp;
+    vector3D<T> *com;
+    bool mass_weighted = false;
+};
+// random_comet's continue_ev_if (gregsys.hpp:1936-1963): true while some body has
+// rest_c < min_max_cor, then for probing_iters more evaluations.
+struct while_rest_below {
+    long double min_max_cor;
+    uint64_t probing_iters;
+};
+// The caller's own device callback: fn enqueues GPU work on the handle's stream (gtd_device_hook).
+struct hook {
+    gtd_device_hook fn;
+    void *user;
+};
+template <typename F>
+struct is_rest_from_com : std::false_type {};
+template <typename T>
+struct is_rest_from_com<rest_from_com<T>> : std::true_type {};
+template <typename F>
+struct is_callback : std::bool_constant<is_rest_from_com<F>::value || std::is_same_v<F, while_rest_below> ||
+                                        std::is_same_v<F, hook>> {};
+}  // namespace device
 
 template <isNumWrapper M = long double, isNumWrapper R = long double, isNumWrapper T = long double,
           bool prog = false, bool mergeOverlappingBodies = false, int collisions = 0, uint64_t memFreq = 0,
@@ -64,6 +98,7 @@ private:
     bool mixed = false;
     gtd_system *dev = nullptr;
     int device = 0;
+    uint64_t callback_step_limit = 0;
 
     void parse_units_format(const std::string &str) {  // gregsys.hpp:245-282
         static const std::regex re{R"(^\s*(m|M)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(d|D)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(t|T)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*$)\d*[1-9]+\d*\s*$)"};
@@ -183,6 +218,23 @@ private:
             b.curr_vel = vector3D<T>{(T)v[3 * i], (T)v[3 * i + 1], (T)v[3 * i + 2]};
             b.acc = vector3D<T>{(T)a[3 * i], (T)a[3 * i + 1], (T)a[3 * i + 2]};
         }
+    }
+    // A callback's writes to the body vector, sent back without restarting the evolve in progress.
+    void update() {
+        const int64_t n = (int64_t)bods.size();
+        int64_t dn = 0;
+        throw_status(gtd_system_num_bodies(dev, &dn));
+        if (n != dn) throw std::logic_error{"an evolve callback changed the number of bodies"};
+        std::vector<double> m(n), r(n), e(n), x(3 * n), v(3 * n);
+        for (int64_t i = 0; i < n; ++i) {
+            const bod_t &b = bods[i];
+            m[i] = (double)b.mass_;
+            r[i] = (double)b.radius;
+            e[i] = (double)b.rest_c;
+            x[3 * i] = (double)b.curr_pos.x; x[3 * i + 1] = (double)b.curr_pos.y; x[3 * i + 2] = (double)b.curr_pos.z;
+            v[3 * i] = (double)b.curr_vel.x; v[3 * i + 1] = (double)b.curr_vel.y; v[3 * i + 2] = (double)b.curr_vel.z;
+        }
+        throw_status(gtd_system_update_bodies(dev, m.data(), r.data(), e.data(), x.data(), v.data()));
     }
     void check_dt() {
         if (dt <= 0) throw std::invalid_argument{"Time-step cannot be zero or negative.\n"};
@@ -372,32 +424,108 @@ public:
     auto end() const { return bods.cend(); }
 
     // ---- evolve (gregsys.hpp:2593-3071) -----------------------------------------------------------
+    // Callbacks are either host callables (the reference's contract: they see the body vector; the
+    // state makes a host round trip per step) or device callbacks (gtd::device::*: GPU work, the
+    // bodies stay on the device and the predicate is evaluated there).  The two kinds cannot mix.
     template <typename evFuncT = std::nullptr_t, typename bodFuncT = std::nullptr_t,
               typename bodsFuncT = std::nullptr_t>
-        requires(std::same_as<evFuncT, std::nullptr_t> || requires(evFuncT f) { { f() } -> std::same_as<bool>; }) &&
-                (std::same_as<bodFuncT, std::nullptr_t> || requires(bodFuncT f, bod_t &b) { { f(b) } -> std::same_as<void>; }) &&
-                (std::same_as<bodsFuncT, std::nullptr_t> ||
+        requires(std::same_as<evFuncT, std::nullptr_t> || device::is_callback<evFuncT>::value ||
+                 requires(evFuncT f) { { f() } -> std::same_as<bool>; }) &&
+                (std::same_as<bodFuncT, std::nullptr_t> || device::is_callback<bodFuncT>::value ||
+                 requires(bodFuncT f, bod_t &b) { { f(b) } -> std::same_as<void>; }) &&
+                (std::same_as<bodsFuncT, std::nullptr_t> || device::is_callback<bodsFuncT>::value ||
                  requires(bodsFuncT f, std::vector<bod_t> &v) { { f(v) } -> std::same_as<void>; })
     const std::chrono::nanoseconds evolve(int integration_method = leapfrog_kdk,
                                           const evFuncT &continue_ev_if = nullptr,
                                           const bodFuncT &for_each_bod = nullptr,
                                           const bodsFuncT &for_all_bods = nullptr) {
         if (bods.empty()) return std::chrono::nanoseconds::zero();
+        constexpr bool no_cb = std::same_as<evFuncT, std::nullptr_t> && std::same_as<bodFuncT, std::nullptr_t> &&
+                               std::same_as<bodsFuncT, std::nullptr_t>;
+        constexpr bool dev_cb = device::is_callback<evFuncT>::value || device::is_callback<bodFuncT>::value ||
+                                device::is_callback<bodsFuncT>::value;
         if constexpr (memFreq != 0)
             for (bod_t &b : bods) b.clear_trajectory();  // clear_evolution (gregsys.hpp:2569-2586)
         push();
-        if constexpr (std::same_as<evFuncT, std::nullptr_t> && std::same_as<bodFuncT, std::nullptr_t> &&
-                      std::same_as<bodsFuncT, std::nullptr_t>) {
+        if constexpr (no_cb) {
             int64_t ns = 0;
             throw_status(gtd_system_evolve(dev, integration_method, &ns));
             pull();
             if constexpr (memFreq != 0) collect_recordings(integration_method);
             time_elapsed = iterations * dt;
             return std::chrono::nanoseconds{ns};
+        } else if constexpr (dev_cb) {
+            static_assert((std::same_as<evFuncT, std::nullptr_t> || device::is_callback<evFuncT>::value) &&
+                              (std::same_as<bodFuncT, std::nullptr_t> || device::is_callback<bodFuncT>::value) &&
+                              (std::same_as<bodsFuncT, std::nullptr_t> || device::is_callback<bodsFuncT>::value),
+                          "device callbacks and host callables cannot be mixed in one evolve");
+            static_assert(memFreq == 0, "memFreq recordings with evolve callbacks are not supported by the engine");
+            gtd_device_hook cf = nullptr, ef = nullptr, af = nullptr;
+            void *cu = nullptr, *eu = nullptr, *au = nullptr;
+            if constexpr (std::same_as<evFuncT, device::hook>) { cf = continue_ev_if.fn; cu = continue_ev_if.user; }
+            if constexpr (std::same_as<bodFuncT, device::hook>) { ef = for_each_bod.fn; eu = for_each_bod.user; }
+            if constexpr (std::same_as<bodsFuncT, device::hook>) { af = for_all_bods.fn; au = for_all_bods.user; }
+            throw_status(gtd_system_set_device_callbacks(dev, cf, cu, ef, eu, af, au));
+            if constexpr (std::same_as<evFuncT, device::while_rest_below>)
+                throw_status(gtd_system_set_continue_while_rest_below(dev, (double)continue_ev_if.min_max_cor,
+                                                                      continue_ev_if.probing_iters));
+            if constexpr (device::is_rest_from_com<bodsFuncT>::value) {
+                const double c[3] = {(double)for_all_bods.com->x, (double)for_all_bods.com->y,
+                                     (double)for_all_bods.com->z};
+                throw_status(gtd_system_set_rest_from_com(dev, (double)for_all_bods.min_cor, (double)for_all_bods.max_cor,
+                                                          (double)for_all_bods.scale_factor, (double)for_all_bods.n_exp,
+                                                          c, for_all_bods.mass_weighted ? 1 : 0));
+            }
+            uint64_t steps = 0;
+            int64_t ns = 0;
+            throw_status(gtd_system_evolve_callbacks(dev, integration_method, callback_step_limit, &steps, &ns));
+            pull();
+            if constexpr (device::is_rest_from_com<bodsFuncT>::value) {
+                double c[3];
+                throw_status(gtd_system_rest_from_com_centre(dev, c));
+                for_all_bods.com->x = c[0];
+                for_all_bods.com->y = c[1];
+                for_all_bods.com->z = c[2];
+            }
+            throw_status(gtd_system_set_device_callbacks(dev, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr));
+            time_elapsed = iterations * dt;  // gregsys.hpp:3069, whatever the steps taken
+            return std::chrono::nanoseconds{ns};
         } else {
             static_assert(memFreq == 0, "memFreq recordings with evolve callbacks are not supported by the engine");
-            // callbacks see the bodies every step: the state makes a host round trip per step
+            // host callables see the bodies every step: the state makes a host round trip for them.
+            // Order per step (gregsys.hpp:16-106, 2970-2987): continue_ev_if, the update, for_all_bods
+            // (inside the step, before the collision pass), the collision pass, for_each_bod.
             const auto start = std::chrono::steady_clock::now();
+            if ((integration_method & barnes_hut) == barnes_hut) {  // this branch calls no callback
+                int64_t ns = 0;
+                throw_status(gtd_system_evolve(dev, integration_method, &ns));
+                pull();
+                time_elapsed = iterations * dt;
+                return std::chrono::nanoseconds{ns};
+            }
+            struct hook_ctx {
+                system *self;
+                const bodsFuncT *all;
+                std::exception_ptr err;
+            } ctx{this, &for_all_bods, nullptr};
+            struct unhook {
+                gtd_system *d;
+                ~unhook() { gtd_system_set_step_hook(d, nullptr, nullptr); }
+            } guard{dev};
+            if constexpr (!std::same_as<bodsFuncT, std::nullptr_t>) {
+                throw_status(gtd_system_set_step_hook(dev, +[](void *u) -> int {
+                    auto *c = static_cast<hook_ctx *>(u);
+                    try {
+                        c->self->pull();
+                        (*c->all)(c->self->bods);
+                        c->self->update();
+                        return 0;
+                    } catch (...) {
+                        c->err = std::current_exception();
+                        return GTD_ERR_CALLBACK;
+                    }
+                }, &ctx));
+            }
             throw_status(gtd_system_evolve_begin(dev, integration_method));
             uint64_t steps = 0;
             while (true) {
@@ -406,20 +534,23 @@ public:
                 } else {
                     if (!continue_ev_if()) break;
                 }
-                throw_status(gtd_system_evolve_steps(dev, 1));
+                const int rc = gtd_system_evolve_steps(dev, 1);
+                if (ctx.err) std::rethrow_exception(ctx.err);
+                throw_status(rc);
                 ++steps;
-                pull();
-                if constexpr (!std::same_as<bodsFuncT, std::nullptr_t>) for_all_bods(bods);
-                if constexpr (!std::same_as<bodFuncT, std::nullptr_t>)
+                if constexpr (!std::same_as<bodFuncT, std::nullptr_t>) {
+                    pull();
                     for (bod_t &b : bods) for_each_bod(b);
-                push();
-                throw_status(gtd_system_evolve_begin(dev, integration_method));
+                    update();
+                }
             }
             pull();
-            time_elapsed = steps * dt;
+            time_elapsed = iterations * dt;  // gregsys.hpp:3069, whatever the steps taken
             return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - start);
         }
     }
+    // Guard for device-callback evolves whose predicate might never turn false (0: none).
+    void set_callback_step_limit(uint64_t max_steps) noexcept { callback_step_limit = max_steps; }
 };
 
 typedef system<long double, long double, long double> sys;

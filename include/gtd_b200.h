@@ -42,6 +42,7 @@ extern "C" {
 #define GTD_ERR_UNSUPPORTED 12            /* a method the reference leaves empty (rk4, rk3_8, ...) */
 #define GTD_ERR_NSYS_LOAD 13              /* gtd::nsys_load_error (gregsys.hpp:125-129) */
 #define GTD_ERR_NSYS_FORMAT 14            /* gtd::nsys_format_error (gregsys.hpp:130-134) */
+#define GTD_ERR_CALLBACK 15               /* an evolve callback (host step hook or device hook) failed */
 
 /* ---- integration-method flags, identical to gtd::system's (gregsys.hpp:156-165) ------------- */
 #define GTD_TWO_BODY 1
@@ -173,6 +174,71 @@ GTD_API int gtd_system_accelerations(gtd_system *sys, int method, double *a3);
  * momentum (sum of body::momentum, gregbod.hpp:595-597) and centre of mass (gregbod.hpp:1096-1106).
  * Any output may be NULL. */
 GTD_API int gtd_system_energy(gtd_system *sys, double *ke, double *pe, double *p3, double *com3);
+
+/* ---- evolve callbacks -------------------------------------------------------------------------
+ * gtd::system::evolve(method, continue_ev_if, for_each_bod, for_all_bods) (gregsys.hpp:2593-3071)
+ * calls continue_ev_if() before every step (without it: `iterations` steps), for_all_bods(bodies)
+ * after the step's update and before the collision pass (FUNC_TEMPL_SELECT, gregsys.hpp:16-106;
+ * leapfrog_kdk_acc_e_and_step, :528-539), and for_each_bod(body) on every body after that.  The
+ * Barnes-Hut branch calls none of them (gregsys.hpp:2893-2945).  Two ways to run them here. */
+
+/* Host callbacks.  `hook` runs on the host inside every step of gtd_system_evolve_steps, at
+ * for_all_bods' place (the state is synchronised then); it may read and write the bodies with
+ * gtd_system_download / gtd_system_update_bodies.  A nonzero return ends the evolve with that
+ * status.  NULL removes the hook. */
+typedef int (*gtd_step_hook)(void *user);
+GTD_API int gtd_system_set_step_hook(gtd_system *sys, gtd_step_hook hook, void *user);
+/* Overwrites the given arrays (any may be NULL) of the live bodies, in download order, without
+ * touching the accelerations or the evolve in progress (what a callback's writes to the reference's
+ * body vector do).  The body count cannot change here. */
+GTD_API int gtd_system_update_bodies(gtd_system *sys, const double *m, const double *r, const double *rest,
+                                     const double *x3, const double *v3);
+
+/* Device callbacks: GPU work that replaces a host callback, so the bodies never leave the device.
+ * A hook ENQUEUES work on `stream` and returns; it must not synchronise, allocate or read the
+ * bodies on the host.  gtd_system_evolve_callbacks records each hook's work once per step shape
+ * into a CUDA graph and replays it every step, so the work must be the same every step (state
+ * that changes belongs in device memory).  The arrays are in device order (upload order whenever
+ * collisions are on). */
+typedef struct gtd_device_bodies {
+    int64_t n;
+    double *pos_mass;              /* [n][4]: x, y, z, m */
+    double *vel;                   /* [n][4]: vx, vy, vz, unused */
+    double *acc;                   /* [n][4]: ax, ay, az, unused */
+    double *radius;                /* [n] */
+    double *rest;                  /* [n] coefficient of restitution (body::rest_c) */
+    const int32_t *upload_index;   /* [n] upload index of the body in each slot */
+    unsigned int *cont;            /* a continue_ev_if hook writes its verdict here: nonzero = step */
+    void *stream;                  /* cudaStream_t of the handle */
+} gtd_device_bodies;
+typedef int (*gtd_device_hook)(void *user, const gtd_device_bodies *bodies);
+/* Sets all three callbacks to user hooks (NULL: none), replacing the built-ins below. */
+GTD_API int gtd_system_set_device_callbacks(gtd_system *sys, gtd_device_hook continue_ev_if, void *cont_user,
+                                            gtd_device_hook for_each_bod, void *each_user,
+                                            gtd_device_hook for_all_bods, void *all_user);
+/* Built-in for_all_bods: random_comet's (gregsys.hpp:1965-1984).  Every step the carried centre
+ * becomes (centre + sum of positions) / N -- or (centre + sum of m x) / M with mass_weighted, the
+ * GREGSYS_MERGERS form -- with N and M the body count and total mass at this call, then every body
+ * takes rest = max_cor - (max_cor - min_cor) d^n_exp / (d^n_exp + scale_factor), d its distance
+ * to the centre.  com is the starting centre. */
+GTD_API int gtd_system_set_rest_from_com(gtd_system *sys, double min_cor, double max_cor, double scale_factor,
+                                         double n_exp, const double com[3], int mass_weighted);
+/* The carried centre of the built-in for_all_bods (random_comet reads it after evolve). */
+GTD_API int gtd_system_rest_from_com_centre(gtd_system *sys, double com[3]);
+/* Built-in continue_ev_if: random_comet's (gregsys.hpp:1936-1963): true while some body has
+ * rest < min_max_cor (resetting a counter), then true for probing_iters more evaluations. */
+GTD_API int gtd_system_set_continue_while_rest_below(gtd_system *sys, double min_max_cor, uint64_t probing_iters);
+/* evolve(method, callbacks) with the device callbacks set above; the predicate is evaluated on the
+ * device and the loop runs as CUDA-graph chunks whose conditional nodes stop at the first false
+ * verdict, so the host waits once per chunk, not per step.  max_steps > 0 stops after that many
+ * steps without evaluating the predicate again (a guard for predicates that never turn false).
+ * *steps_taken: steps run; *elapsed_ns: device time. */
+GTD_API int gtd_system_evolve_callbacks(gtd_system *sys, int method, uint64_t max_steps, uint64_t *steps_taken,
+                                        int64_t *elapsed_ns);
+/* How the last gtd_system_evolve_callbacks ran: host waits for the device (one per graph chunk, or
+ * one per step in the eager form used with merging collisions, the mixed path's periodic reorder or
+ * force timing) and whether the graph form ran. */
+GTD_API int gtd_system_callback_stats(const gtd_system *sys, uint64_t *host_waits, int *graph_loop);
 
 /* ---- instrumentation (no counterpart in the reference, which only returns evolve()'s wall time,
  * gregsys.hpp:2608-2625, 3061-3070) ------------------------------------------------------------ */

@@ -248,10 +248,37 @@ class RefOracle:
         L.ref_bh_kdk.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, C.c_uint64, C.c_double, C.c_double,
                                  C.c_char_p, _dp, _dp, _dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
 
+        L.ref_evolve_callbacks.restype = C.c_int
+        L.ref_evolve_callbacks.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_uint64,
+                                           C.c_char_p, C.c_int, C.c_double, C.c_uint64, C.c_int, C.c_double,
+                                           C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double,
+                                           C.c_uint64, _dp, _dp, _dp, _dp, C.POINTER(C.c_uint64)]
+
     def _chk(self, rc):
         if rc < 0:
             raise RuntimeError(self.lib.ref_last_error().decode())
         return rc
+
+    def evolve_callbacks(self, method, m, x, v, dt, iterations, units, r=None, rest=None, coll=0, cont=None,
+                         rest_from_com=None, each_factor=None, max_steps=0):
+        """The reference's evolve(method, continue_ev_if, for_each_bod, for_all_bods) with random_comet's
+        callbacks (ref_oracle.cpp, ref_access::evolve_callbacks).  cont: (min_max_cor, probing_iters)
+        or None; rest_from_com: (min_cor, max_cor, scale_factor, n_exp, com3, mass_weighted) or None;
+        each_factor: velocity scale of for_each_bod, or None.  Returns x, v, rest, steps, com."""
+        n = len(m)
+        xo, vo, ro = np.zeros(3 * n), np.zeros(3 * n), np.zeros(n)
+        r = _c3(np.zeros(n) if r is None else r)
+        rest = _c3(np.ones(n) if rest is None else rest)
+        mmc, probing = cont if cont is not None else (0.0, 0)
+        mn, mx, sc, ne, com, mw = rest_from_com if rest_from_com is not None else (0.0, 1.0, 1.0, 1.0, (0, 0, 0), 0)
+        com = np.ascontiguousarray(np.asarray(com, dtype=np.float64).copy())
+        steps = C.c_uint64()
+        self._chk(self.lib.ref_evolve_callbacks(
+            method, coll, n, _c3(m), r, rest, _c3(x), _c3(v), dt, iterations, units.encode(),
+            1 if cont is not None else 0, mmc, probing, 1 if rest_from_com is not None else 0, mn, mx, sc, ne,
+            int(mw), 1 if each_factor is not None else 0, each_factor or 1.0, max_steps, com, xo, vo, ro,
+            C.byref(steps)))
+        return xo.reshape(n, 3), vo.reshape(n, 3), ro, steps.value, com
 
     def G(self, units="M66743:66740,D1:1,T1:1"):
         g = C.c_longdouble()

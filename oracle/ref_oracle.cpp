@@ -208,6 +208,77 @@ public:
 
     template <typename A, typename B>
     static void merge_into(A &a, const B &b) { a += b; }
+
+    /* evolve(method, continue_ev_if, for_each_bod, for_all_bods) on the reference's own loop with the
+     * callbacks random_comet passes (gregsys.hpp:1935-1984), restated here as lambdas: continue
+     * while some body has rest_c < min_max_cor (resetting a counter), then probing_iters more
+     * steps; for_all_bods carries the centre (com += positions, then /= N, or m-weighted /= M) and
+     * sets rest_c from the distance to it.  for_each_bod (each_mode 1) scales every velocity by
+     * each_factor.  max_steps > 0 makes the predicate false once that many steps ran. */
+    struct cb_args {
+        int cont_mode, all_mode, each_mode, mass_weighted;
+        long double min_max_cor, min_cor, max_cor, scale_factor, n_exp;
+        uint64_t probing_iters, max_steps;
+        double each_factor;
+    };
+    template <typename S, typename C, typename E, typename A>
+    static void call_evolve(S &s, int method, const C &c, const E &e, const A &a) {
+        s.evolve(method, c, e, a);
+    }
+    template <typename S>
+    static uint64_t evolve_callbacks(S &s, int method, const cb_args &p, double *com_io) {
+        auto &bods = s.bods;
+        gtd::vector3D<double> com{com_io[0], com_io[1], com_io[2]};
+        const uint64_t n_ = bods.size();
+        double tot_mass = 0;
+        for (const auto &b : bods) tot_mass += b.mass_;
+        uint64_t count = 0, taken = 0;
+        auto cont = [&]() -> bool {
+            if (p.max_steps && taken >= p.max_steps) return false;
+            bool go = false, below = false;
+            for (const auto &b : bods)
+                if (b.rest_c < p.min_max_cor) {
+                    below = true;
+                    break;
+                }
+            if (below) {
+                count = 0;
+                go = true;
+            } else {
+                go = count++ < p.probing_iters;
+            }
+            if (go) ++taken;
+            return go;
+        };
+        auto all = [&](auto &bodies) {
+            if (p.mass_weighted) {
+                for (const auto &b : bodies) com += b.mass_ * b.curr_pos;
+                com /= tot_mass;
+            } else {
+                for (const auto &b : bodies) com += b.curr_pos;
+                com /= n_;
+            }
+            long double dist_exp;
+            for (auto &b : bodies) {
+                dist_exp = powl((b.curr_pos - com).magnitude(), p.n_exp);
+                b.rest_c = p.max_cor - (p.max_cor - p.min_cor) * (dist_exp / (dist_exp + p.scale_factor));
+            }
+        };
+        auto each = [&](auto &b) { b.curr_vel *= p.each_factor; };
+        const bool c = p.cont_mode != 0, a = p.all_mode != 0, e = p.each_mode != 0;
+        if (c && e && a) call_evolve(s, method, cont, each, all);
+        else if (c && e) call_evolve(s, method, cont, each, nullptr);
+        else if (c && a) call_evolve(s, method, cont, nullptr, all);
+        else if (c) call_evolve(s, method, cont, nullptr, nullptr);
+        else if (e && a) call_evolve(s, method, nullptr, each, all);
+        else if (e) call_evolve(s, method, nullptr, each, nullptr);
+        else if (a) call_evolve(s, method, nullptr, nullptr, all);
+        else call_evolve(s, method, nullptr, nullptr, nullptr);
+        com_io[0] = com.get_x();
+        com_io[1] = com.get_y();
+        com_io[2] = com.get_z();
+        return c ? taken : s.iterations;
+    }
 };
 }  // namespace gtd
 
@@ -618,4 +689,41 @@ int ref_bench_kdk(int n, const double *m, const double *x3, const double *v3, do
     return 0;
     REF_CATCH
 }
+}
+
+/* evolve(method, continue_ev_if, for_each_bod, for_all_bods) of
+ * gtd::system<double,double,double,false,false,coll,0,0,false> (coll 0 or 3) with random_comet's
+ * callbacks (ref_access::evolve_callbacks).  cont_mode / all_mode / each_mode 0 pass nullptr.
+ * com_io: the starting centre in, the carried centre out; rest_o: every body's rest_c after. */
+extern "C" int ref_evolve_callbacks(int method, int coll, int n, const double *m, const double *r, const double *rest,
+                                    const double *x3, const double *v3, double dt, uint64_t iterations,
+                                    const char *units, int cont_mode, double min_max_cor, uint64_t probing_iters,
+                                    int all_mode, double min_cor, double max_cor, double scale_factor, double n_exp,
+                                    int mass_weighted, int each_mode, double each_factor, uint64_t max_steps,
+                                    double *com_io, double *x3o, double *v3o, double *rest_o, uint64_t *steps) {
+    REF_TRY
+    ref_access::cb_args p{cont_mode, all_mode, each_mode, mass_weighted, (long double)min_max_cor,
+                          (long double)min_cor, (long double)max_cor, (long double)scale_factor, (long double)n_exp,
+                          probing_iters, max_steps, each_factor};
+    auto finish = [&](auto &s, uint64_t k) {
+        read_back(s, x3o, v3o, nullptr, nullptr, nullptr);
+        auto &b = ref_access::bodies(s);
+        for (size_t i = 0; i < b.size(); ++i) rest_o[i] = (double)ref_access::rest(b[i]);
+        *steps = k;
+    };
+    if (coll == 0) {
+        gtd::system<double, double, double, false, false, 0, 0, 0, false> s{make_bodies(n, m, r, rest, x3, v3),
+                                                                         (long double)dt, iterations, units, true};
+        finish(s, ref_access::evolve_callbacks(s, method, p, com_io));
+        return 0;
+    }
+    if (coll == 3) {
+        gtd::system<double, double, double, false, false, 3, 0, 0, false> s{make_bodies(n, m, r, rest, x3, v3),
+                                                                         (long double)dt, iterations, units, true};
+        finish(s, ref_access::evolve_callbacks(s, method, p, com_io));
+        return 0;
+    }
+    std::snprintf(g_err, sizeof g_err, "unsupported collision mode %d", coll);
+    return -1;
+    REF_CATCH
 }

@@ -133,6 +133,95 @@ def overlap_cluster(n: int, seed: int):
     return m, r, rest, x, v
 
 
+def comet_ball(n: int, R: float, b: float, seed: int):
+    """n non-overlapping bodies of radius b uniform in a ball of radius R, at rest (the placement of
+    random_comet, gregsys.hpp:1798-1850, with numpy's generator instead of mt19937_64)."""
+    rng = np.random.default_rng(seed)
+    pts = []
+    while len(pts) < n:
+        u = rng.uniform(-1.0, 1.0, 3)
+        if u @ u > 1.0:
+            continue
+        p = u * R
+        if all(np.linalg.norm(p - q) >= 2 * b for q in pts):
+            pts.append(p)
+    return np.array(pts)
+
+
+CB_UNITS = "M1:1,D1:1,T1:1"
+
+
+def comet_setup(n=64, R=8.0, b=1.0, mass=1.5e9, seed=3, weighted=False):
+    """random_comet's evolve stage (gregsys.hpp:1909-1984) with n_exp = 2 and d_scale = max_dist:
+    rest from the distance to the centre, min_cor 0.5, max_cor 1; continue while some body is
+    beyond max_dist, then 20 probing steps."""
+    x = comet_ball(n, R, b, seed)
+    m = np.full(n, mass) if not weighted else mass * np.exp(np.random.default_rng(seed + 1).uniform(-0.2, 0.2, n))
+    com = (m @ x) / m.sum() if weighted else x.mean(axis=0)
+    md = b * np.cbrt(n / (np.pi / 6))  # max_dist of random_comet for SCP packing
+    sf = md ** 2
+    mmc = 1.0 - 0.5 * (md ** 2 / (md ** 2 + sf))
+    d2 = np.sum((x - com) ** 2, axis=1)
+    rest0 = 1.0 - 0.5 * (d2 / (d2 + sf))
+    return dict(m=m, x=x, v=np.zeros_like(x), r=np.full(n, b), rest=rest0, com=com, sf=sf, mmc=mmc)
+
+
+def callback_fixtures(r, out):
+    """evolve(method, continue_ev_if, for_each_bod, for_all_bods) of the reference with
+    random_comet's callbacks (ref_access::evolve_callbacks in oracle/ref_oracle.cpp)."""
+    # (1) the comet stage itself: leapfrog KDK with overlap collisions until the predicate ends it
+    for tag, weighted in (("cbk", False), ("cbw", True)):
+        c = comet_setup(weighted=weighted)
+        xo, vo, ro, steps, com = r.evolve_callbacks(
+            16, c["m"], c["x"], c["v"], 0.25, 1000, CB_UNITS, r=c["r"], rest=c["rest"], coll=3,
+            cont=(c["mmc"], 20), rest_from_com=(0.5, 1.0, c["sf"], 2.0, c["com"], weighted), max_steps=3000)
+        for k in ("m", "x", "v", "r", "rest", "com"):
+            out[f"{tag}_{k}"] = c[k]
+        out[f"{tag}_par"] = np.array([c["mmc"], c["sf"]])
+        out[f"{tag}_xo"], out[f"{tag}_vo"], out[f"{tag}_ro"] = xo, vo, ro
+        out[f"{tag}_steps"], out[f"{tag}_como"] = np.array(steps), com
+    # the m-weighted run is chaotic well before it ends (a 1e-16 nudge of the initial positions
+    # moves its final state by 0.1): its state is also kept at step 131, where that nudge moves it
+    # by 3e-10 (positions) and 3e-9 (velocities); 131 = two 64-step chunks and an odd remainder
+    c = comet_setup(weighted=True)
+    xo, vo, ro, steps, com = r.evolve_callbacks(
+        16, c["m"], c["x"], c["v"], 0.25, 1000, CB_UNITS, r=c["r"], rest=c["rest"], coll=3,
+        cont=(c["mmc"], 20), rest_from_com=(0.5, 1.0, c["sf"], 2.0, c["com"], True), max_steps=131)
+    out["cbw131_xo"], out["cbw131_vo"], out["cbw131_ro"] = xo, vo, ro
+    out["cbw131_steps"], out["cbw131_como"] = np.array(steps), com
+    # (2) every method, 8 fixed steps (no predicate), for_all_bods + collisions + for_each_bod:
+    # the restitution of each step's collision pass comes from that step's for_all_bods
+    c = comet_setup(n=48, R=5.0, b=1.0, mass=4e9, seed=5)
+    for k in ("m", "x", "v", "r", "rest", "com"):
+        out[f"cbs_{k}"] = c[k]
+    out["cbs_par"] = np.array([c["mmc"], c["sf"]])
+    for name, meth in METHODS.items():
+        xo, vo, ro, steps, com = r.evolve_callbacks(
+            meth, c["m"], c["x"], c["v"], 0.25, 8, CB_UNITS, r=c["r"], rest=c["rest"], coll=3,
+            rest_from_com=(0.5, 1.0, c["sf"], 2.0, c["com"], False), each_factor=0.999)
+        out[f"cbs_{name}_xo"], out[f"cbs_{name}_vo"], out[f"cbs_{name}_ro"] = xo, vo, ro
+        out[f"cbs_{name}_como"] = com
+    # (3) the predicate alone on a collisionless Plummer sphere (rest never changes): all bodies at
+    # or above the bound -> exactly probing_iters steps (0, 63, 64, 70: around the 64-step graph
+    # chunks); one body below -> the predicate never ends, max_steps 37 does
+    m, x, v = plummer(40, 11)
+    out["cbp_m"], out["cbp_x"], out["cbp_v"] = m, x, v
+    rest_hi = np.full(40, 0.9)
+    rest_lo = rest_hi.copy()
+    rest_lo[17] = 0.1
+    out["cbp_rest_hi"], out["cbp_rest_lo"] = rest_hi, rest_lo
+    cases = []
+    for meth_name in ("leapfrog_kdk", "leapfrog_dkd", "euler"):
+        for probing, lo, cap in ((0, 0, 0), (63, 0, 0), (64, 0, 0), (70, 0, 0), (5, 1, 37)):
+            xo, vo, ro, steps, _ = r.evolve_callbacks(
+                METHODS[meth_name], m, x, v, 3600.0, 1000, UNITS_G6674, rest=rest_lo if lo else rest_hi,
+                cont=(0.5, probing), max_steps=cap)
+            key = f"cbp_{meth_name}_{probing}_{lo}_{cap}"
+            out[f"{key}_xo"], out[f"{key}_vo"], out[f"{key}_steps"] = xo, vo, np.array(steps)
+            cases.append(key)
+    out["cbp_cases"] = np.array(cases)
+
+
 def main():
     ensure_built(ref=True)
     r = RefOracle()
@@ -215,6 +304,7 @@ def main():
     out["bhck_xo"], out["bhck_vo"] = r.bh_kdk_coll(mk, rk, ek, xk, vk, 3600.0, 5, 0.5, UNITS_G6674)
     nsys_fixtures(r, out)
     record_fixtures(r, out)
+    callback_fixtures(r, out)
     path = os.path.join(HERE, "reference_golden.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes,", len(out), "arrays")
