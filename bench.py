@@ -62,7 +62,7 @@ def parse_args():
                    help="instead of the benchmark: evolve the workload this many steps in both the mixed and the "
                         "FP64 path and report |dE/E| and momentum drift every --drift-every steps")
     p.add_argument("--drift-every", type=int, default=100)
-    p.add_argument("--workload", choices=["direct-mixed", "direct-fp64-1024", "bh", "ensemble", "adjoint"],
+    p.add_argument("--workload", choices=["direct-mixed", "direct-fp64-1024", "bh", "ensemble", "adjoint", "comet"],
                    default="direct-mixed", help="direct-mixed is the headline; the others print their own line")
     p.add_argument("--bh-n", type=int, default=4194304)
     p.add_argument("--bh-cpu-n", type=int, default=10000)
@@ -73,6 +73,9 @@ def parse_args():
     p.add_argument("--adj-steps", type=int, default=2000)
     p.add_argument("--adj-every", type=int, default=45)
     p.add_argument("--adj-fd", type=int, default=0)
+    p.add_argument("--comet-steps", type=int, default=20000)
+    p.add_argument("--comet-host-steps", type=int, default=200)
+    p.add_argument("--comet-ref-steps", type=int, default=300)
     p.add_argument("--mixed-variant", type=int, default=-1,
                    help="use this mixed force-kernel variant instead of the autotuner's choice")
     return p.parse_args()
@@ -712,6 +715,96 @@ def run_adjoint(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_comet(args, local):
+    """random_comet's evolve stage as rsl9.cpp drives it (gregsys.hpp:1881-1984): N=727 bodies of
+    75 m and 4.197e9 kg at rest in a 1600 m ball, n_exp = 3, d_scale = 1200 m, restitution 0.5..0.95,
+    dt = 1/128 s, overlap collisions, leapfrog KDK; continue_ev_if (some body beyond max_dist, then
+    50000 probing steps) and for_all_bods (restitution from the carried centre) every step.  The
+    predicate stays true far longer than a benchmark runs, so max_steps fixes the steps timed.
+    Arms: device callbacks (the CUDA-graph loop), host callables (the reference's contract: a host
+    round trip of the state per step), the reference's own evolve on one core."""
+    from gregpackagescpp_b200 import RestFromCom, System, WhileRestBelow
+    from gregpackagescpp_b200.ics import comet_stage
+    c = comet_stage(727, 1600.0, 75.0, 4197481476.49696707306, 3.0, 1200.0, 0.5, 0.95, 0.0, args.seed)
+    dt, units, probing = 0.0625 / 8, "M1:1,D1:1,T1:1", 50000
+    mmc, sf = c["min_max_cor"], c["scale_factor"]
+
+    def fresh():
+        return System(c["m"], c["x"], c["v"], r=c["r"], rest=c["rest"], timestep=dt, num_iterations=100,
+                      units_format=units, collisions=3, device=local)
+
+    def launches(s):
+        k = C.c_uint64()
+        _lib.check(s._L.gtd_system_launch_count(s._h, C.byref(k)))
+        return k.value
+
+    from gregpackagescpp_b200 import _lib
+    K = args.comet_steps
+    s = fresh()
+    fab = RestFromCom(0.5, 0.95, sf, 3.0, c["com"])
+    s.evolve(16, WhileRestBelow(mmc, probing), None, fab, max_steps=max(args.warmup, 3) * 64)  # warm-up
+    l0 = launches(s)
+    t0 = time.perf_counter()
+    ns = s.evolve(16, WhileRestBelow(mmc, probing), None, fab, max_steps=K)
+    wall = time.perf_counter() - t0
+    st = s.callback_stats()
+    line = {"workload": "random_comet evolve stage (rsl9.cpp): N=727, leapfrog KDK dt=1/128 s, overlap "
+                        "collisions, restitution from the carried centre every step", "unit": "comet steps/s",
+            "steps": s.steps_taken, "value": s.steps_taken / (ns * 1e-9), "us_per_step": ns * 1e-3 / s.steps_taken,
+            "e2e_value": s.steps_taken / wall, "host_waits": st["host_waits"], "graph_loop": st["graph_loop"],
+            "gpu_launches": launches(s) - l0}
+    # host callables: the same callbacks in numpy, the state brought back every step
+    h = fresh()
+    cnt = {"probe": 0, "taken": 0}
+    hc = {"com": c["com"].copy()}
+    KH = args.comet_host_steps
+
+    def cont():
+        if cnt["taken"] >= KH:
+            return False
+        if (h.rest < mmc).any():
+            cnt["probe"] = 0
+            go = True
+        else:
+            go = cnt["probe"] < probing
+            cnt["probe"] += 1
+        cnt["taken"] += go
+        return go
+
+    def for_all(sys_):
+        hc["com"] = (hc["com"] + sys_.x.sum(axis=0)) / len(sys_.m)
+        de = np.sqrt(((sys_.x - hc["com"]) ** 2).sum(axis=1)) ** 3.0
+        sys_.rest = 0.95 - (0.95 - 0.5) * (de / (de + sf))
+
+    t0 = time.perf_counter()
+    h.evolve(16, cont, None, for_all)
+    line["host_callbacks"] = {"value": h.steps_taken / (time.perf_counter() - t0), "steps": h.steps_taken}
+    try:
+        from oracle.oracle import RefOracle
+        if RefOracle.available():
+            ro = RefOracle()
+            KR = args.comet_ref_steps
+            args_ref = dict(r=c["r"], rest=c["rest"], coll=3, cont=(mmc, probing),
+                            rest_from_com=(0.5, 0.95, sf, 3.0, c["com"], 0))
+            t0 = time.perf_counter()
+            ro.evolve_callbacks(16, c["m"], c["x"], c["v"], dt, 100, units, max_steps=1, **args_ref)
+            t1 = time.perf_counter()
+            xr, vr, rr, kr, _ = ro.evolve_callbacks(16, c["m"], c["x"], c["v"], dt, 100, units, max_steps=KR,
+                                                    **args_ref)
+            t2 = time.perf_counter()
+            line["reference_cpu"] = {"value": (KR - 1) / ((t2 - t1) - (t1 - t0)), "cores": 1,
+                                     "sample": f"{KR} steps (one step subtracted: construction, first force)"}
+            d = fresh()
+            d.evolve(16, WhileRestBelow(mmc, probing), None, RestFromCom(0.5, 0.95, sf, 3.0, c["com"]),
+                     max_steps=KR)
+            line["final_state_rel_err"] = {"x": float(np.abs(d.x - xr).max() / np.abs(xr).max()),
+                                           "v": float(np.abs(d.v - vr).max() / max(np.abs(vr).max(), 1e-300)),
+                                           "steps": KR}
+    except Exception as exc:  # the reference library is optional on a box
+        line["reference_cpu"] = {"unavailable": str(exc)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_init()
@@ -724,7 +817,7 @@ def main():
         elif args.workload != "direct-mixed":
             if rank == 0:
                 {"direct-fp64-1024": run_fp64_small, "bh": run_bh, "ensemble": run_ensemble,
-                 "adjoint": run_adjoint}[args.workload](args, local)
+                 "adjoint": run_adjoint, "comet": run_comet}[args.workload](args, local)
         else:
             run_ours(args, rank, world, local)
     finally:

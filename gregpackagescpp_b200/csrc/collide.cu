@@ -10,12 +10,15 @@
 //    the merge itself is body::operator+= (gregbod.hpp:1066-1082): mass-weighted position,
 //    velocity and acceleration, summed mass, r = cbrt(r1^3 + r2^3), mean restitution.
 //
-// Detection of all overlapping pairs is a tiled O(N^2) kernel (FP64); the order-dependent
-// resolution runs on one thread (restitution) or one block (merges), as the reference's
-// sequential loops define the result.
+// Detection of all overlapping pairs is a tiled O(N^2) kernel (FP64).  The order-dependent
+// restitution is resolved by one CTA that orders the outer bodies' groups by their data
+// dependencies and applies independent groups in parallel, reproducing the sequential loop's
+// result (a single thread takes over above kFastCand pairs); merges run on one block, as the
+// reference's sequential scan defines the result.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "gtd_internal.cuh"
 #include "gtd_system.cuh"
@@ -30,38 +33,54 @@ struct Cand {
     double dist;
 };
 
-// All pairs o < i with dist < r_o + r_i; appends (o, i, dist) to the candidate list.
-__global__ void __launch_bounds__(kCT) overlap_pairs_kernel(int64_t n, const double4 *pm, const double *rad,
-                                                            Cand *cand, int *count, int cap) {
-    __shared__ double4 tp[kCT];
-    __shared__ double tr[kCT];
-    const int64_t o = (int64_t)blockIdx.x * kCT + threadIdx.x;
-    const double4 po = o < n ? pm[o] : make_double4(0, 0, 0, 0);
-    const double ro = o < n ? rad[o] : 0.0;
-    const int64_t first_tile = (int64_t)blockIdx.x * kCT;
-    for (int64_t j0 = first_tile; j0 < n; j0 += kCT) {
-        const int64_t j = j0 + threadIdx.x;
-        tp[threadIdx.x] = j < n ? pm[j] : make_double4(0, 0, 0, 0);
-        tr[threadIdx.x] = j < n ? rad[j] : 0.0;
-        __syncthreads();
-        if (o < n) {
-            const int lim = (int)min((int64_t)kCT, n - j0);
-            for (int jj = 0; jj < lim; ++jj) {
-                const int64_t i = j0 + jj;
-                if (i <= o) continue;
-                const double4 q = tp[jj];
-                const double dx = __dsub_rn(q.x, po.x), dy = __dsub_rn(q.y, po.y), dz = __dsub_rn(q.z, po.z);
-                const double d = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-                const double rsum = __dadd_rn(ro, tr[jj]);
-                if (rsum > d) {
-                    const int k = atomicAdd(count, 1);
-                    if (k < cap) cand[k] = Cand{(int32_t)o, (int32_t)i, d};
-                }
-            }
+// All pairs o < i with dist < r_o + r_i; appends (o, i, dist) to the candidate list.  One CTA per
+// (o-tile, j-tile) pair of the upper triangle of kDT x kDT tiles, so that small systems still spread
+// over the SMs.  The square root is taken only for pairs whose squared distance is not clearly
+// above (r_o + r_i)^2; the overlap decision is the one of the exact test.
+constexpr int kDT = 64;
+
+__global__ void __launch_bounds__(kDT) overlap_pairs_kernel(int64_t n, int64_t tiles, const double4 *pm,
+                                                            const double *rad, Cand *cand, int *count, int cap) {
+    __shared__ double4 tp[kDT];
+    __shared__ double tr[kDT];
+    // block -> (to, tj), to <= tj: row r of the triangle starts at r*T - r(r-1)/2
+    const int64_t b = blockIdx.x, T = tiles;
+    auto row_start = [&](int64_t r) { return r * T - r * (r - 1) / 2; };
+    const double q = (double)(2 * T + 1);
+    int64_t to = (int64_t)floor((q - sqrt(q * q - 8.0 * (double)b)) * 0.5);
+    if (to < 0) to = 0;
+    if (to > T - 1) to = T - 1;
+    while (to > 0 && row_start(to) > b) --to;
+    while (to + 1 < T && row_start(to + 1) <= b) ++to;
+    const int64_t tj = to + (b - row_start(to));
+    const int t = threadIdx.x;
+    const int64_t j = tj * kDT + t;
+    tp[t] = j < n ? pm[j] : make_double4(0, 0, 0, 0);
+    tr[t] = j < n ? rad[j] : 0.0;
+    __syncthreads();
+    const int64_t o = to * kDT + t;
+    if (o >= n) return;
+    const double4 po = pm[o];
+    const double ro = rad[o];
+    const int lim = (int)min((int64_t)kDT, n - tj * kDT);
+    for (int jj = 0; jj < lim; ++jj) {
+        const int64_t i = tj * kDT + jj;
+        if (i <= o) continue;
+        const double4 qj = tp[jj];
+        const double dx = __dsub_rn(qj.x, po.x), dy = __dsub_rn(qj.y, po.y), dz = __dsub_rn(qj.z, po.z);
+        const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        const double rsum = __dadd_rn(ro, tr[jj]);
+        // d2 > rsum^2 (1 + 2^-40) implies sqrt(d2) > rsum whatever the roundings: no overlap
+        if (d2 > __dmul_rn(__dmul_rn(rsum, rsum), 1.0 + 0x1p-40)) continue;
+        const double d = sqrt(d2);
+        if (rsum > d) {
+            const int k = atomicAdd(count, 1);
+            if (k < cap) cand[k] = Cand{(int32_t)o, (int32_t)i, d};
         }
-        __syncthreads();
     }
 }
+
+int64_t overlap_tiles(int64_t n) { return (n + kDT - 1) / kDT; }
 
 __device__ __forceinline__ bool cand_less(const Cand &a, const Cand &b) {
     if (a.o != b.o) return a.o < b.o;
@@ -69,18 +88,42 @@ __device__ __forceinline__ bool cand_less(const Cand &a, const Cand &b) {
     return a.i < b.i;
 }
 
-// One thread: heap sort of the candidates by (o, dist, i), then the sequential s_coll response.
-// With perm != nullptr the candidates hold Barnes-Hut slots (the order of the reference's leaf and
-// neighbour iteration) and perm maps them to bodies.
-__global__ void restitution_kernel(Cand *cand, const int *count, int cap, const int32_t *perm, const double4 *pm,
-                                   const double *rest, double4 *vel, int *status) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    int c = *count;
-    if (c > cap) {
-        *status = GTD_ERR_CAPACITY;
-        return;
-    }
-    // heap sort
+// The s_coll response to one candidate k of outer body o (gregsys.hpp:808-836): the momenta along
+// the unit separation were snapshotted for the whole group (pp); returns whether the pair gets the
+// impulse, with o's velocity change d_o along u and i's velocity vi updated.
+__device__ __forceinline__ bool pair_impulse(const double4 &xo, double rest_o, const double4 &xi, double rest_i,
+                                             double d, double2 pp, double4 &vi, double &d_o, double &ux,
+                                             double &uy, double &uz) {
+    ux = (xi.x - xo.x) / d;
+    uy = (xi.y - xo.y) / d;
+    uz = (xi.z - xo.z) / d;
+    const double mo = xo.w, mi = xi.w;
+    const double o_vel = pp.x / mo, i_vel = pp.y / mi;
+    const double o_minus_i = o_vel - i_vel;
+    const double avg_rest = 0.5 * (rest_o + rest_i);
+    if (!(o_vel > 0 || i_vel < 0)) return false;
+    if (o_vel <= 0 && i_vel < 0 && o_vel < i_vel) return false;  // already separating
+    if (o_vel > 0 && i_vel >= 0 && o_vel < i_vel) return false;
+    const double psum = pp.x + pp.y, msum = mo + mi;
+    const double new_o = (psum - mi * avg_rest * o_minus_i) / msum;
+    const double new_i = (psum + mo * avg_rest * o_minus_i) / msum;
+    d_o = new_o - o_vel;
+    const double d_i = new_i - i_vel;
+    vi.x += d_i * ux;
+    vi.y += d_i * uy;
+    vi.z += d_i * uz;
+    return true;
+}
+
+// Momentum of a body along u, as bod->momentum()*r12 (gregbod.hpp:595-597, dot gregvec.hpp:3742).
+__device__ __forceinline__ double axis_momentum(const double4 &x, const double4 &v, double ux, double uy, double uz) {
+    return x.w * v.x * ux + x.w * v.y * uy + x.w * v.z * uz;
+}
+
+// The sequential form (one thread): heap sort of the candidates by (o, dist, i), then the groups in
+// order.  Used above kFastCand candidates.
+__device__ void resolve_serial(Cand *cand, int c, int cap, const int32_t *perm, const double4 *pm,
+                               const double *rest, double4 *vel) {
     for (int start = c / 2 - 1; start >= 0; --start) {
         int root = start;
         while (true) {
@@ -105,6 +148,7 @@ __global__ void restitution_kernel(Cand *cand, const int *count, int cap, const 
         }
     }
     auto body = [&](int32_t q) { return perm ? perm[q] : q; };
+    double2 *mom = reinterpret_cast<double2 *>(cand + cap);
     int g = 0;
     while (g < c) {
         const int og = cand[g].o;
@@ -118,41 +162,339 @@ __global__ void restitution_kernel(Cand *cand, const int *count, int cap, const 
             const double4 xi = pm[i];
             const double d = cand[k].dist;
             const double ux = (xi.x - xo.x) / d, uy = (xi.y - xo.y) / d, uz = (xi.z - xo.z) / d;
-            const double4 vo = vel[o], vi = vel[i];
-            const double po = xo.w * vo.x * ux + xo.w * vo.y * uy + xo.w * vo.z * uz;
-            const double pi = xi.w * vi.x * ux + xi.w * vi.y * uy + xi.w * vi.z * uz;
-            // reuse the record: dist keeps the key, o/i the bodies; stash momenta in a side slot
-            cand[k].dist = d;
-            reinterpret_cast<double2 *>(cand + cap)[k] = make_double2(po, pi);
+            mom[k] = make_double2(axis_momentum(xo, vel[o], ux, uy, uz), axis_momentum(xi, vel[i], ux, uy, uz));
         }
-        double prev = -1.0;
         for (int k = g; k < e; ++k) {
-            const double d = cand[k].dist;
-            if (k > g && d == prev) continue;  // std::map::emplace keeps the first equal key
-            prev = d;
+            if (k > g && cand[k].dist == cand[k - 1].dist) continue;  // std::map::emplace keeps the first key
             const int i = body(cand[k].i);
-            const double4 xi = pm[i];
-            const double ux = (xi.x - xo.x) / d, uy = (xi.y - xo.y) / d, uz = (xi.z - xo.z) / d;
-            const double2 pp = reinterpret_cast<double2 *>(cand + cap)[k];
-            const double mo = xo.w, mi = xi.w;
-            const double o_vel = pp.x / mo, i_vel = pp.y / mi;
-            const double o_minus_i = o_vel - i_vel;
-            const double avg_rest = 0.5 * (rest[o] + rest[i]);
-            if (o_vel > 0 || i_vel < 0) {
-                if (o_vel <= 0 && i_vel < 0 && o_vel < i_vel) continue;
-                if (o_vel > 0 && i_vel >= 0 && o_vel < i_vel) continue;
-                const double psum = pp.x + pp.y, msum = mo + mi;
-                const double new_o = (psum - mi * avg_rest * o_minus_i) / msum;
-                const double new_i = (psum + mo * avg_rest * o_minus_i) / msum;
-                const double d_o = new_o - o_vel, d_i = new_i - i_vel;
-                double4 vo = vel[o], vi = vel[i];
-                vo.x += d_o * ux; vo.y += d_o * uy; vo.z += d_o * uz;
-                vi.x += d_i * ux; vi.y += d_i * uy; vi.z += d_i * uz;
-                vel[o] = vo;
+            double d_o, ux, uy, uz;
+            double4 vi = vel[i];
+            if (pair_impulse(xo, rest[o], pm[i], rest[i], cand[k].dist, mom[k], vi, d_o, ux, uy, uz)) {
                 vel[i] = vi;
+                double4 vo = vel[o];
+                vo.x += d_o * ux;
+                vo.y += d_o * uy;
+                vo.z += d_o * uz;
+                vel[o] = vo;
             }
         }
         g = e;
+    }
+}
+
+// ---- the parallel resolution ------------------------------------------------------------------
+// The reference resolves the outer bodies' groups in order; a group reads and writes the
+// velocities of its outer body and of its partners only.  So a group depends on the earlier groups
+// that share a body with it, and groups at the same depth of that dependency order touch disjoint
+// bodies.  One CTA: sorts the candidates by outer body (bitonic on 64-bit keys in shared memory)
+// and each group by (distance, partner); gives every group its depth (the longest chain of earlier
+// groups sharing a body, found by relaxing over each body's groups in order); lists the groups of
+// each depth; then applies the depths one after another, a warp per group and a lane per pair.
+// Every velocity sees exactly the updates, in the order, that the sequential loop gives it.
+constexpr int kResolveThreads = 512;
+constexpr int kFastCand = 4096;
+
+// Shared-memory layout of restitution_kernel, sized for kFastCand candidates.
+struct ResolveSmem {
+    static constexpr size_t F = kFastCand;
+    static constexpr size_t ck = 0;                      // u64 [F + 2]: (o, k) keys; later depth lists
+    static constexpr size_t sd = ck + 8 * (F + 2);       // double [F]: distances (sorted order)
+    static constexpr size_t si = sd + 8 * F;             // int [F]: partners (sorted order)
+    static constexpr size_t go = si + 4 * F;             // int [F]: outer body of each group
+    static constexpr size_t gstart = go + 4 * F;         // int [F + 1]
+    static constexpr size_t aux = gstart + 4 * (F + 1);  // int [F]: scan, group ids, cursors
+    static constexpr size_t key = aux + 4 * F + 12;      // u64 [2F] (16-aligned): (body, group); later momenta
+    static constexpr size_t lev = key + 16 * F;          // int [F]: depths
+    static constexpr size_t scratch = lev + 4 * F;       // int [64]
+    static constexpr size_t bytes = scratch + 4 * 64;
+};
+static_assert(ResolveSmem::key % 16 == 0, "momenta alias the key array as double2");
+
+size_t resolve_smem_bytes() { return ResolveSmem::bytes; }
+
+template <typename Less, typename Swap>
+__device__ void bitonic_sort(int P, Less less, Swap swp) {
+    for (int k = 2; k <= P; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int x = threadIdx.x; x < P / 2; x += blockDim.x) {
+                const int i = (x / j) * 2 * j + (x % j);
+                const int l = i + j;
+                const bool up = (i & k) == 0;
+                if (up ? less(l, i) : less(i, l)) swp(i, l);
+            }
+            __syncthreads();
+        }
+}
+
+__device__ void bitonic_sort_u64(unsigned long long *a, int P) {
+    bitonic_sort(
+        P, [&](int x, int y) { return a[x] < a[y]; },
+        [&](int x, int y) {
+            const unsigned long long v = a[x];
+            a[x] = a[y];
+            a[y] = v;
+        });
+}
+
+// Exclusive prefix sum of a[0..len) in place; returns the total.  scratch: 33 ints.
+__device__ int block_exclusive_scan(int *a, int len, int *scratch) {
+    const int t = threadIdx.x, nt = blockDim.x, lane = t & 31;
+    const int per = (len + nt - 1) / nt;
+    const int b0 = min(len, t * per), b1 = min(len, b0 + per);
+    int s = 0;
+    for (int k = b0; k < b1; ++k) s += a[k];
+    int x = s;
+    for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) scratch[t >> 5] = x;
+    __syncthreads();
+    if (t < 32) {
+        const int w = t < (nt >> 5) ? scratch[t] : 0;
+        int z = w;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, z, d);
+            if (t >= d) z += y;
+        }
+        scratch[t] = z - w;
+        if (t == 31) scratch[32] = z;
+    }
+    __syncthreads();
+    int run = scratch[t >> 5] + (x - s);
+    for (int k = b0; k < b1; ++k) {
+        const int v = a[k];
+        a[k] = run;
+        run += v;
+    }
+    __syncthreads();
+    const int total = scratch[32];
+    __syncthreads();
+    return total;
+}
+
+// With perm != nullptr the candidates hold Barnes-Hut slots (the order of the reference's leaf and
+// neighbour iteration) and perm maps them to bodies.
+__global__ void __launch_bounds__(kResolveThreads, 1) restitution_kernel(Cand *cand, const int *count, int cap,
+                                                                         const int32_t *perm, const double4 *pm,
+                                                                         const double *rest, double4 *vel,
+                                                                         int *status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    using L = ResolveSmem;
+    const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, warp = t >> 5, nw = nt >> 5;
+    const int c = *count;
+    if (c > cap) {
+        if (t == 0) *status = GTD_ERR_CAPACITY;
+        return;
+    }
+    if (c <= 0) return;
+    if (c > kFastCand) {
+        if (t == 0) resolve_serial(cand, c, cap, perm, pm, rest, vel);
+        return;
+    }
+    unsigned long long *ck = reinterpret_cast<unsigned long long *>(smem + L::ck);
+    double *sd = reinterpret_cast<double *>(smem + L::sd);
+    int *si = reinterpret_cast<int *>(smem + L::si);
+    int *go = reinterpret_cast<int *>(smem + L::go);
+    int *gstart = reinterpret_cast<int *>(smem + L::gstart);
+    int *aux = reinterpret_cast<int *>(smem + L::aux);
+    unsigned long long *key = reinterpret_cast<unsigned long long *>(smem + L::key);
+    int *lev = reinterpret_cast<int *>(smem + L::lev);
+    int *scratch = reinterpret_cast<int *>(smem + L::scratch);
+    int *flag = scratch + 40;
+    auto body = [&](int q) { return perm ? perm[q] : q; };
+    constexpr unsigned long long kNone = ~0ull;
+
+    int P = 2;
+    while (P < c) P <<= 1;
+    // (outer body, arrival index) keys; distances and partners stay in arrival order for now
+    for (int k = t; k < P; k += nt) {
+        if (k < c) {
+            const Cand cd = cand[k];
+            ck[k] = ((unsigned long long)(unsigned)cd.o << 32) | (unsigned)k;
+            sd[k] = cd.dist;
+            si[k] = cd.i;
+        } else {
+            ck[k] = kNone;
+        }
+    }
+    __syncthreads();
+    bitonic_sort_u64(ck, P);
+    // groups: heads where the outer body changes
+    for (int p = t; p < P; p += nt) aux[p] = (p < c && (p == 0 || (ck[p] >> 32) != (ck[p - 1] >> 32))) ? 1 : 0;
+    __syncthreads();
+    const int G = block_exclusive_scan(aux, P, scratch);
+    for (int p = t; p < c; p += nt) {
+        const bool head = p == 0 || (ck[p] >> 32) != (ck[p - 1] >> 32);
+        const int g = aux[p] + (head ? 1 : 0) - 1;
+        if (head) {
+            gstart[g] = p;
+            go[g] = (int)(ck[p] >> 32);
+        }
+        aux[p] = g;
+    }
+    if (t == 0) gstart[G] = c;
+    __syncthreads();
+    // each group by (distance, partner): the std::map order, the first of equal keys kept
+    for (int g = t; g < G; g += nt) {
+        const int b0 = gstart[g], b1 = gstart[g + 1];
+        for (int p = b0 + 1; p < b1; ++p) {
+            const unsigned long long v = ck[p];
+            const int kv = (int)(v & 0xffffffffu);
+            int q = p - 1;
+            while (q >= b0) {
+                const int kq = (int)(ck[q] & 0xffffffffu);
+                if (sd[kq] < sd[kv] || (sd[kq] == sd[kv] && si[kq] < si[kv])) break;
+                ck[q + 1] = ck[q];
+                --q;
+            }
+            ck[q + 1] = v;
+        }
+    }
+    __syncthreads();
+    // distances and partners into sorted order (the key array is free scratch until its keys)
+    {
+        double *td = reinterpret_cast<double *>(key);
+        int *ti = reinterpret_cast<int *>(td + kFastCand);
+        for (int p = t; p < c; p += nt) {
+            const int k = (int)(ck[p] & 0xffffffffu);
+            td[p] = sd[k];
+            ti[p] = si[k];
+        }
+        __syncthreads();
+        for (int p = t; p < c; p += nt) {
+            sd[p] = td[p];
+            si[p] = ti[p];
+        }
+        __syncthreads();
+    }
+    // (body, group) keys: every group's outer body and every kept partner
+    const int E = G + c;
+    int E2 = 2;
+    while (E2 < E) E2 <<= 1;
+    for (int e = t; e < E2; e += nt) {
+        unsigned long long kv = kNone;
+        if (e < G) {
+            kv = ((unsigned long long)(unsigned)go[e] << 32) | (unsigned)e;
+        } else if (e < E) {
+            const int p = e - G, g = aux[p];
+            const bool dup = p > gstart[g] && sd[p] == sd[p - 1];
+            if (!dup) kv = ((unsigned long long)(unsigned)si[p] << 32) | (unsigned)g;
+        }
+        key[e] = kv;
+    }
+    for (int g = t; g < G; g += nt) lev[g] = 0;
+    __syncthreads();
+    bitonic_sort_u64(key, E2);
+    // depths: a group is one deeper than the last earlier group that shares a body with it
+    for (int it = 0; it <= G; ++it) {
+        if (t == 0) flag[0] = 0;
+        __syncthreads();
+        for (int e = t + 1; e < E; e += nt) {
+            const unsigned long long ke = key[e], kp = key[e - 1];
+            if (ke == kNone || (ke >> 32) != (kp >> 32)) continue;
+            const int g = (int)(ke & 0xffffffffu), q = (int)(kp & 0xffffffffu);
+            const int need = lev[q] + 1;
+            if (lev[g] < need) {
+                atomicMax(&lev[g], need);
+                flag[0] = 1;
+            }
+        }
+        __syncthreads();
+        if (!flag[0]) break;
+        __syncthreads();
+    }
+    if (t == 0) flag[1] = 0;
+    __syncthreads();
+    for (int g = t; g < G; g += nt) atomicMax(&flag[1], lev[g]);
+    __syncthreads();
+    const int D = flag[1] + 1;
+    // the groups of each depth: lorder[lstart[d] .. lstart[d + 1])
+    int *lorder = reinterpret_cast<int *>(ck);
+    int *lstart = lorder + kFastCand;
+    for (int d = t; d <= D; d += nt) lstart[d] = 0;
+    for (int d = t; d < D; d += nt) aux[d] = 0;
+    __syncthreads();
+    for (int g = t; g < G; g += nt) atomicAdd(&lstart[lev[g]], 1);
+    __syncthreads();
+    block_exclusive_scan(lstart, D + 1, scratch);
+    for (int g = t; g < G; g += nt) {
+        const int d = lev[g];
+        lorder[lstart[d] + atomicAdd(&aux[d], 1)] = g;
+    }
+    __syncthreads();
+    // apply the depths in order; a warp per group, a lane per pair
+    double2 *mom = reinterpret_cast<double2 *>(key);
+    for (int d = 0; d < D; ++d) {
+        const int q1 = lstart[d + 1];
+        for (int q = lstart[d] + warp; q < q1; q += nw) {
+            const int g = lorder[q];
+            const int k0 = gstart[g], k1 = gstart[g + 1];
+            const int o = body(go[g]);
+            const double4 xo = pm[o];
+            const double4 vo0 = vel[o];
+            const double rest_o = rest[o];
+            // momenta along r12 snapshotted for the whole group before any update
+            // (gregsys.hpp:740-742); the first 32 partners stay in registers
+            int i0 = 0;
+            double4 xi0 = make_double4(0, 0, 0, 0), vi0 = xi0;
+            double ri0 = 0.0;
+            for (int kb = k0; kb < k1; kb += 32) {
+                const int k = kb + lane;
+                if (k < k1) {
+                    const int i = body(si[k]);
+                    const double4 xi = pm[i], vi = vel[i];
+                    const double dd = sd[k];
+                    const double ux = (xi.x - xo.x) / dd, uy = (xi.y - xo.y) / dd, uz = (xi.z - xo.z) / dd;
+                    mom[k] = make_double2(axis_momentum(xo, vo0, ux, uy, uz), axis_momentum(xi, vi, ux, uy, uz));
+                    if (kb == k0) {
+                        i0 = i;
+                        xi0 = xi;
+                        vi0 = vi;
+                        ri0 = rest[i];
+                    }
+                }
+            }
+            __syncwarp();
+            double4 vo = vo0;
+            for (int kb = k0; kb < k1; kb += 32) {
+                const int k = kb + lane;
+                double d_o = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+                int hit = 0;
+                if (k < k1 && !(k > k0 && sd[k] == sd[k - 1])) {  // std::map keeps the first equal key
+                    int i = i0;
+                    double4 xi = xi0, vi = vi0;
+                    double ri = ri0;
+                    if (kb != k0) {
+                        i = body(si[k]);
+                        xi = pm[i];
+                        vi = vel[i];
+                        ri = rest[i];
+                    }
+                    if (pair_impulse(xo, rest_o, xi, ri, sd[k], mom[k], vi, d_o, ux, uy, uz)) {
+                        vel[i] = vi;
+                        hit = 1;
+                    }
+                }
+                // o's velocity takes the changes in candidate order, as the sequential loop adds them
+                const int m = min(32, k1 - kb);
+                for (int j = 0; j < m; ++j) {
+                    const int h = __shfl_sync(0xffffffffu, hit, j);
+                    const double a = __shfl_sync(0xffffffffu, d_o, j);
+                    const double bx = __shfl_sync(0xffffffffu, ux, j);
+                    const double by = __shfl_sync(0xffffffffu, uy, j);
+                    const double bz = __shfl_sync(0xffffffffu, uz, j);
+                    if (h) {
+                        vo.x += a * bx;
+                        vo.y += a * by;
+                        vo.z += a * bz;
+                    }
+                }
+            }
+            if (lane == 0) vel[o] = vo;
+            __syncwarp();
+        }
+        __syncthreads();
     }
 }
 
@@ -358,6 +700,8 @@ void release_collide(gtd_system *s) {
 static int ensure_coll(gtd_system *s) {
     const size_t need = sizeof(Cand) * kMaxCand + sizeof(double2) * kMaxCand + 256;
     if (s->coll_buf && s->coll_bytes >= need) return GTD_OK;
+    GTD_CUDA(cudaFuncSetAttribute(restitution_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)resolve_smem_bytes()));
     release_collide(s);
     GTD_CUDA(cudaMalloc(&s->coll_buf, need));
     s->coll_bytes = need;
@@ -434,11 +778,12 @@ int enqueue_collisions(gtd_system *s) {
     CollPtrs p = coll_ptrs(s);
     cudaStream_t st = s->stream;
     GTD_CUDA(cudaMemsetAsync(p.count, 0, 64, st));
-    overlap_pairs_kernel<<<(unsigned)((s->n + kCT - 1) / kCT), kCT, 0, st>>>(s->n, s->pm[s->cur], s->rad, p.cand,
-                                                                           p.count, kMaxCand);
+    const int64_t tiles = overlap_tiles(s->n);
+    overlap_pairs_kernel<<<(unsigned)(tiles * (tiles + 1) / 2), kDT, 0, st>>>(s->n, tiles, s->pm[s->cur], s->rad,
+                                                                            p.cand, p.count, kMaxCand);
     GTD_CHECK_LAUNCH();
-    restitution_kernel<<<1, 32, 0, st>>>(p.cand, p.count, kMaxCand, nullptr, s->pm[s->cur], s->rest, s->vel,
-                                         p.status);
+    restitution_kernel<<<1, kResolveThreads, resolve_smem_bytes(), st>>>(p.cand, p.count, kMaxCand, nullptr,
+                                                                         s->pm[s->cur], s->rest, s->vel, p.status);
     GTD_CHECK_LAUNCH();
     s->launches += 2;
     return GTD_OK;
@@ -488,8 +833,8 @@ int run_bh_collisions(gtd_system *s) {
                                               s->nskip, s->coll_nbox, s->pm[s->cur], s->rad, p.cand, p.count,
                                               kMaxCand);
     GTD_CHECK_LAUNCH();
-    restitution_kernel<<<1, 32, 0, st>>>(p.cand, p.count, kMaxCand, s->perm, s->pm[s->cur], s->rest, s->vel,
-                                         p.status);
+    restitution_kernel<<<1, kResolveThreads, resolve_smem_bytes(), st>>>(p.cand, p.count, kMaxCand, s->perm,
+                                                                         s->pm[s->cur], s->rest, s->vel, p.status);
     GTD_CHECK_LAUNCH();
     s->launches += 3;
     int host[2] = {0, 0};

@@ -9,6 +9,8 @@ These are inputs, not the hot path: they stand in for the reference drivers' gen
 * ``two_plummer``  - two equal spheres on a parabolic approach (Barnes-Hut workload).
 * ``ensemble``     - many independent few-body systems of uneven size with radii from a constant
                      density (batched collision workload).
+* ``comet_stage``  - the collapsing cloud of random_comet's evolve stage and the constants of its
+                     callbacks (callback-driven evolve workload).
 """
 from __future__ import annotations
 
@@ -96,3 +98,43 @@ def ensemble(n_systems: int, seed: int, n_min: int = 3, n_max: int = 2048, m_lo:
     x = _isotropic(rng, tot) * (u * r_ball)[:, None]
     v = rng.normal(0.0, sigma_v, (tot, 3))
     return off, m, r, np.ascontiguousarray(x), np.ascontiguousarray(v)
+
+
+def comet_stage(n: int, bounding_rad: float, b_rad: float, b_mass: float, n_exp: float, d_scale: float = 0.0,
+                min_cor: float = 0.5, max_cor: float = 1.0, dist_tol: float = 0.0, seed: int = 0) -> dict:
+    """The evolve stage of random_comet (gregsys.hpp:1881-1984): n bodies of radius b_rad and mass
+    b_mass at rest, uniform in a ball of radius bounding_rad (r = R cbrt(u), isotropic direction)
+    with any body closer than 2 b_rad to an earlier one redrawn (gregsys.hpp:1798-1836; numpy's
+    generator instead of mt19937_64), their mean position ``com``, and the callbacks' constants:
+    max_dist = cbrt(n v_b / (pi/6) * 3 / (4 pi)) with v_b the body volume; scale_factor =
+    d_scale^n_exp (d_scale <= 0: max_dist); max_dist *= 1 + dist_tol; min_max_cor = max_cor -
+    (max_cor - min_cor) max_dist^n_exp / (max_dist^n_exp + scale_factor); every body's rest =
+    max_cor - (max_cor - min_cor) d^n_exp / (d^n_exp + scale_factor), d its distance to com."""
+    rng = np.random.default_rng(seed)
+    x = np.empty((n, 3))
+    k = 0
+    while k < n:
+        r = bounding_rad * np.cbrt(rng.uniform(0.0, 1.0))
+        phi = rng.uniform(0.0, 2.0 * np.pi)
+        cth = 1.0 - 2.0 * rng.uniform(0.0, 1.0)
+        sth = np.sqrt(max(0.0, 1.0 - cth * cth))
+        p = np.array([r * sth * np.cos(phi), r * sth * np.sin(phi), r * cth])
+        if k and (np.sqrt(((x[:k] - p) ** 2).sum(axis=1)) < 2.0 * b_rad).any():
+            continue
+        x[k] = p
+        k += 1
+    com = x.mean(axis=0)
+    small_vol = 4.0 / 3.0 * np.pi * b_rad ** 3
+    max_dist = np.cbrt(small_vol * n / (np.pi / 6.0) * 3.0 / (4.0 * np.pi))
+    if d_scale <= 0:
+        d_scale = max_dist
+    scale_factor = d_scale ** n_exp
+    max_dist *= 1.0 + dist_tol
+    mde = max_dist ** n_exp
+    min_max_cor = max_cor - (max_cor - min_cor) * (mde / (mde + scale_factor))
+    de = np.sqrt(((x - com) ** 2).sum(axis=1)) ** n_exp
+    rest = max_cor - (max_cor - min_cor) * (de / (de + scale_factor))
+    return {"m": np.full(n, float(b_mass)), "x": x, "v": np.zeros((n, 3)), "r": np.full(n, float(b_rad)),
+            "rest": rest, "com": com, "scale_factor": float(scale_factor), "min_max_cor": float(min_max_cor),
+            "n_exp": float(n_exp), "min_cor": float(min_cor), "max_cor": float(max_cor)}
+

@@ -37,6 +37,37 @@ def test_restitution_vs_oracle_many_steps(gpu, oracle):
     assert np.abs(s.v - vo).max() / np.abs(vo).max() < 1e-9
 
 
+def _cluster(n, seed, rscale):
+    """Bodies in a 0.05 AU cube with radii of the order of their spacing times rscale."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-1.0, 1.0, (n, 3)) * 0.05 * AU
+    v = rng.normal(0.0, 3e3, (n, 3))
+    m = np.exp(rng.uniform(np.log(1e24), np.log(1e28), n))
+    r = rscale * 0.02 * AU * n ** (-1.0 / 3.0) * rng.uniform(0.5, 3.0, n)
+    rest = rng.uniform(0.3, 1.0, n)
+    return m, r, rest, x, v
+
+
+@pytest.mark.parametrize("n,rscale,pairs", [(500, 1.0, 354), (500, 2.0, 2534), (1200, 2.0, 7260)])
+def test_single_pass_vs_oracle(gpu, oracle, n, rscale, pairs):
+    """One s_coll pass on dense clusters: 354 and 2534 overlapping pairs (the one-CTA resolution,
+    depth-ordered groups) and 7260 (above its 4096-pair capacity: the sequential form), against
+    the oracle's restatement of gregsys.hpp:690-914.  An Euler step of dt = 1 s with masses of
+    1e-24 of the cluster's leaves gravity below the last bit of the velocities, so the state after
+    it is exactly s_coll(x + v, v); restitution only sees mass ratios."""
+    m, r, rest, x, v = _cluster(n, 7, rscale)
+    x1 = x + v
+    d = np.sqrt(((x1[:, None, :] - x1[None, :, :]) ** 2).sum(-1))
+    assert np.triu(r[:, None] + r[None, :] > d, 1).sum() == pairs
+    m = m * 1e-24
+    s = System(m, x, v, r=r, rest=rest, timestep=1.0, num_iterations=1, collisions=3)
+    s.evolve(System.euler)
+    assert np.array_equal(s.x, x1)
+    want = oracle.s_coll(m, r, rest, x1, v)
+    assert np.abs(want - v).max() > 1.0  # the pass changes velocities
+    assert np.abs(s.v - want).max() / np.abs(want).max() < 1e-13
+
+
 def test_check_overlap_raises_like_reference(gpu):
     m, x, v = plummer(50, 62)
     x[30] = x[7] + 10.0
