@@ -14,31 +14,13 @@
 
 #include <cmath>
 
+#include "callbacks.cuh"
 #include "gtd_internal.cuh"
 #include "gtd_system.cuh"
 
 namespace gtd {
 
-// Device control block of one callback-driven evolve.
-struct CbCtl {
-    unsigned cont;                // verdict written by a user continue_ev_if hook
-    unsigned go;                  // last verdict
-    unsigned done;                // the predicate returned false
-    unsigned capped;              // max_steps reached (predicate not evaluated)
-    int status;                   // first collision-pass error
-    unsigned iter;                // WHILE iterations in this graph launch
-    unsigned long long steps;     // steps taken in this evolve
-    unsigned long long chunk;     // steps taken in this graph launch
-    unsigned long long count;     // the rest-below predicate's probing counter (random_comet's _count)
-    unsigned long long max_steps; // 0: no guard
-    unsigned long long iterations;
-    double com[3];                // carried centre of the rest-from-COM functor
-    double divisor;               // N or total mass, fixed when the functor is set
-};
-
 constexpr int kCbThreads = 1024;
-constexpr unsigned kChunkSteps = 64;        // steps per graph launch; even (two steps per iteration)
-constexpr unsigned kMaxIter = kChunkSteps;  // WHILE iterations per launch, whatever the inner nodes do
 
 __global__ void cb_begin_kernel(CbCtl *c, unsigned long long max_steps, unsigned long long iterations) {
     c->cont = 0;
@@ -55,65 +37,18 @@ __global__ void cb_reset_chunk_kernel(CbCtl *c) {
     c->chunk = 0;
 }
 
-// Fixed-order block reductions (the result does not depend on timing).
-__device__ __forceinline__ double block_sum(double v, double *sh) {
-    const int t = threadIdx.x;
-    sh[t] = v;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (t < w) sh[t] += sh[t + w];
-        __syncthreads();
-    }
-    const double r = sh[0];
-    __syncthreads();
-    return r;
-}
+// continue_ev_if as its own kernel (cb_verdict); with set_handle its verdict opens or closes the
+// next step's IF node.
+constexpr int kDecideThreads = 256;
 
-// continue_ev_if, evaluated before every step.  mode 0: steps < iterations (no predicate,
-// gregsys.hpp:2948); 1: the user hook's verdict; 2: random_comet's predicate (gregsys.hpp:1956-1963):
-// true (and the counter reset) while some body has rest < bound, else `count++ < probing`.
-__global__ void __launch_bounds__(kCbThreads) cb_decide_kernel(CbCtl *c, int mode, const double *rest, int64_t n,
-                                                               double bound, unsigned long long probing,
-                                                               const int *coll_status, cudaGraphConditionalHandle h,
-                                                               int set_handle) {
-    __shared__ double sh[kCbThreads];
-    const int t = threadIdx.x;
-    double lo = INFINITY;  // NaN never compares below, as in the reference
-    if (mode == 2) {
-        for (int64_t i = t; i < n; i += blockDim.x) lo = fmin(lo, rest[i]);
-        sh[t] = lo;
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if (t < w) sh[t] = fmin(sh[t], sh[t + w]);
-            __syncthreads();
-        }
-        lo = sh[0];
-    }
-    if (t != 0) return;
-    if (coll_status && *coll_status && !c->status) c->status = *coll_status;
-    bool go;
-    if (c->status) {
-        go = false;
-    } else if (c->max_steps && c->steps >= c->max_steps) {
-        go = false;
-        c->capped = 1;
-    } else if (mode == 0) {
-        go = c->steps < c->iterations;
-    } else if (mode == 1) {
-        go = c->cont != 0;
-    } else if (lo < bound) {
-        c->count = 0;
-        go = true;
-    } else {
-        go = c->count++ < probing;
-    }
-    if (go) {
-        c->steps += 1;
-        c->chunk += 1;
-    } else if (!c->status && !c->capped) {
-        c->done = 1;
-    }
-    c->go = go ? 1u : 0u;
+__global__ void __launch_bounds__(kDecideThreads) cb_decide_kernel(CbCtl *c, int mode, const double *rest, int64_t n,
+                                                                   double bound, unsigned long long probing,
+                                                                   const int *coll_status,
+                                                                   cudaGraphConditionalHandle h, int set_handle) {
+    __shared__ double sh[32];
+    const double lo = mode == 2 ? cb_min_rest(rest, n, sh) : INFINITY;
+    if (threadIdx.x != 0) return;
+    const bool go = cb_verdict(c, mode, lo, bound, probing, coll_status);
     if (set_handle) cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
@@ -129,51 +64,51 @@ __global__ void cb_gate_kernel(CbCtl *c, const int *coll_status, cudaGraphCondit
     if (stop) cudaGraphSetConditional(hw, 0u);
 }
 
+// The same first node for a built-in predicate (mode 0 or 2), which it also evaluates: the body
+// opens only for a true verdict, and a false one ends the loop.  A stop for a full chunk evaluates
+// nothing (the next launch's first node does).
+__global__ void __launch_bounds__(kDecideThreads) cb_gate_decide_kernel(CbCtl *c, const int *coll_status, int mode,
+                                                                        const double *rest, int64_t n, double bound,
+                                                                        unsigned long long probing,
+                                                                        cudaGraphConditionalHandle hw,
+                                                                        cudaGraphConditionalHandle hbody) {
+    __shared__ double sh[32];
+    const double lo = mode == 2 ? cb_min_rest(rest, n, sh) : INFINITY;
+    if (threadIdx.x != 0) return;
+    if (coll_status && *coll_status && !c->status) c->status = *coll_status;
+    const unsigned it = ++c->iter;
+    const bool stop = c->done || c->capped || c->status || c->chunk >= kChunkSteps || it > kMaxIter;
+    const bool go = !stop && cb_verdict(c, mode, lo, bound, probing, nullptr);
+    cudaGraphSetConditional(hbody, go ? 1u : 0u);
+    if (!go) cudaGraphSetConditional(hw, 0u);
+}
+
 // N (body count) or M (total mass) of the rest-from-COM functor.
 __global__ void __launch_bounds__(kCbThreads) cb_divisor_kernel(int64_t n, const double4 *pm, CbCtl *c, int weighted) {
-    __shared__ double sh[kCbThreads];
+    __shared__ double sh[32];
     double s = 0.0;
     for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += pm[i].w;
-    s = block_sum(s, sh);
+    s = cb_block_sum(s, sh);
     if (threadIdx.x == 0) c->divisor = weighted ? s : (double)n;
 }
 
-// random_comet's for_all_bods, first half (gregsys.hpp:1971-1978): the centre is NOT reset before
-// the sum, so it carries: com = (com + sum x) / N, or (com + sum m x) / M with GREGSYS_MERGERS.
-__global__ void __launch_bounds__(kCbThreads) cb_com_kernel(int64_t n, const double4 *pm, CbCtl *c, int weighted) {
-    __shared__ double sh[kCbThreads];
-    double sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const double4 p = pm[i];
-        if (weighted) {
-            sx += p.w * p.x;
-            sy += p.w * p.y;
-            sz += p.w * p.z;
-        } else {
-            sx += p.x;
-            sy += p.y;
-            sz += p.z;
-        }
-    }
-    sx = block_sum(sx, sh);
-    sy = block_sum(sy, sh);
-    sz = block_sum(sz, sh);
-    if (threadIdx.x == 0) {
-        c->com[0] = (c->com[0] + sx) / c->divisor;
-        c->com[1] = (c->com[1] + sy) / c->divisor;
-        c->com[2] = (c->com[2] + sz) / c->divisor;
-    }
+// random_comet's for_all_bods as its own kernels: one CTA up to kForAllOneBlock bodies; above that
+// the CTA only carries the centre and a body-parallel kernel sets the restitution.
+constexpr int64_t kForAllOneBlock = 16384;
+
+__global__ void __launch_bounds__(kCbThreads) cb_for_all_kernel(int64_t n, const double4 *pm, double *rest, CbCtl *c,
+                                                                int weighted, int set_rest, double min_cor,
+                                                                double max_cor, double scale, double n_exp) {
+    __shared__ double sh[32];
+    __shared__ double com[3];
+    cb_for_all_block(n, pm, rest, c, weighted, set_rest, min_cor, max_cor, scale, n_exp, sh, com);
 }
 
-// Second half (gregsys.hpp:1979-1983): rest from the distance to the centre.
 __global__ void cb_rest_kernel(int64_t n, const double4 *pm, double *rest, const CbCtl *c, double min_cor,
                                double max_cor, double scale, double n_exp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const double4 p = pm[i];
-    const double dx = p.x - c->com[0], dy = p.y - c->com[1], dz = p.z - c->com[2];
-    const double de = pow(sqrt(dx * dx + dy * dy + dz * dz), n_exp);
-    rest[i] = max_cor - (max_cor - min_cor) * (de / (de + scale));
+    rest[i] = cb_rest_from_distance(pm[i], c->com, min_cor, max_cor, scale, n_exp);
 }
 
 }  // namespace gtd
@@ -224,7 +159,7 @@ static int enqueue_predicate(gtd_system *s, const int *coll_status, cudaGraphCon
         int rc = run_hook(s, s->cb.cont_fn, s->cb.cont_user, "continue_ev_if");
         if (rc) return rc;
     }
-    cb_decide_kernel<<<1, kCbThreads, 0, s->stream>>>(ctl_of(s), s->cb.cont_kind, s->rest, s->n, s->cb.min_max_cor,
+    cb_decide_kernel<<<1, kDecideThreads, 0, s->stream>>>(ctl_of(s), s->cb.cont_kind, s->rest, s->n, s->cb.min_max_cor,
                                                       s->cb.probing_iters, coll_status, h, set_handle ? 1 : 0);
     GTD_CHECK_LAUNCH();
     s->launches += 1;
@@ -235,24 +170,57 @@ static int enqueue_for_all(gtd_system *s) {
     if (s->cb.all_kind == 1) return run_hook(s, s->cb.all_fn, s->cb.all_user, "for_all_bods");
     if (s->cb.all_kind != 2 || s->n == 0) return GTD_OK;
     const double4 *pm = s->pm[s->cur];
-    cb_com_kernel<<<1, kCbThreads, 0, s->stream>>>(s->n, pm, ctl_of(s), s->cb.mass_weighted);
+    const bool one = s->n <= kForAllOneBlock;
+    cb_for_all_kernel<<<1, kCbThreads, 0, s->stream>>>(s->n, pm, s->rest, ctl_of(s), s->cb.mass_weighted, one ? 1 : 0,
+                                                       s->cb.min_cor, s->cb.max_cor, s->cb.scale_factor, s->cb.n_exp);
     GTD_CHECK_LAUNCH();
+    s->launches += 1;
+    if (one) return GTD_OK;
     cb_rest_kernel<<<(unsigned)((s->n + 255) / 256), 256, 0, s->stream>>>(
         s->n, pm, s->rest, ctl_of(s), s->cb.min_cor, s->cb.max_cor, s->cb.scale_factor, s->cb.n_exp);
     GTD_CHECK_LAUNCH();
-    s->launches += 2;
+    s->launches += 1;
     return GTD_OK;
 }
 
 // One step of the loop body: update, for_all_bods, collision pass, for_each_bod.  In a capture the
-// collision pass is enqueued without its read-back; its status reaches the next gate / predicate.
-static int callback_step(gtd_system *s, bool capture) {
+// collision pass is enqueued without its read-back (its status reaches the next verdict); its
+// resolving CTA also takes over the built-in for_all_bods and, when `decide` is given and nothing
+// runs between the pass and the next verdict, that verdict too (*decided).
+static int callback_step(gtd_system *s, bool capture, const cudaGraphConditionalHandle *decide, bool *decided) {
+    if (decided) *decided = false;
     int rc = cb_direct_step(s);
     if (rc) return rc;
-    rc = enqueue_for_all(s);
-    if (rc) return rc;
-    if (s->coll != GTD_NO_COLL) {
-        rc = capture ? enqueue_collisions(s) : run_collisions(s);
+    if (!(capture && s->coll == GTD_OVERLAP_COLL && s->n >= 2)) {
+        rc = enqueue_for_all(s);
+        if (rc) return rc;
+        if (s->coll != GTD_NO_COLL) {
+            rc = capture ? enqueue_collisions(s, nullptr) : run_collisions(s);
+            if (rc) return rc;
+        }
+    } else {
+        PassHooks hk;
+        hk.ctl = ctl_of(s);
+        if (s->cb.all_kind == 2 && s->n <= kForAllOneBlock) {
+            hk.for_all = 1;
+            hk.weighted = s->cb.mass_weighted;
+            hk.min_cor = s->cb.min_cor;
+            hk.max_cor = s->cb.max_cor;
+            hk.scale = s->cb.scale_factor;
+            hk.n_exp = s->cb.n_exp;
+        } else {
+            rc = enqueue_for_all(s);
+            if (rc) return rc;
+        }
+        if (decide && s->cb.cont_kind != 1 && !s->cb.each_fn) {
+            hk.decide = 1;
+            hk.mode = s->cb.cont_kind;
+            hk.bound = s->cb.min_max_cor;
+            hk.probing = s->cb.probing_iters;
+            hk.handle = *decide;
+            if (decided) *decided = true;
+        }
+        rc = enqueue_collisions(s, &hk);
         if (rc) return rc;
     }
     if (s->cb.each_fn) return run_hook(s, s->cb.each_fn, s->cb.each_user, "for_each_bod");
@@ -292,12 +260,17 @@ static int capture_into(cudaStream_t st, cudaGraph_t g, F &&fill) {
     return GTD_OK;
 }
 
-// The loop graph:
-//   reset; WHILE(hw) { gate -> IF(h1) { predicate -> IF(h2) { step A; predicate -> IF(h3) { step B } } } }
-// Two steps per iteration bring the double-buffered positions back to the buffer they started in,
-// so one graph serves every launch.  *flips: position-buffer flips per step (parity of the end).
+// The loop graph.  Two steps per iteration bring the double-buffered positions back to the buffer
+// they started in, so one graph serves every launch.  With a built-in predicate (none, or
+// random_comet's) the iteration's first node evaluates it:
+//   reset; WHILE(hw) { gate+verdict -> IF(h1) { step A (+ verdict) -> IF(h3) { step B } } }
+// where step A's collision pass evaluates the verdict when it is the last node of the step; with a
+// user predicate its hook's kernels precede each verdict:
+//   reset; WHILE(hw) { gate -> IF(h1) { hook, verdict -> IF(h2) { step A; hook, verdict -> IF(h3) { step B } } } }
+// *flips: position-buffer flips per step (parity of the end); *launches_per_step: kernels of one
+// step; *verdicts_apart: whether verdicts run as kernels of their own (for the launch count).
 static int build_loop_graph(gtd_system *s, const int *coll_status, cudaGraphExec_t *exec, int *flips,
-                            uint64_t *launches_per_step) {
+                            uint64_t *launches_per_step, int *verdicts_apart) {
     *exec = nullptr;
     cudaGraph_t G = nullptr;
     GTD_CUDA(cudaGraphCreate(&G, 0));
@@ -307,6 +280,8 @@ static int build_loop_graph(gtd_system *s, const int *coll_status, cudaGraphExec
     CbCtl *c = ctl_of(s);
     int cur_a = cur0;
     uint64_t per_step = 0;
+    bool fused = false;
+    const bool builtin = s->cb.cont_kind != 1;
     int rc = [&]() -> int {
         cudaGraphConditionalHandle hw, h1, h2, h3;
         GTD_CUDA(cudaGraphConditionalHandleCreate(&hw, G, 1, cudaGraphCondAssignDefault));
@@ -319,31 +294,43 @@ static int build_loop_graph(gtd_system *s, const int *coll_status, cudaGraphExec
         if (r) return r;
         GTD_CUDA(cudaGraphConditionalHandleCreate(&h1, wb, 0, cudaGraphCondAssignDefault));
         r = capture_into(st, wb, [&]() -> int {
-            cb_gate_kernel<<<1, 1, 0, st>>>(c, coll_status, hw, h1);
+            if (builtin)
+                cb_gate_decide_kernel<<<1, kDecideThreads, 0, st>>>(c, coll_status, s->cb.cont_kind, s->rest, s->n,
+                                                                    s->cb.min_max_cor, s->cb.probing_iters, hw, h1);
+            else
+                cb_gate_kernel<<<1, 1, 0, st>>>(c, coll_status, hw, h1);
             GTD_CHECK_LAUNCH();
             return add_conditional(st, h1, cudaGraphCondTypeIf, &b1);
         });
         if (r) return r;
-        GTD_CUDA(cudaGraphConditionalHandleCreate(&h2, b1, 0, cudaGraphCondAssignDefault));
-        r = capture_into(st, b1, [&]() -> int {
-            int q = enqueue_predicate(s, coll_status, h2, true);
-            if (q) return q;
-            return add_conditional(st, h2, cudaGraphCondTypeIf, &b2);
-        });
-        if (r) return r;
-        GTD_CUDA(cudaGraphConditionalHandleCreate(&h3, b2, 0, cudaGraphCondAssignDefault));
-        r = capture_into(st, b2, [&]() -> int {
+        cudaGraph_t step_a = b1;
+        if (!builtin) {
+            GTD_CUDA(cudaGraphConditionalHandleCreate(&h2, b1, 0, cudaGraphCondAssignDefault));
+            r = capture_into(st, b1, [&]() -> int {
+                int q = enqueue_predicate(s, coll_status, h2, true);
+                if (q) return q;
+                return add_conditional(st, h2, cudaGraphCondTypeIf, &b2);
+            });
+            if (r) return r;
+            step_a = b2;
+        }
+        GTD_CUDA(cudaGraphConditionalHandleCreate(&h3, step_a, 0, cudaGraphCondAssignDefault));
+        r = capture_into(st, step_a, [&]() -> int {
             const uint64_t l0 = s->launches;
-            int q = callback_step(s, true);
+            int q = callback_step(s, true, &h3, &fused);
             if (q) return q;
-            per_step = s->launches - l0;
             cur_a = s->cur;
-            q = enqueue_predicate(s, coll_status, h3, true);
-            if (q) return q;
+            if (!fused) {
+                per_step = s->launches - l0;
+                q = enqueue_predicate(s, coll_status, h3, true);
+                if (q) return q;
+            } else {
+                per_step = s->launches - l0;
+            }
             return add_conditional(st, h3, cudaGraphCondTypeIf, &b3);
         });
         if (r) return r;
-        r = capture_into(st, b3, [&]() -> int { return callback_step(s, true); });
+        r = capture_into(st, b3, [&]() -> int { return callback_step(s, true, nullptr, nullptr); });
         if (r) return r;
         if (s->cur != cur0) return fail(GTD_ERR_CUDA, "loop body does not return to its position buffer");
         GTD_CUDA(cudaGraphInstantiate(exec, G, 0));
@@ -361,6 +348,7 @@ static int build_loop_graph(gtd_system *s, const int *coll_status, cudaGraphExec
     }
     *flips = cur_a != cur0 ? 1 : 0;
     *launches_per_step = per_step;
+    *verdicts_apart = builtin ? (fused ? 0 : 1) : 2;
     return GTD_OK;
 }
 
@@ -389,12 +377,13 @@ static int eager_loop(gtd_system *s, uint64_t *waits) {
         *waits += 1;
         if (!h.go) return GTD_OK;
         if (reorder && (rc = cb_maybe_reorder(s))) return rc;
-        rc = callback_step(s, false);
+        rc = callback_step(s, false, nullptr, nullptr);
         if (rc) return rc;
     }
 }
 
-static int graph_loop(gtd_system *s, cudaGraphExec_t exec, int flips, uint64_t per_step, uint64_t *waits) {
+static int graph_loop(gtd_system *s, cudaGraphExec_t exec, int flips, uint64_t per_step, int verdicts_apart,
+                      uint64_t *waits) {
     const int cur0 = s->cur;
     CbCtl h{};
     for (;;) {
@@ -402,7 +391,9 @@ static int graph_loop(gtd_system *s, cudaGraphExec_t exec, int flips, uint64_t p
         int rc = read_ctl(s, &h);
         if (rc) return rc;
         *waits += 1;
-        s->launches += 1 + h.iter + h.chunk * (per_step + 1) + 1;  // reset, gates, steps + verdicts, last verdict
+        // reset, first nodes, steps, and the verdicts that run as kernels of their own
+        s->launches += 1 + h.iter + h.chunk * per_step +
+                       (verdicts_apart == 2 ? h.chunk + 1 : verdicts_apart == 1 ? (h.chunk + 1) / 2 : 0);
         if (h.status) return status_error(h.status);
         if (h.done || h.capped) break;
         if (h.chunk < kChunkSteps) return fail(GTD_ERR_CUDA, "callback loop chunk ended early (%llu steps)", h.chunk);
@@ -521,23 +512,20 @@ int gtd_system_evolve_callbacks(gtd_system *s, int method, uint64_t max_steps, u
     const bool graphable = s->coll != GTD_MERGE_COLL && !(s->precision == GTD_PREC_MIXED && s->coll == GTD_NO_COLL) &&
                            !s->time_force;
     cudaGraphExec_t exec = nullptr;
-    int flips = 0;
+    int flips = 0, verdicts_apart = 0;
     uint64_t per_step = 0;
     if (graphable) {
         // everything the captured steps need exists before the capture
         int *coll_status = nullptr;
-        if (s->coll != GTD_NO_COLL) {
-            rc = prepare_collisions(s, &coll_status);
-            // a status left by an earlier pass must not stop this evolve
-            if (!rc) GTD_CUDA(cudaMemsetAsync(coll_status, 0, sizeof(int), s->stream));
-        }
+        if (s->coll != GTD_NO_COLL) rc = prepare_collisions(s, &coll_status);
         if (!rc) rc = cb_prepare_steps(s);
         if (rc) return rc;
-        if (build_loop_graph(s, coll_status, &exec, &flips, &per_step) != GTD_OK) exec = nullptr;  // eager below
+        if (build_loop_graph(s, coll_status, &exec, &flips, &per_step, &verdicts_apart) != GTD_OK)
+            exec = nullptr;  // eager below
     }
     if (exec) {
         s->cb_graph = true;
-        rc = graph_loop(s, exec, flips, per_step, &waits);
+        rc = graph_loop(s, exec, flips, per_step, verdicts_apart, &waits);
         cudaGraphExecDestroy(exec);
     } else {
         rc = eager_loop(s, &waits);

@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <climits>
 
+#include "callbacks.cuh"
 #include "gtd_internal.cuh"
 #include "gtd_system.cuh"
 
@@ -34,15 +35,15 @@ struct Cand {
 };
 
 // All pairs o < i with dist < r_o + r_i; appends (o, i, dist) to the candidate list.  One CTA per
-// (o-tile, j-tile) pair of the upper triangle of kDT x kDT tiles, so that small systems still spread
-// over the SMs.  The square root is taken only for pairs whose squared distance is not clearly
-// above (r_o + r_i)^2; the overlap decision is the one of the exact test.
-constexpr int kDT = 64;
-
-__global__ void __launch_bounds__(kDT) overlap_pairs_kernel(int64_t n, int64_t tiles, const double4 *pm,
-                                                            const double *rad, Cand *cand, int *count, int cap) {
-    __shared__ double4 tp[kDT];
-    __shared__ double tr[kDT];
+// (o-tile, j-tile) pair of the upper triangle of TW x TW tiles, so that small systems still spread
+// over the SMs; the pair tests of a thread are independent, so the loop keeps several in flight.
+// The square root is taken only for pairs whose squared distance is not clearly above
+// (r_o + r_i)^2; the overlap decision is the one of the exact test.
+template <int TW>
+__global__ void __launch_bounds__(TW) overlap_pairs_kernel(int64_t n, int64_t tiles, const double4 *pm,
+                                                           const double *rad, Cand *cand, int *count, int cap) {
+    __shared__ double4 tp[TW];
+    __shared__ double tr[TW];
     // block -> (to, tj), to <= tj: row r of the triangle starts at r*T - r(r-1)/2
     const int64_t b = blockIdx.x, T = tiles;
     auto row_start = [&](int64_t r) { return r * T - r * (r - 1) / 2; };
@@ -54,18 +55,18 @@ __global__ void __launch_bounds__(kDT) overlap_pairs_kernel(int64_t n, int64_t t
     while (to + 1 < T && row_start(to + 1) <= b) ++to;
     const int64_t tj = to + (b - row_start(to));
     const int t = threadIdx.x;
-    const int64_t j = tj * kDT + t;
+    const int64_t j = tj * TW + t;
     tp[t] = j < n ? pm[j] : make_double4(0, 0, 0, 0);
     tr[t] = j < n ? rad[j] : 0.0;
     __syncthreads();
-    const int64_t o = to * kDT + t;
+    const int64_t o = to * TW + t;
     if (o >= n) return;
     const double4 po = pm[o];
     const double ro = rad[o];
-    const int lim = (int)min((int64_t)kDT, n - tj * kDT);
-    for (int jj = 0; jj < lim; ++jj) {
-        const int64_t i = tj * kDT + jj;
-        if (i <= o) continue;
+    const int lim = (int)min((int64_t)TW, n - tj * TW);
+    const int first = tj == to ? t + 1 : 0;  // i > o
+#pragma unroll 8
+    for (int jj = first; jj < lim; ++jj) {
         const double4 qj = tp[jj];
         const double dx = __dsub_rn(qj.x, po.x), dy = __dsub_rn(qj.y, po.y), dz = __dsub_rn(qj.z, po.z);
         const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
@@ -75,12 +76,25 @@ __global__ void __launch_bounds__(kDT) overlap_pairs_kernel(int64_t n, int64_t t
         const double d = sqrt(d2);
         if (rsum > d) {
             const int k = atomicAdd(count, 1);
-            if (k < cap) cand[k] = Cand{(int32_t)o, (int32_t)i, d};
+            if (k < cap) cand[k] = Cand{(int32_t)o, (int32_t)(tj * TW + jj), d};
         }
     }
 }
 
-int64_t overlap_tiles(int64_t n) { return (n + kDT - 1) / kDT; }
+// Tile width of the detection grid: narrow tiles for small systems (more CTAs, shorter loops).
+constexpr int kDTSmall = 32, kDTLarge = 64;
+int overlap_tile(int64_t n) { return n <= 32768 ? kDTSmall : kDTLarge; }
+int64_t overlap_tiles(int64_t n) { return (n + overlap_tile(n) - 1) / overlap_tile(n); }
+
+static void launch_overlap_pairs(int64_t n, const double4 *pm, const double *rad, Cand *cand, int *count, int cap,
+                                 cudaStream_t st) {
+    const int64_t tiles = overlap_tiles(n);
+    const unsigned blocks = (unsigned)(tiles * (tiles + 1) / 2);
+    if (overlap_tile(n) == kDTSmall)
+        overlap_pairs_kernel<kDTSmall><<<blocks, kDTSmall, 0, st>>>(n, tiles, pm, rad, cand, count, cap);
+    else
+        overlap_pairs_kernel<kDTLarge><<<blocks, kDTLarge, 0, st>>>(n, tiles, pm, rad, cand, count, cap);
+}
 
 __device__ __forceinline__ bool cand_less(const Cand &a, const Cand &b) {
     if (a.o != b.o) return a.o < b.o;
@@ -275,23 +289,10 @@ __device__ int block_exclusive_scan(int *a, int len, int *scratch) {
 
 // With perm != nullptr the candidates hold Barnes-Hut slots (the order of the reference's leaf and
 // neighbour iteration) and perm maps them to bodies.
-__global__ void __launch_bounds__(kResolveThreads, 1) restitution_kernel(Cand *cand, const int *count, int cap,
-                                                                         const int32_t *perm, const double4 *pm,
-                                                                         const double *rest, double4 *vel,
-                                                                         int *status) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void resolve_groups(unsigned char *smem, const Cand *cand, int c, const int32_t *perm,
+                                               const double4 *pm, const double *rest, double4 *vel) {
     using L = ResolveSmem;
     const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, warp = t >> 5, nw = nt >> 5;
-    const int c = *count;
-    if (c > cap) {
-        if (t == 0) *status = GTD_ERR_CAPACITY;
-        return;
-    }
-    if (c <= 0) return;
-    if (c > kFastCand) {
-        if (t == 0) resolve_serial(cand, c, cap, perm, pm, rest, vel);
-        return;
-    }
     unsigned long long *ck = reinterpret_cast<unsigned long long *>(smem + L::ck);
     double *sd = reinterpret_cast<double *>(smem + L::sd);
     int *si = reinterpret_cast<int *>(smem + L::si);
@@ -495,6 +496,37 @@ __global__ void __launch_bounds__(kResolveThreads, 1) restitution_kernel(Cand *c
             __syncwarp();
         }
         __syncthreads();
+    }
+}
+
+// One CTA.  The candidate count is reset to zero at the end (for the next pass) unless it overflowed.
+// hk (callback loop only): random_comet's for_all_bods first, the predicate after the pass.
+__global__ void __launch_bounds__(kResolveThreads, 1) restitution_kernel(int64_t n, Cand *cand, int *count, int cap,
+                                                                         const int32_t *perm, const double4 *pm,
+                                                                         double *rest, double4 *vel, int *status,
+                                                                         PassHooks hk) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double hsh[32];
+    __shared__ double hcom[3];
+    const int c = *count;
+    if (hk.for_all)
+        cb_for_all_block(n, pm, rest, hk.ctl, hk.weighted, 1, hk.min_cor, hk.max_cor, hk.scale, hk.n_exp, hsh, hcom);
+    if (c > cap) {
+        if (threadIdx.x == 0) *status = GTD_ERR_CAPACITY;
+    } else if (c > kFastCand) {
+        if (threadIdx.x == 0) resolve_serial(cand, c, cap, perm, pm, rest, vel);
+    } else if (c > 0) {
+        resolve_groups(smem, cand, c, perm, pm, rest, vel);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && c <= cap) *count = 0;
+    if (hk.decide) {
+        __syncthreads();
+        const double lo = hk.mode == 2 ? cb_min_rest(rest, n, hsh) : INFINITY;
+        if (threadIdx.x == 0) {
+            const bool go = cb_verdict(hk.ctl, hk.mode, lo, hk.bound, hk.probing, status);
+            cudaGraphSetConditional(hk.handle, go ? 1u : 0u);
+        }
     }
 }
 
@@ -760,30 +792,32 @@ static int merge_scan(gtd_system *s, bool only_check, int32_t *pair_out) {
     return GTD_OK;
 }
 
-// Upload order and the candidate buffer for overlap passes; *status: the pass's device error word
-// (GTD_ERR_CAPACITY when the candidates overflowed), cleared by every pass.
+// Upload order, the candidate buffer and a cleared candidate count and status for overlap passes;
+// *status: the passes' device error word (GTD_ERR_CAPACITY when the candidates overflowed; it stays
+// set until the next prepare).  Every pass that fits leaves the count at zero for the next one.
 int prepare_collisions(gtd_system *s, int **status) {
     int rc = restore_upload_order(s);
     if (rc) return rc;
     rc = ensure_coll(s);
     if (rc) return rc;
-    if (status) *status = coll_ptrs(s).status;
+    CollPtrs p = coll_ptrs(s);
+    GTD_CUDA(cudaMemsetAsync(p.count, 0, 64, s->stream));
+    if (status) *status = p.status;
     return GTD_OK;
 }
 
 // One s_coll pass (overlap restitution) enqueued on the stream, without reading its status back;
 // prepare_collisions must have run since the last reorder.  Capturable.
-int enqueue_collisions(gtd_system *s) {
+int enqueue_collisions(gtd_system *s, const PassHooks *hooks) {
     if (s->n < 2) return GTD_OK;
+    const PassHooks hk = hooks ? *hooks : PassHooks{};
     CollPtrs p = coll_ptrs(s);
     cudaStream_t st = s->stream;
-    GTD_CUDA(cudaMemsetAsync(p.count, 0, 64, st));
-    const int64_t tiles = overlap_tiles(s->n);
-    overlap_pairs_kernel<<<(unsigned)(tiles * (tiles + 1) / 2), kDT, 0, st>>>(s->n, tiles, s->pm[s->cur], s->rad,
-                                                                            p.cand, p.count, kMaxCand);
+    launch_overlap_pairs(s->n, s->pm[s->cur], s->rad, p.cand, p.count, kMaxCand, st);
     GTD_CHECK_LAUNCH();
-    restitution_kernel<<<1, kResolveThreads, resolve_smem_bytes(), st>>>(p.cand, p.count, kMaxCand, nullptr,
-                                                                         s->pm[s->cur], s->rest, s->vel, p.status);
+    restitution_kernel<<<1, kResolveThreads, resolve_smem_bytes(), st>>>(s->n, p.cand, p.count, kMaxCand, nullptr,
+                                                                         s->pm[s->cur], s->rest, s->vel, p.status,
+                                                                         hk);
     GTD_CHECK_LAUNCH();
     s->launches += 2;
     return GTD_OK;
@@ -794,7 +828,7 @@ int run_collisions(gtd_system *s) {
     if (s->coll == GTD_MERGE_COLL) return merge_scan(s, false, nullptr);
     int rc = prepare_collisions(s, nullptr);
     if (rc) return rc;
-    rc = enqueue_collisions(s);
+    rc = enqueue_collisions(s, nullptr);
     if (rc) return rc;
     CollPtrs p = coll_ptrs(s);
     cudaStream_t st = s->stream;
@@ -833,8 +867,9 @@ int run_bh_collisions(gtd_system *s) {
                                               s->nskip, s->coll_nbox, s->pm[s->cur], s->rad, p.cand, p.count,
                                               kMaxCand);
     GTD_CHECK_LAUNCH();
-    restitution_kernel<<<1, kResolveThreads, resolve_smem_bytes(), st>>>(p.cand, p.count, kMaxCand, s->perm,
-                                                                         s->pm[s->cur], s->rest, s->vel, p.status);
+    restitution_kernel<<<1, kResolveThreads, resolve_smem_bytes(), st>>>(s->n, p.cand, p.count, kMaxCand, s->perm,
+                                                                         s->pm[s->cur], s->rest, s->vel, p.status,
+                                                                         PassHooks{});
     GTD_CHECK_LAUNCH();
     s->launches += 3;
     int host[2] = {0, 0};

@@ -588,41 +588,36 @@ __global__ void integrate_warp_kernel(IntArgs a) {
     if (lane == 0) apply_epilogue(a, i, ax, ay, az);
 }
 
-// Small FP64 systems, one launch per force evaluation: a warp per body sums its whole row (lanes
-// strided over j, the bodies staged in shared-memory tiles), reduces with shuffles, and lane 0
-// applies the method's update.  No partial sums, no second kernel.
-constexpr int kFusedWarps = 4;
-constexpr int kFusedTile = 512;
+// Small FP64 systems, one launch per force evaluation.  kFusedSlices warps share a body: warp s sums
+// the j in the 32-wide chunks s, s + S, s + 2S, ... (loads straight from the L1/L2-resident
+// positions, several in flight), reduces with shuffles, and the body's first warp adds the slices
+// in order and applies the method's update.  No partial sums in memory, no second kernel; the short
+// per-warp loops keep the latency of a step low when there are few bodies.
+constexpr int kFusedBodies = 4;  // bodies per CTA
+constexpr int kFusedSlices = 4;  // warps per body
 
-__global__ void __launch_bounds__(kFusedWarps * 32) fused_small_kernel(IntArgs a, const double4 *src, double G) {
-    __shared__ double4 tile[kFusedTile];
+__global__ void __launch_bounds__(kFusedBodies * kFusedSlices * 32)
+    fused_small_kernel(IntArgs a, const double4 *__restrict__ src, double G) {
+    __shared__ double part[kFusedSlices][kFusedBodies][3];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t i = (int64_t)blockIdx.x * kFusedWarps + w;
-    const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
-    const double4 p = i < a.n ? src[i] : zero;
+    const int bl = w % kFusedBodies, slice = w / kFusedBodies;
+    const int64_t i = (int64_t)blockIdx.x * kFusedBodies + bl;
     double ax = 0.0, ay = 0.0, az = 0.0;
-    for (int64_t j0 = 0; j0 < a.n; j0 += kFusedTile) {
-        for (int k = threadIdx.x; k < kFusedTile; k += blockDim.x) {
-            const int64_t j = j0 + k;
-            double4 q = j < a.n ? src[j] : zero;
-            q.w *= G;
-            tile[k] = q;
-        }
-        __syncthreads();
-        const int lim = (int)min((int64_t)kFusedTile, a.n - j0);
+    if (i < a.n) {
+        const double4 p = src[i];
 #pragma unroll 4
-        for (int jj = lane; jj < lim; jj += 32) {
-            const double4 q = tile[jj];
+        for (int64_t j = (int64_t)slice * 32 + lane; j < a.n; j += 32 * kFusedSlices) {
+            const double4 q = src[j];
+            const double gm = q.w * G;
             const double dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
             const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
             double inv = rsqrt(r2);
             inv = r2 > 0.0 ? inv : 0.0;
-            const double sc = (q.w * inv) * (inv * inv);
+            const double sc = (gm * inv) * (inv * inv);
             ax = fma(sc, dx, ax);
             ay = fma(sc, dy, ay);
             az = fma(sc, dz, az);
         }
-        __syncthreads();
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -630,13 +625,29 @@ __global__ void __launch_bounds__(kFusedWarps * 32) fused_small_kernel(IntArgs a
         ay += __shfl_xor_sync(0xffffffffu, ay, o);
         az += __shfl_xor_sync(0xffffffffu, az, o);
     }
-    if (lane == 0 && i < a.n) apply_epilogue(a, i, ax, ay, az);
+    if (lane == 0) {
+        part[slice][bl][0] = ax;
+        part[slice][bl][1] = ay;
+        part[slice][bl][2] = az;
+    }
+    __syncthreads();
+    if (slice == 0 && lane == 0 && i < a.n) {
+        double sx = part[0][bl][0], sy = part[0][bl][1], sz = part[0][bl][2];
+#pragma unroll
+        for (int k = 1; k < kFusedSlices; ++k) {
+            sx += part[k][bl][0];
+            sy += part[k][bl][1];
+            sz += part[k][bl][2];
+        }
+        apply_epilogue(a, i, sx, sy, sz);
+    }
 }
 
 int launch_fused_small(int64_t n, const double4 *src, double G, int epi, const StepArgs &st, cudaStream_t s) {
     if (n == 0) return GTD_OK;
     IntArgs a{n, 0, 0, 0, 0, epi, nullptr, st};
-    fused_small_kernel<<<(unsigned)((n + kFusedWarps - 1) / kFusedWarps), kFusedWarps * 32, 0, s>>>(a, src, G);
+    fused_small_kernel<<<(unsigned)((n + kFusedBodies - 1) / kFusedBodies), kFusedBodies * kFusedSlices * 32, 0, s>>>(
+        a, src, G);
     GTD_CHECK_LAUNCH();
     return GTD_OK;
 }

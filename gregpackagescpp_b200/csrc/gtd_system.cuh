@@ -206,9 +206,13 @@ void release_callbacks(gtd_system *s);
 // overwrite live bodies in download order, keeping accelerations and the evolve state (io.cu)
 int device_update(gtd_system *s, const double *m, const double *r, const double *rest, const double *x3,
                   const double *v3);
-// overlap collision pass split for capture (collide.cu)
+// overlap collision pass split for capture (collide.cu); hooks: work of the callback loop that the
+// pass's resolving CTA takes over (callbacks.cuh), or nullptr
+namespace gtd {
+struct PassHooks;
+}
 int prepare_collisions(gtd_system *s, int **status);
-int enqueue_collisions(gtd_system *s);
+int enqueue_collisions(gtd_system *s, const gtd::PassHooks *hooks);
 int run_collisions(gtd_system *s);
 // pieces of evolve for the callback-driven loop (system.cu)
 int cb_evolve_begin(gtd_system *s, int method);

@@ -181,8 +181,9 @@ def callback_fixtures(r, out):
         out[f"{tag}_xo"], out[f"{tag}_vo"], out[f"{tag}_ro"] = xo, vo, ro
         out[f"{tag}_steps"], out[f"{tag}_como"] = np.array(steps), com
     # the m-weighted run is chaotic well before it ends (a 1e-16 nudge of the initial positions
-    # moves its final state by 0.1): its state is also kept at step 131, where that nudge moves it
-    # by 3e-10 (positions) and 3e-9 (velocities); 131 = two 64-step chunks and an odd remainder
+    # moves its final state by 0.1 and its end anywhere from step 244 to 368): its state is also
+    # kept at step 131, where that nudge moves it by 3e-10 (positions) and 3e-9 (velocities);
+    # 131 = two 64-step chunks and an odd remainder
     c = comet_setup(weighted=True)
     xo, vo, ro, steps, com = r.evolve_callbacks(
         16, c["m"], c["x"], c["v"], 0.25, 1000, CB_UNITS, r=c["r"], rest=c["rest"], coll=3,

@@ -10,9 +10,10 @@ to the largest coordinate, the FP64 bar.  The comet runs are chaotic, so their s
 against the reference's own sensitivity: perturbing its initial positions by 1e-16 (relative)
 moves its final state by 3e-8 / 4e-7 (positions / velocities) after the 183 steps of the
 equal-mass comet, checked here at 1e-5 / 1e-4, and by 3e-10 / 3e-9 after 131 steps of the
-m-weighted one, checked at 1e-7 / 1e-6; the m-weighted run to its end (263 steps), where that
-perturbation moves the state by 0.1, is checked by its step count and carried centre only.  The
-engine's per-step differences are FP64 rounding against the reference's long-double
+m-weighted one, checked at 1e-7 / 1e-6.  The equal-mass comet ends on step 183 under 24 such
+perturbations out of 24, so its end step is checked exactly; the m-weighted one ends anywhere from
+step 244 to 368 under them (263 unperturbed), so its full run is checked for an end in that range
+only.  The engine's per-step differences are FP64 rounding against the reference's long-double
 intermediates."""
 import ctypes as C
 import os
@@ -63,18 +64,21 @@ def _comet_system(g, tag, iterations=1000):
 @pytest.mark.parametrize("tag,weighted", [("cbk", False), ("cbw", True)])
 def test_comet_device_callbacks(gpu, golden, tag, weighted):
     """random_comet's evolve stage with both callbacks on the device: the loop runs as CUDA-graph
-    chunks (one host wait per 64 steps) and ends on the reference's step."""
+    chunks (one host wait per 64 steps) and ends where the reference's does (see the module
+    docstring for the m-weighted comet)."""
     g = golden
     mmc, sf = g[f"{tag}_par"]
     s = _comet_system(g, tag)
     fab = RestFromCom(0.5, 1.0, sf, 2.0, g[f"{tag}_com"], mass_weighted=weighted)
     s.evolve(System.leapfrog_kdk, WhileRestBelow(mmc, 20), None, fab, max_steps=3000)
-    assert s.steps_taken == int(g[f"{tag}_steps"])
     st = s.callback_stats()
     assert st["graph_loop"] and st["host_waits"] == s.steps_taken // 64 + 1
-    assert _rel(fab.com, g[f"{tag}_como"]) < 1e-9
     assert s.time_elapsed == 1000 * 0.25  # iterations * dt, whatever the steps (gregsys.hpp:3069)
-    if not weighted:
+    assert _rel(fab.com, g[f"{tag}_como"]) < 1e-9  # the carried centre follows the conserved mean
+    if weighted:
+        assert 244 <= s.steps_taken <= 368
+    else:
+        assert s.steps_taken == int(g[f"{tag}_steps"])
         assert _rel(s.x, g[f"{tag}_xo"]) < 1e-5
         assert _rel(s.v, g[f"{tag}_vo"]) < 1e-4
         assert _rel(s.rest, g[f"{tag}_ro"]) < 1e-5
