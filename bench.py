@@ -76,6 +76,9 @@ def parse_args():
     p.add_argument("--comet-steps", type=int, default=20000)
     p.add_argument("--comet-host-steps", type=int, default=200)
     p.add_argument("--comet-ref-steps", type=int, default=300)
+    p.add_argument("--comet-form", choices=["graph", "eager"], default="graph",
+                   help="eager: the device-callback loop with one launch per kernel and a host read of the "
+                        "verdict per step (the form ncu can profile kernel by kernel)")
     p.add_argument("--mixed-variant", type=int, default=-1,
                    help="use this mixed force-kernel variant instead of the autotuner's choice")
     return p.parse_args()
@@ -741,6 +744,9 @@ def run_comet(args, local):
     from gregpackagescpp_b200 import _lib
     K = args.comet_steps
     s = fresh()
+    if args.comet_form == "eager":  # force-kernel timing keeps the loop out of the conditional graph
+        s._push()
+        _lib.check(s._L.gtd_system_time_force_kernels(s._h, 1))
     fab = RestFromCom(0.5, 0.95, sf, 3.0, c["com"])
     s.evolve(16, WhileRestBelow(mmc, probing), None, fab, max_steps=max(args.warmup, 3) * 64)  # warm-up
     l0 = launches(s)
