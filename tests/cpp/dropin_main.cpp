@@ -125,6 +125,46 @@ int main() {
         std::printf(".nsys round trip: %d, size mismatch threw: %d\n", (int)same, (int)thrown);
         fails += !(same && thrown);
     }
+    {  // evolve callbacks: random_comet's for_all_bods as a host lambda (public body API) and as the
+       // device functor; a predicate true 7 times as a host lambda and as the device predicate
+        const auto ci = make(200, 23, 1.5e10);
+        const int n = (int)ci.size();
+        gtd::vector3D<double> mean{};
+        for (const bod &b : ci) mean += b.pos();
+        mean = gtd::vector3D<double>{mean.x / n, mean.y / n, mean.z / n};
+        const long double sf = 1e22L, min_cor = 0.5L, max_cor = 1.0L;
+        csys_t h{ci, 3600, 5, "M66743:66740,D1:1,T1:1", true};
+        gtd::vector3D<double> hcom = mean;
+        h.evolve(csys_t::leapfrog_kdk, nullptr, nullptr, [&](std::vector<csys_t::bod_t> &bs) {
+            for (const auto &b : bs) hcom += b.pos();
+            hcom = gtd::vector3D<double>{hcom.x / n, hcom.y / n, hcom.z / n};
+            for (auto &b : bs) {
+                const long double de = powl((b.pos() - hcom).magnitude(), 2.0L);
+                b.set_restitution(max_cor - (max_cor - min_cor) * (de / (de + sf)));
+            }
+        });
+        csys_t d{ci, 3600, 5, "M66743:66740,D1:1,T1:1", true};
+        gtd::vector3D<double> dcom = mean;
+        d.evolve(csys_t::leapfrog_kdk, nullptr, nullptr,
+                 gtd::device::rest_from_com<double>{min_cor, max_cor, sf, 2.0L, &dcom});
+        double err = 0, scale = 0, rerr = 0;
+        for (int i = 0; i < n; ++i) {
+            err = std::fmax(err, std::fabs(h[i].pos().x - d[i].pos().x) + std::fabs(h[i].vel().y - d[i].vel().y));
+            scale = std::fmax(scale, std::fabs(h[i].pos().x));
+            rerr = std::fmax(rerr, (double)std::fabs(h[i].restitution() - d[i].restitution()));
+        }
+        const double cerr = std::fabs(hcom.x - dcom.x) / std::fabs(hcom.x);
+        uint64_t k = 0;
+        csys_t p{ci, 3600, 100, "M66743:66740,D1:1,T1:1", true};
+        p.evolve(csys_t::leapfrog_kdk, [&]() { return k++ < 7; });
+        csys_t q{ci, 3600, 100, "M66743:66740,D1:1,T1:1", true};
+        q.evolve(csys_t::leapfrog_kdk, gtd::device::while_rest_below{0.0L, 7});
+        double perr = 0;
+        for (int i = 0; i < n; ++i) perr = std::fmax(perr, std::fabs(p[i].pos().z - q[i].pos().z));
+        std::printf("callbacks: host vs device %.3e (rest %.3e, centre %.3e), predicate %.3e\n", err / scale, rerr,
+                    cerr, perr / scale);
+        fails += !(err / scale < 1e-12 && rerr < 1e-12 && cerr < 1e-13 && perr == 0.0);
+    }
     std::printf(fails ? "FAIL\n" : "OK\n");
     return fails ? 1 : 0;
 }
