@@ -236,3 +236,39 @@ def test_barnes_hut_ignores_callbacks(gpu, golden):
     c.evolve(meth, lambda: False)
     for s in (b, c):
         assert np.array_equal(s.x, a.x) and np.array_equal(s.v, a.v)
+
+
+def _counting(k):
+    """A host predicate true for the first k evaluations."""
+    state = {"n": 0}
+
+    def cont():
+        state["n"] += 1
+        return state["n"] <= k
+    return cont
+
+
+@pytest.mark.parametrize("precision,coll,merge,graph", [("f64", 3, True, False), ("mixed", 0, False, False),
+                                                         ("mixed", 3, False, True)])
+def test_device_predicate_matches_host_predicate(gpu, precision, coll, merge, graph):
+    """The same loop driven by the device predicate and by a host callable is bit-identical: with
+    merging collisions (the eager form: the body count changes), with the mixed-precision path and
+    its periodic Morton reorder (eager form), and with mixed precision and overlap collisions (the
+    graph form)."""
+    from gregpackagescpp_b200.ics import AU, plummer
+    m, x, v = plummer(3000 if precision == "mixed" else 400, 66)
+    r = np.full(len(m), 0.03 * AU if merge else 0.02 * AU)
+    kw = dict(r=r, timestep=3600.0, num_iterations=1000, units_format=UNITS_G6674, collisions=coll,
+              merge_overlapping=merge, precision=precision)
+    a = System(m, x, v, **kw)
+    a.evolve(System.leapfrog_kdk, WhileRestBelow(0.0, 40))  # rest never below 0: exactly 40 steps
+    st = a.callback_stats()
+    assert a.steps_taken == 40 and st["graph_loop"] == graph
+    assert st["host_waits"] == (1 if graph else 41)
+    b = System(m, x, v, **kw)
+    b.evolve(System.leapfrog_kdk, _counting(40))
+    if merge:
+        assert len(a.m) < len(m)  # merges happened
+    assert len(a.m) == len(b.m)
+    for p, q in ((a.m, b.m), (a.x, b.x), (a.v, b.v)):
+        assert np.array_equal(p, q)
