@@ -9,6 +9,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -43,17 +44,21 @@ def build(verbose: bool = False, force: bool = False) -> str:
     nvcc = _nvcc()
     os.makedirs(OBJDIR, exist_ok=True)
     hdr_time = max((os.path.getmtime(h) for h in _headers()), default=0)
-    objs = []
+    objs, cmds = [], []
     for src in sources():
         obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
         if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
                 and os.path.getmtime(obj) >= hdr_time):
             continue
-        cmd = [nvcc, *ARCH, *NVFLAGS, "-dc" if False else "-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append([nvcc, *ARCH, *NVFLAGS, "-c", src, "-o", obj])
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd), flush=True)
+        for f in [pool.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC", *objs, "-o", LIB]
