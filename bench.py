@@ -66,6 +66,8 @@ def parse_args():
                    default="direct-mixed", help="direct-mixed is the headline; the others print their own line")
     p.add_argument("--bh-n", type=int, default=4194304)
     p.add_argument("--bh-cpu-n", type=int, default=10000)
+    p.add_argument("--bh-walk-variant", type=int, default=-1,
+                   help="node records of the float-tree walk: -1 default, 0 separate arrays, 1 interleaved")
     p.add_argument("--ens-systems", type=int, default=4096)
     p.add_argument("--ens-config", type=str, default="",
                    help="THREADS,BODIES_PER_THREAD for the ensemble kernel instead of the autotuner's choice")
@@ -540,6 +542,7 @@ def run_bh(args, local):
     check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, args.steps, 0.0, 0.5))
     check(L.gtd_system_upload(h, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
     check(L.gtd_bh_set_tree_float(h, 1))
+    check(L.gtd_bh_set_walk_variant(h, args.bh_walk_variant))
     # phase timing: build, walk
     import torch
     p = C.c_void_p()
@@ -580,7 +583,7 @@ def run_bh(args, local):
             "walk_interactions_per_s": inter / (walk_ms * 1e-3),
             "walk_flops_20_per_interaction_TFLOPs": 20 * inter / (walk_ms * 1e-3) / 1e12,
             "build_algorithmic_GBs": build_bytes / (build_ms * 1e-3) / 1e9,
-            "evolve_steps": args.steps, "evolve_s": ns.value * 1e-9,
+            "walk_variant": args.bh_walk_variant, "evolve_steps": args.steps, "evolve_s": ns.value * 1e-9,
             "steps_per_s": args.steps / (ns.value * 1e-9)}
     try:
         from gregpackagescpp_b200.ics import two_plummer as tp

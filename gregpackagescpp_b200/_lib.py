@@ -152,6 +152,7 @@ def load():
     L.gtd_system_autotune_direct.argtypes = [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.gtd_bh_build.argtypes = [vp, ip]
     L.gtd_bh_set_tree_float.argtypes = [vp, ip]
+    L.gtd_bh_set_walk_variant.argtypes = [vp, ip]
     L.gtd_bh_tree_size.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), dp]
     L.gtd_bh_tree_download.argtypes = [vp] + [dp] * 10
     L.gtd_bh_accelerations.argtypes = [vp, dp, dp]

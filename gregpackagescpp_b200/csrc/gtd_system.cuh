@@ -99,6 +99,8 @@ struct gtd_system {
     void *nwalk_a = nullptr;            // walk record: com xyz + G M (float4 / double4)
     int4 *nwalk_b = nullptr;            // walk record: skip, first, count | leaf<<31, width^2 bits
     double *nwalk_w2 = nullptr;         // width^2 for the FP64 walk
+    int walk_variant = -1;              // float walk records: -1 default (interleaved), 0 split, 1 interleaved
+    int walk_interleaved = 0;           // layout of the built float tree's records (1: A,B adjacent, 32 B)
     int32_t *depth_list = nullptr;      // internal nodes grouped by depth
     uint32_t *depth_off = nullptr;      // [22] offsets + [22] cursors
     double box[6] = {0, 0, 0, 0, 0, 0};

@@ -479,6 +479,7 @@ class System:
     def bh_build(self, tree_float: bool = True) -> None:
         """bh_tree::add_bodies + calc_com (greg8tree.hpp:1062-1078) on the device."""
         self._push()
+        check(self._L.gtd_bh_set_walk_variant(self._h, getattr(self, "_walk_variant", -1)))
         check(self._L.gtd_bh_build(self._h, 1 if tree_float else 0))
 
     def bh_tree(self) -> dict:
@@ -505,6 +506,13 @@ class System:
         cnt = np.zeros(len(self.m), np.uint32)
         check(self._L.gtd_bh_accelerations(self._h, ptr(a), ptr(cnt)))
         return a, cnt
+
+    def set_bh_walk_variant(self, variant: int) -> None:
+        """Node-record layout of the float-tree walk (-1 default, 0 separate arrays, 1 interleaved
+        32-byte records); both take the same interactions in the same order."""
+        if variant < -1 or variant > 1:
+            raise ValueError(f"walk variant {variant} out of range")
+        self._walk_variant = int(variant)
 
     def bh_tree_float(self, tree_float: bool) -> None:
         """Selects T=float (True, the default) or T=double geometry for the Barnes-Hut evolve."""
