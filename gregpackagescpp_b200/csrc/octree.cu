@@ -89,18 +89,27 @@ __global__ void bbox_partial_kernel(const double4 *pm, int64_t n, double *part) 
     if (t < 6) part[(size_t)blockIdx.x * 6 + t] = red[t][0];
 }
 
-// One thread: the reference's arithmetic for the cube, greg8tree.hpp:1037-1046, in T.
+// One warp folds the block partials (min and max are exact, so the lane split does not change the
+// result); then one thread does the reference's arithmetic for the cube, greg8tree.hpp:1037-1046, in T.
 template <bool F>
 __global__ void bbox_final_kernel(const double *part, int blocks, double *box, int *status) {
     using TT = TreeT<F>;
     using T = typename TT::T;
-    if (threadIdx.x != 0) return;
+    const int lane = threadIdx.x & 31;
     double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (int b = 0; b < blocks; ++b)
+    for (int b = lane; b < blocks; b += 32)
         for (int k = 0; k < 3; ++k) {
             mn[k] = fmin(mn[k], part[b * 6 + k]);
             mx[k] = fmax(mx[k], part[b * 6 + 3 + k]);
         }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fmin(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+        }
+    if (threadIdx.x != 0) return;
     const T xr = TT::sub((T)mx[0], (T)mn[0]), yr = TT::sub((T)mx[1], (T)mn[1]), zr = TT::sub((T)mx[2], (T)mn[2]);
     T edge = xr > yr ? (xr > zr ? xr : zr) : (yr > zr ? yr : zr);
     // pad = edge / 20.0l: the long-double quotient rounded to T equals the correctly rounded T
@@ -231,7 +240,6 @@ struct EmitArgs {
     int32_t *first, *count, *skip, *own;
     double4 *com;
     double *width;
-    uint32_t *depth_hist;  // [21] internal nodes per depth
 };
 
 template <bool F>
@@ -265,7 +273,6 @@ __global__ void emit_kernel(EmitArgs e) {
         e.count[node] = (int32_t)(last - a + 1);
         e.skip[node] = (int32_t)e.node_start[last + 1];
         e.width[node] = cell_width<F>(ca, d, e.box);
-        atomicAdd(&e.depth_hist[d], 1u);
     }
     if (lm < kMaxDepth) {
         const int64_t last = la == kMaxDepth ? range_end(e.codes, e.n, a, kMaxDepth) : a;
@@ -310,12 +317,55 @@ __global__ void depth_offsets_kernel(uint32_t *depth_off) {
     depth_off[kMaxDepth] = run;
 }
 
-__global__ void depth_scatter_kernel(const int8_t *depth, const int8_t *leaf, int64_t n_nodes, uint32_t *depth_off,
-                                     int32_t *list) {
-    const int64_t nd = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (nd >= n_nodes || leaf[nd]) return;
-    const uint32_t pos = atomicAdd(&depth_off[22 + depth[nd]], 1u);
-    list[pos] = (int32_t)nd;
+// Internal nodes per depth.  Each CTA counts a chunk of kDepthChunk nodes in shared memory and adds
+// its counts with one global atomic per depth: a global atomic per node would serialise ~N atomics
+// on 21 addresses (about 1 ms at N = 4194304).
+constexpr int kDepthChunk = 16 * kTT;
+
+__global__ void __launch_bounds__(kTT) depth_count_kernel(const int8_t *depth, const int8_t *leaf, int64_t n_nodes,
+                                                          uint32_t *depth_off) {
+    __shared__ uint32_t cnt[kMaxDepth];
+    const int t = threadIdx.x;
+    if (t < kMaxDepth) cnt[t] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kDepthChunk;
+    for (int k = 0; k < kDepthChunk / kTT; ++k) {
+        const int64_t nd = base + (int64_t)k * kTT + t;
+        if (nd < n_nodes && !leaf[nd]) atomicAdd(&cnt[depth[nd]], 1u);
+    }
+    __syncthreads();
+    if (t < kMaxDepth && cnt[t]) atomicAdd(&depth_off[t], cnt[t]);
+}
+
+// Lists the internal nodes by depth (the order inside a depth is free: each node's moments are
+// computed from its own children alone).  A CTA ranks its chunk's nodes per depth in shared memory
+// and reserves one range per depth with a single global atomic.
+__global__ void __launch_bounds__(kTT) depth_scatter_kernel(const int8_t *depth, const int8_t *leaf, int64_t n_nodes,
+                                                            uint32_t *depth_off, int32_t *list) {
+    constexpr int kItems = kDepthChunk / kTT;
+    __shared__ uint32_t cnt[kMaxDepth], start[kMaxDepth];
+    const int t = threadIdx.x;
+    if (t < kMaxDepth) cnt[t] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kDepthChunk;
+    int8_t d[kItems];
+    uint32_t r[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const int64_t nd = base + (int64_t)k * kTT + t;
+        d[k] = -1;
+        r[k] = 0;
+        if (nd < n_nodes && !leaf[nd]) {
+            d[k] = depth[nd];
+            r[k] = atomicAdd(&cnt[d[k]], 1u);
+        }
+    }
+    __syncthreads();
+    if (t < kMaxDepth && cnt[t]) start[t] = atomicAdd(&depth_off[22 + t], cnt[t]);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kItems; ++k)
+        if (d[k] >= 0) list[start[d[k]] + r[k]] = (int32_t)(base + (int64_t)k * kTT + t);
 }
 
 // Internal nodes of one depth: FP64 moments of the children in octant order.
@@ -716,14 +766,16 @@ static int bh_build_impl(gtd_system *s, int tree_float) {
     if (rc) return rc;
     GTD_CUDA(cudaMemsetAsync(s->depth_off, 0, 64 * sizeof(uint32_t), st));
     EmitArgs e{n, s->codes, s->perm, s->lcp, s->node_start, pm, s->box_dev, s->ndepth, s->nleaf, s->nfirst,
-               s->ncount, s->nskip, s->own_leaf, s->ncom, s->nwidth, s->depth_off};
+               s->ncount, s->nskip, s->own_leaf, s->ncom, s->nwidth};
     if (tree_float) emit_kernel<true><<<blocks_for(n), kTT, 0, st>>>(e);
     else emit_kernel<false><<<blocks_for(n), kTT, 0, st>>>(e);
     GTD_CHECK_LAUNCH();
+    const unsigned depth_blocks = (unsigned)((nodes + kDepthChunk - 1) / kDepthChunk);
+    depth_count_kernel<<<depth_blocks, kTT, 0, st>>>(s->ndepth, s->nleaf, nodes, s->depth_off);
     depth_offsets_kernel<<<1, 32, 0, st>>>(s->depth_off);
-    depth_scatter_kernel<<<blocks_for(nodes), kTT, 0, st>>>(s->ndepth, s->nleaf, nodes, s->depth_off, s->depth_list);
+    depth_scatter_kernel<<<depth_blocks, kTT, 0, st>>>(s->ndepth, s->nleaf, nodes, s->depth_off, s->depth_list);
     GTD_CHECK_LAUNCH();
-    s->launches += 3;
+    s->launches += 4;
     for (int d = kMaxDepth - 1; d >= 0; --d) {
         com_level_kernel<<<4 * 148, kTT, 0, st>>>(s->depth_list, s->depth_off, d, s->nskip, s->ncom);
         s->launches += 1;
