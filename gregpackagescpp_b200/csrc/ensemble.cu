@@ -78,6 +78,16 @@ __device__ __forceinline__ float ens_rsqrt(float x) {
     return y;
 }
 
+// Smallest r2 floor that keeps the self pair's G m / r^3 finite in FP32 for every body of a system
+// whose largest G m is Gm: floor^(3/2) >= Gm * 2^-120, and at least 2^-100 (a normal float whose
+// 1/r^2 = 2^100 stays finite).  For G m = 6.7e20 (1e31 kg, SI) that is 6.3e-11 m^2: it changes r2
+// only for pairs closer than ~5 cm, far inside the FP32 resolution of the staged coordinates.
+__device__ __forceinline__ float ens_r2_floor(float Gm) {
+    const double c = cbrt((double)Gm * 0x1p-120);
+    const double f = c * c;
+    return f > 0x1p-100 ? (float)f : 0x1p-100f;
+}
+
 __device__ void ens_merge_into(double4 &po, double4 &vo, double4 &ao, double &ro, double &eo, const double4 &pi,
                                const double4 &vi, const double4 &ai, double ri, double ei) {
     const double ma = po.w, mb = pi.w, ms = __dadd_rn(ma, mb);
@@ -159,10 +169,14 @@ __device__ int ens_merge_scan(int n, double4 *pos, double4 *vel, double4 *acc, d
 
 // Forces on the IB bodies i0, i0 + T, ... (those below nc) of a staged system: each staged j pair is
 // read from shared memory once for all IB bodies.  Returns whether any of them may overlap another.
+// floor2 is added to every r2 inside its first FMA (no extra instruction): the self pair gets
+// r2 = floor2 exactly, a finite 1/r and a zero term (dx = 0), and the overlap minimum skips it by
+// its bit pattern.  floor2 is far below the staged coordinates' resolution (ens_r2_floor).
 template <int IB>
 __device__ __forceinline__ int ens_force_rows(int i0, int T, int nc, int npad, const float *sx, const float *sy,
                                               const float *sz, const float *sm, double4 *pos, double4 *vel,
-                                              double4 *acc, const double *rad, float rmx, bool kick, double h2) {
+                                              double4 *acc, const double *rad, float rmx, bool kick, double h2,
+                                              float floor2) {
     const float2 *X2 = reinterpret_cast<const float2 *>(sx);
     const float2 *Y2 = reinterpret_cast<const float2 *>(sy);
     const float2 *Z2 = reinterpret_cast<const float2 *>(sz);
@@ -178,8 +192,10 @@ __device__ __forceinline__ int ens_force_rows(int i0, int T, int nc, int npad, c
         ny[b] = make_float2(-sy[ic], -sy[ic]);
         nz[b] = make_float2(-sz[ic], -sz[ic]);
         ax[b] = ay[b] = az[b] = 0.0;
-        mnr[b] = 0xffffffffu;  // min over j != i of r2 bits, the self pair (r2 = 0) excluded
+        mnr[b] = 0xffffffffu;  // min over j != i of r2 bits, the self pair (r2 = floor2) excluded
     }
+    const float2 fl2 = make_float2(floor2, floor2);
+    const unsigned fbits = (unsigned)__float_as_int(floor2) + 1u;
     for (int q0 = 0; q0 < npad / 2; q0 += kEnsFold / 2) {
         const int q1 = min(q0 + kEnsFold / 2, npad / 2);
         float2 fx[IB], fy[IB], fz[IB];
@@ -191,13 +207,12 @@ __device__ __forceinline__ int ens_force_rows(int i0, int T, int nc, int npad, c
 #pragma unroll
             for (int b = 0; b < IB; ++b) {
                 const float2 dx = __fadd2_rn(X, nx[b]), dy = __fadd2_rn(Y, ny[b]), dz = __fadd2_rn(Z, nz[b]);
-                float2 r2 = __fmul2_rn(dx, dx);
+                float2 r2 = __ffma2_rn(dx, dx, fl2);
                 r2 = __ffma2_rn(dy, dy, r2);
                 r2 = __ffma2_rn(dz, dz, r2);
-                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.x) - 1u);
-                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.y) - 1u);
-                // the self pair has r2 == 0: clamping to 1 mm^2 makes its term exactly 0
-                const float2 inv = make_float2(ens_rsqrt(fmaxf(r2.x, 1e-6f)), ens_rsqrt(fmaxf(r2.y, 1e-6f)));
+                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.x) - fbits);
+                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.y) - fbits);
+                const float2 inv = make_float2(ens_rsqrt(r2.x), ens_rsqrt(r2.y));
                 const float2 inv2 = __fmul2_rn(inv, inv);
                 float2 sc = __fmul2_rn(M, inv);
                 sc = __fmul2_rn(sc, inv2);
@@ -219,7 +234,7 @@ __device__ __forceinline__ int ens_force_rows(int i0, int T, int nc, int npad, c
         const int i = i0 + b * T;
         if (i >= nc) continue;
         if (mnr[b] != 0xffffffffu) {  // some other body exists
-            const float mind2 = __int_as_float((int)(mnr[b] + 1u));
+            const float mind2 = __int_as_float((int)(mnr[b] + fbits));
             const float reach = (float)rad[i] + rmx;
             if (mind2 < reach * reach * 1.0001f) flagged = 1;
         }
@@ -244,9 +259,9 @@ __global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsA
     float *sm = sz + a.stride;
     __shared__ double red[3][32];
     __shared__ double cen[3];
-    __shared__ float redr[32];
+    __shared__ float redr[32], redg[32];
     __shared__ int sh[8];
-    __shared__ float rmax_s;
+    __shared__ float rmax_s, floor_s;
     const int t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5, nw = (T + 31) >> 5;
     const double h = a.h, h2 = 0.5 * a.h;
     while (true) {
@@ -266,7 +281,7 @@ __global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsA
         for (int pass = 0; pass < 2; ++pass) {
             const bool first = pass == 0;
             double cx = 0.0, cy = 0.0, cz = 0.0;
-            float rmax = 0.f;
+            float rmax = 0.f, gmax = 0.f;
             for (int i = t; i < nc; i += T) {
                 double4 p = pos[i];
                 if (a.kdk && first) {
@@ -279,6 +294,7 @@ __global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsA
                 }
                 cx += p.x; cy += p.y; cz += p.z;
                 rmax = fmaxf(rmax, (float)rad[i]);
+                gmax = fmaxf(gmax, (float)(a.G * p.w));
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -286,22 +302,29 @@ __global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsA
                 cy += __shfl_xor_sync(0xffffffffu, cy, o);
                 cz += __shfl_xor_sync(0xffffffffu, cz, o);
                 rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+                gmax = fmaxf(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
             }
             if (lane == 0) {
                 red[0][warp] = cx; red[1][warp] = cy; red[2][warp] = cz;
                 redr[warp] = rmax;
+                redg[warp] = gmax;
             }
             __syncthreads();
             if (t == 0) {
                 double X = 0, Y = 0, Z = 0;
-                float R = 0.f;
-                for (int w = 0; w < nw; ++w) { X += red[0][w]; Y += red[1][w]; Z += red[2][w]; R = fmaxf(R, redr[w]); }
+                float R = 0.f, Gm = 0.f;
+                for (int w = 0; w < nw; ++w) {
+                    X += red[0][w]; Y += red[1][w]; Z += red[2][w];
+                    R = fmaxf(R, redr[w]);
+                    Gm = fmaxf(Gm, redg[w]);
+                }
                 cen[0] = X / nc; cen[1] = Y / nc; cen[2] = Z / nc;
                 rmax_s = R;
+                floor_s = ens_r2_floor(Gm);
             }
             __syncthreads();
             const double mx = cen[0], my = cen[1], mz = cen[2];
-            const float rmx = rmax_s;
+            const float rmx = rmax_s, floor2 = floor_s;
             // stage the system: FP32 relative positions and G m (pad to an even count, far and massless)
             const int npad = (nc + 1) & ~1;
             for (int i = t; i < npad; i += T) {
@@ -317,7 +340,7 @@ __global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsA
             int flagged = 0;
             for (int i0 = t; i0 < nc; i0 += IB * T)
                 flagged |= ens_force_rows<IB>(i0, T, nc, npad, sx, sy, sz, sm, pos, vel, acc, rad, rmx, a.kdk && first,
-                                              h2);
+                                              h2, floor2);
             flagged = __syncthreads_or(flagged);
             if (!first || !flagged || !a.merge) break;
             const int nn = ens_merge_scan(nc, pos, vel, acc, rad, a.rest + b0, a.ids + b0, sh);

@@ -109,49 +109,106 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const unsigned
     hist[(size_t)threadIdx.x * blocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Stable scatter: each block walks its chunk in rounds of 256 keys in order; within a round,
-// equal digits are ranked by lane (match_any) and by warp (per-warp digit counts).
+// Stable scatter.  A block takes its chunk in two halves of kHalf keys.  For each half it counts the
+// digits, ranks every key stably inside its digit (rounds of 256 keys in index order; within a round
+// by lane (match_any) and warp), places the keys digit-sorted in shared memory, and then writes them
+// out in that order: keys of one digit go to consecutive addresses, so the stores fill whole sectors
+// instead of one 8-byte store per key.
+constexpr int kHalfItems = kSortItems / 2;
+constexpr int kHalf = kSortThreads * kHalfItems;
+
 __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsigned long long *keys_in,
                                                                      const int32_t *vals_in,
                                                                      unsigned long long *keys_out,
                                                                      int32_t *vals_out, int64_t n, int shift,
                                                                      const uint32_t *offsets, int blocks) {
     constexpr int kWarps = kSortThreads / 32;
+    __shared__ unsigned long long sk[kHalf];
+    __shared__ int32_t sv[kHalf];
     __shared__ uint32_t wcnt[kWarps][256];
-    __shared__ uint32_t run[256];
+    __shared__ uint32_t cnt[256], pre[256], run_local[256], run_global[256], wsum[kWarps];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    run[t] = offsets[(size_t)t * blocks + blockIdx.x];
-    const int64_t base = (int64_t)blockIdx.x * kChunk;
     const unsigned lt = (1u << lane) - 1u;
-    for (int k = 0; k < kSortItems; ++k) {
+    run_global[t] = offsets[(size_t)t * blocks + blockIdx.x];
+    const int64_t base = (int64_t)blockIdx.x * kChunk;
+    for (int h = 0; h < 2; ++h) {
+        const int64_t hbase = base + (int64_t)h * kHalf;
+        unsigned long long key[kHalfItems];
+        int32_t val[kHalfItems];
+        uint32_t dig[kHalfItems];
+        cnt[t] = 0;
+        __syncthreads();
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) wcnt[w][t] = 0;
-        __syncthreads();
-        const int64_t i = base + (int64_t)k * kSortThreads + t;
-        const bool valid = i < n;
-        unsigned long long key = 0;
-        int32_t val = 0;
-        uint32_t d = 256;  // invalid lanes get a digit no key has
-        if (valid) {
-            key = keys_in[i];
-            val = vals_in[i];
-            d = (uint32_t)((key >> shift) & 0xffu);
-        }
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        const unsigned rank = __popc(peers & lt);
-        if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
-        __syncthreads();
-        if (valid) {
-            uint32_t pos = run[d] + rank;
-            for (int w = 0; w < warp; ++w) pos += wcnt[w][d];
-            keys_out[pos] = key;
-            vals_out[pos] = val;
+        for (int k = 0; k < kHalfItems; ++k) {
+            const int64_t i = hbase + (int64_t)k * kSortThreads + t;
+            key[k] = 0;
+            val[k] = 0;
+            dig[k] = 256;  // absent keys get a digit no key has
+            if (i < n) {
+                key[k] = keys_in[i];
+                val[k] = vals_in[i];
+                dig[k] = (uint32_t)((key[k] >> shift) & 0xffu);
+                atomicAdd(&cnt[dig[k]], 1u);
+            }
         }
         __syncthreads();
-        uint32_t tot = 0;
+        // exclusive scan of the half's digit counts, one digit per thread
+        const uint32_t c = cnt[t];
+        uint32_t incl = c;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) tot += wcnt[w][t];
-        run[t] += tot;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t wofs = 0;
+        for (int w = 0; w < warp; ++w) wofs += wsum[w];
+        pre[t] = wofs + incl - c;
+        run_local[t] = wofs + incl - c;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kHalfItems; ++k) {
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) wcnt[w][t] = 0;
+            __syncthreads();
+            const uint32_t d = dig[k];
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const unsigned rank = __popc(peers & lt);
+            if (d < 256 && rank == 0) wcnt[warp][d] = __popc(peers);
+            __syncthreads();
+            if (d < 256) {
+                uint32_t pos = run_local[d] + rank;
+                for (int w = 0; w < warp; ++w) pos += wcnt[w][d];
+                if (pos < (uint32_t)kHalf) {
+                    sk[pos] = key[k];
+                    sv[pos] = val[k];
+                }
+            }
+            __syncthreads();
+            uint32_t tot = 0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) tot += wcnt[w][t];
+            run_local[t] += tot;
+            __syncthreads();
+        }
+        const int64_t rem = n - hbase;
+        const int hcount = rem <= 0 ? 0 : (rem < kHalf ? (int)rem : kHalf);
+#pragma unroll
+        for (int k = 0; k < kHalfItems; ++k) {
+            const int i = k * kSortThreads + t;
+            if (i < hcount) {
+                const unsigned long long kk = sk[i];
+                const uint32_t d = (uint32_t)((kk >> shift) & 0xffu);
+                const uint32_t g = run_global[d] + (uint32_t)i - pre[d];
+                if ((int64_t)g < n) {
+                    keys_out[g] = kk;
+                    vals_out[g] = sv[i];
+                }
+            }
+        }
+        __syncthreads();
+        run_global[t] += c;
         __syncthreads();
     }
 }
