@@ -612,7 +612,9 @@ def run_ensemble(args, local):
         e.set_bodies_per_thread(ib)
     else:
         threads, tune_ms = e.autotune()
-    e.evolve(args.warmup)
+    # at least one 16-step chunk in the warm-up, so that the step graph is captured and instantiated
+    # before the timed region
+    e.evolve(max(args.warmup, 16))
     counts0, merges0, l0 = e.counts()
     K = max(args.steps, 16)
     ns = e.evolve(K)
