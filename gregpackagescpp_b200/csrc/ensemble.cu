@@ -682,7 +682,7 @@ int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
         const int c = cf[0];
         e->threads = c;
         e->ib = cf[1];
-        for (int rep = 0; rep < 3 && !rc; ++rep) {
+        for (int rep = 0; rep < 6 && !rc; ++rep) {  // the first launch is not counted; min of five
             if ((rc = cudaEventRecord(e->ev0, e->stream) ? GTD_ERR_CUDA : GTD_OK)) break;
             rc = ens_launch(e, 1);
             if (rc) break;

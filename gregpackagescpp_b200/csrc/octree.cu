@@ -461,8 +461,10 @@ __device__ __forceinline__ double sub_t(double a, double b) { return __dsub_rn(a
 // is loaded once for the lanes that need it and each body meets exactly the nodes of its own walk,
 // in its own order.  IL: the float tree's A and B halves of a node are interleaved in rec_a, so the
 // two 16-byte loads hit one 32-byte sector (measured 23.2 -> 21.5 ms at N = 4194304, theta = 0.5).
-template <typename T, bool IL = false>
-__global__ void __launch_bounds__(kTT) walk_kernel(int64_t n, int64_t n_nodes, const void *rec_a_v, const int4 *rec_b,
+// SOFT = false drops the + eps^2 of an unsoftened walk (eps = 0, the reference's default; adding 0
+// changes no value); COUNT = false skips the per-body interaction count nobody reads.
+template <typename T, bool IL = false, bool SOFT = true, bool COUNT = true>
+__global__ void __launch_bounds__(kTT, sizeof(T) == 4 ? 8 : 1) walk_kernel(int64_t n, int64_t n_nodes, const void *rec_a_v, const int4 *rec_b,
                                                    const double *w2_64, const void *slot_pos_v, const int32_t *own,
                                                    T th2, T eps2, void *slot_acc_v, uint32_t *slot_cnt) {
     using V = typename V4<T>::type;
@@ -501,26 +503,26 @@ __global__ void __launch_bounds__(kTT) walk_kernel(int64_t n, int64_t n_nodes, c
             if (count == 1) {
                 if ((int32_t)node != ol) {
                     const T dx = A.x - p.x, dy = A.y - p.y, dz = A.z - p.z;
-                    const T r2 = dx * dx + dy * dy + dz * dz + eps2;
+                    const T r2 = SOFT ? dx * dx + dy * dy + dz * dz + eps2 : dx * dx + dy * dy + dz * dz;
                     const T inv = rsqrt_t(r2);
                     const T sc = A.w * inv * inv * inv;
                     ax += sc * dx;
                     ay += sc * dy;
                     az += sc * dz;
-                    ++cnt;
+                    if constexpr (COUNT) ++cnt;
                 }
             } else {
                 for (int q = B.y; q < B.y + count; ++q) {
                     if (q == (int)s) continue;
                     const V Q = bodies[q];
                     const T dx = Q.x - p.x, dy = Q.y - p.y, dz = Q.z - p.z;
-                    const T r2 = dx * dx + dy * dy + dz * dz + eps2;
+                    const T r2 = SOFT ? dx * dx + dy * dy + dz * dz + eps2 : dx * dx + dy * dy + dz * dz;
                     const T inv = rsqrt_t(r2);
                     const T sc = Q.w * inv * inv * inv;
                     ax += sc * dx;
                     ay += sc * dy;
                     az += sc * dz;
-                    ++cnt;
+                    if constexpr (COUNT) ++cnt;
                 }
             }
             next = (uint32_t)B.x;
@@ -529,13 +531,13 @@ __global__ void __launch_bounds__(kTT) walk_kernel(int64_t n, int64_t n_nodes, c
             const T r2 = fma_t(dz, dz, fma_t(dy, dy, mul_t(dx, dx)));
             const T w2 = sizeof(T) == 4 ? (T)__int_as_float(B.w) : (T)w2_64[node];
             if (w2 < mul_t(th2, r2)) {
-                const T r2e = r2 + eps2;
+                const T r2e = SOFT ? r2 + eps2 : r2;
                 const T inv = rsqrt_t(r2e);
                 const T sc = A.w * inv * inv * inv;
                 ax += sc * dx;
                 ay += sc * dy;
                 az += sc * dz;
-                ++cnt;
+                if constexpr (COUNT) ++cnt;
                 next = (uint32_t)B.x;
             } else {
                 next = node + 1;
@@ -546,7 +548,7 @@ __global__ void __launch_bounds__(kTT) walk_kernel(int64_t n, int64_t n_nodes, c
         V o;
         o.x = ax; o.y = ay; o.z = az; o.w = (T)0;
         reinterpret_cast<V *>(slot_acc_v)[s] = o;
-        slot_cnt[s] = cnt;
+        if constexpr (COUNT) slot_cnt[s] = cnt;
     }
 }
 
@@ -804,33 +806,45 @@ static int bh_build_impl(gtd_system *s, int tree_float) {
     return GTD_OK;
 }
 
-// Walk for every body; accelerations in body order, optionally kicking v by kick * a.
-static int bh_walk_impl(gtd_system *s, double kick, bool do_kick) {
+// Launches the walk form for (softened?, counted?) on the handle's stream.
+template <typename T, bool IL>
+static void launch_walk(gtd_system *s, T th2, T e2, bool count) {
+    const int64_t n = s->n;
+    const bool soft = e2 != (T)0;
+    auto go = [&](auto kern) {
+        kern<<<blocks_for(n), kTT, 0, s->stream>>>(n, s->n_nodes, s->nwalk_a, s->nwalk_b, s->nwalk_w2, s->slot_pos,
+                                                   s->own_leaf, th2, e2, s->slot_acc, s->slot_cnt);
+    };
+    if (soft) {
+        if (count) go(walk_kernel<T, IL, true, true>);
+        else go(walk_kernel<T, IL, true, false>);
+    } else {
+        if (count) go(walk_kernel<T, IL, false, true>);
+        else go(walk_kernel<T, IL, false, false>);
+    }
+}
+
+// Walk for every body; accelerations in body order, optionally kicking v by kick * a, and with
+// `count` the interactions each body took (for gtd_bh_accelerations' n_inter).
+static int bh_walk_impl(gtd_system *s, double kick, bool do_kick, bool count) {
     if (!s->tree_valid) return fail(GTD_ERR_INVALID_ARGUMENT, "no Barnes-Hut tree: call gtd_bh_build first");
     const int64_t n = s->n;
     cudaStream_t st = s->stream;
     if (!s->bh_ninter) GTD_CUDA(cudaMalloc(&s->bh_ninter, sizeof(uint32_t) * (size_t)s->cap));
+    uint32_t *ninter = count ? s->bh_ninter : nullptr;
     if (s->tree_float) {
         const float th2 = (float)(s->theta * s->theta), e2 = (float)(s->eps * s->eps);
-        if (s->walk_interleaved)
-            walk_kernel<float, true><<<blocks_for(n), kTT, 0, st>>>(n, s->n_nodes, s->nwalk_a, s->nwalk_b,
-                                                                    s->nwalk_w2, s->slot_pos, s->own_leaf, th2, e2,
-                                                                    s->slot_acc, s->slot_cnt);
-        else
-            walk_kernel<float><<<blocks_for(n), kTT, 0, st>>>(n, s->n_nodes, s->nwalk_a, s->nwalk_b, s->nwalk_w2,
-                                                              s->slot_pos, s->own_leaf, th2, e2, s->slot_acc,
-                                                              s->slot_cnt);
+        if (s->walk_interleaved) launch_walk<float, true>(s, th2, e2, count);
+        else launch_walk<float, false>(s, th2, e2, count);
         GTD_CHECK_LAUNCH();
         scatter_acc_kernel<float><<<blocks_for(n), kTT, 0, st>>>(n, s->perm, s->slot_acc, s->slot_cnt, s->acc,
-                                                                 s->bh_ninter, do_kick ? s->vel : nullptr, kick);
+                                                                 ninter, do_kick ? s->vel : nullptr, kick);
     } else {
         const double th2 = s->theta * s->theta, e2 = s->eps * s->eps;
-        walk_kernel<double><<<blocks_for(n), kTT, 0, st>>>(n, s->n_nodes, s->nwalk_a, s->nwalk_b, s->nwalk_w2,
-                                                           s->slot_pos, s->own_leaf, th2, e2, s->slot_acc,
-                                                           s->slot_cnt);
+        launch_walk<double, false>(s, th2, e2, count);
         GTD_CHECK_LAUNCH();
         scatter_acc_kernel<double><<<blocks_for(n), kTT, 0, st>>>(n, s->perm, s->slot_acc, s->slot_cnt, s->acc,
-                                                                  s->bh_ninter, do_kick ? s->vel : nullptr, kick);
+                                                                  ninter, do_kick ? s->vel : nullptr, kick);
     }
     GTD_CHECK_LAUNCH();
     s->launches += 2;
@@ -845,7 +859,7 @@ int bh_evolve_kdk(gtd_system *s, uint64_t steps) {
     const int tf = s->tree_float;
     int rc = bh_build_impl(s, tf);
     if (rc) return rc;
-    rc = bh_walk_impl(s, 0.5 * s->dt, true);
+    rc = bh_walk_impl(s, 0.5 * s->dt, true, false);
     if (rc) return rc;
     for (uint64_t k = 0; k < steps; ++k) {
         drift_kernel<<<blocks_for(s->n), kTT, 0, s->stream>>>(s->n, s->pm[s->cur], s->vel, s->dt);
@@ -853,7 +867,7 @@ int bh_evolve_kdk(gtd_system *s, uint64_t steps) {
         s->launches += 1;
         rc = bh_build_impl(s, tf);
         if (rc) return rc;
-        rc = bh_walk_impl(s, s->dt, true);
+        rc = bh_walk_impl(s, s->dt, true, false);
         if (rc) return rc;
         if (s->coll != GTD_NO_COLL) {
             rc = run_bh_collisions(s);
@@ -884,7 +898,7 @@ static int copy_bh_out(gtd_system *s, double *a3, uint32_t *n_inter) {
 int bh_accelerations(gtd_system *s, double *a3, uint32_t *n_inter) {
     int rc = bh_build_impl(s, s->tree_float);
     if (rc) return rc;
-    rc = bh_walk_impl(s, 0.0, false);
+    rc = bh_walk_impl(s, 0.0, false, n_inter != nullptr);
     if (rc) return rc;
     return copy_bh_out(s, a3, n_inter);
 }
@@ -1029,7 +1043,7 @@ int gtd_bh_tree_download(gtd_system *s, uint64_t *codes, int32_t *perm, int8_t *
 int gtd_bh_accelerations(gtd_system *s, double *a3, uint32_t *n_inter) {
     if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
     if (!s->tree_valid) return fail(GTD_ERR_INVALID_ARGUMENT, "no Barnes-Hut tree: call gtd_bh_build first");
-    int rc = bh_walk_impl(s, 0.0, false);
+    int rc = bh_walk_impl(s, 0.0, false, n_inter != nullptr);
     if (rc) return rc;
     return copy_bh_out(s, a3, n_inter);
 }
