@@ -644,8 +644,8 @@ int gtd_ensemble_config(const gtd_ensemble *e, int *threads, int *bodies_per_thr
     return GTD_OK;
 }
 
-// Times one step for each CTA size on a copy of the current state (restored afterwards) and keeps
-// the fastest: the project's tile autotuner for the ensemble.
+// Times a few steps for each CTA size and bodies-per-thread choice on a copy of the current state
+// (restored afterwards) and keeps the fastest: the project's tile autotuner for the ensemble.
 int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
     if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
     if (e->n_sys == 0) return fail(GTD_ERR_INVALID_ARGUMENT, "autotune needs systems");
@@ -674,30 +674,38 @@ int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
     };
     int rc = save(false);
     const bool was_begun = e->begun;
+    const int orig_threads = e->threads, orig_ib = e->ib;
     const int cands[][2] = {{128, 1}, {256, 1}, {512, 1}, {128, 2}, {256, 2}};
-    int best = e->threads, best_ib = e->ib;
-    double bestv = 1e300;
-    for (const auto &cf : cands) {
-        if (rc) break;
-        const int c = cf[0];
-        e->threads = c;
-        e->ib = cf[1];
-        for (int rep = 0; rep < 6 && !rc; ++rep) {  // the first launch is not counted; min of five
+    constexpr int kCands = sizeof(cands) / sizeof(cands[0]);
+    // Each timing runs kTuneSteps consecutive steps from the saved state, so a candidate is judged on
+    // steady stepping rather than on one launch.  The candidates take turns (round robin) so that a
+    // clock still ramping up after the upload favours none of them; the first round only warms up.
+    constexpr int kTuneSteps = 4, kRounds = 3;
+    double per[kCands];
+    for (int k = 0; k < kCands; ++k) per[k] = 1e300;
+    for (int round = 0; round < kRounds && !rc; ++round) {
+        for (int k = 0; k < kCands && !rc; ++k) {
+            e->threads = cands[k][0];
+            e->ib = cands[k][1];
             if ((rc = cudaEventRecord(e->ev0, e->stream) ? GTD_ERR_CUDA : GTD_OK)) break;
-            rc = ens_launch(e, 1);
+            for (int q = 0; q < kTuneSteps && !rc; ++q) rc = ens_launch(e, 1);
             if (rc) break;
             cudaEventRecord(e->ev1, e->stream);
             cudaEventSynchronize(e->ev1);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e->ev0, e->ev1);
-            if (rep > 0 && ms < bestv) {
-                bestv = ms;
-                best = c;
-                best_ib = cf[1];
-            }
-            if (!rc) rc = save(true);
+            if (round > 0) per[k] = std::min(per[k], (double)ms / kTuneSteps);
+            rc = save(true);
         }
     }
+    int best = orig_threads, best_ib = orig_ib;  // kept if no timing completed
+    double bestv = 1e300;
+    for (int k = 0; k < kCands; ++k)
+        if (per[k] < bestv) {
+            bestv = per[k];
+            best = cands[k][0];
+            best_ib = cands[k][1];
+        }
     e->threads = best;
     e->ib = best_ib;
     e->begun = was_begun;
