@@ -165,6 +165,21 @@ def test_graph_replayed_steps_are_bit_identical(gpu, name):
     assert np.array_equal(a.x, b.x) and np.array_equal(a.v, b.v)
 
 
+@pytest.mark.parametrize("n", [37, 4096])
+def test_graph_replayed_small_n_bit_identical(gpu, n):
+    """The one-launch-per-step FP64 kernel replayed from the step graph: 40 graph-replayed KDK
+    steps equal 40 steps launched one by one, bit for bit, for an odd N and for N = 4096, whose
+    grid (1024 CTAs) is larger than what the GPU holds at once."""
+    from gregpackagescpp_b200 import _lib
+    m, x, v = plummer(n, 900 + n)
+    a = System(m, x, v, timestep=3600.0, num_iterations=40, units_format=UNITS_G6674)
+    b = System(m, x, v, timestep=3600.0, num_iterations=40, units_format=UNITS_G6674)
+    _lib.check(b._L.gtd_system_time_force_kernels(b._h, 1))
+    a.evolve(METHODS["leapfrog_kdk"])
+    b.evolve(METHODS["leapfrog_kdk"])
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.v, b.v)
+
+
 @pytest.mark.parametrize("n", [1, 2, 31, 1024, 4096, 4097])
 def test_fused_small_path_vs_oracle(gpu, oracle, n):
     """FP64 systems up to 4096 bodies evaluate each force with its update in one launch (a warp per
