@@ -58,17 +58,25 @@ def parse_args():
     p.add_argument("--cpu-sample-steps", type=int, default=3)
     p.add_argument("--cpu-baseline-steps", type=int, default=40,
                    help="steps of the single-core reference sample beside the GPU line (~10 s at N=8192)")
-    p.add_argument("--drift-steps", type=int, default=0,
-                   help="instead of the benchmark: evolve the workload this many steps in both the mixed and the "
-                        "FP64 path and report |dE/E| and momentum drift every --drift-every steps")
+    p.add_argument("--drift-steps", type=int, default=1000,
+                   help="after the timed loop (untimed, one GPU): evolve the workload this many steps in both the "
+                        "mixed and the FP64 path and report |dE/E| and momentum drift every --drift-every steps "
+                        "(0: skip)")
     p.add_argument("--drift-every", type=int, default=100)
+    p.add_argument("--drift-only", action="store_true", help="print only the drift series")
+    p.add_argument("--oracle-rows", type=int, default=512,
+                   help="rows of the N-body force checked against the CPU oracle (untimed)")
+    p.add_argument("--configs", choices=["all", "none"], default="all",
+                   help="after the headline (untimed, one GPU): the other configurations of the path")
     p.add_argument("--workload", choices=["direct-mixed", "direct-fp64-1024", "bh", "ensemble", "adjoint", "comet"],
                    default="direct-mixed", help="direct-mixed is the headline; the others print their own line")
     p.add_argument("--bh-n", type=int, default=4194304)
     p.add_argument("--bh-cpu-n", type=int, default=10000)
+    p.add_argument("--bh-steps", type=int, default=200, help="evolve(leapfrog_kdk | barnes_hut) steps timed end to end")
     p.add_argument("--bh-walk-variant", type=int, default=-1,
                    help="node records of the float-tree walk: -1 default, 0 separate arrays, 1 interleaved")
     p.add_argument("--ens-systems", type=int, default=4096)
+    p.add_argument("--ens-steps", type=int, default=128, help="ensemble steps timed (after the warm-up chunk)")
     p.add_argument("--ens-config", type=str, default="",
                    help="THREADS,BODIES_PER_THREAD for the ensemble kernel instead of the autotuner's choice")
     p.add_argument("--adj-n", type=int, default=16384)
@@ -263,6 +271,62 @@ def run_reference(args, rank, world):
 # ------------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------------
+def _dist_stats(rel):
+    """Distribution of per-body relative errors."""
+    rel = np.asarray(rel, dtype=np.float64)
+    return {"rms": float(np.sqrt((rel ** 2).mean())), "median": float(np.median(rel)),
+            "p99": float(np.quantile(rel, 0.99)), "p99_9": float(np.quantile(rel, 0.999)), "max": float(rel.max())}
+
+
+def oracle_rows_check(m, x, accs, n_rows, seed, threads):
+    """The checker beside the CPU baseline: accelerations on `n_rows` seeded rows from the oracle
+    (the reference's cumulative_acc arithmetic, summed over all other bodies), against each GPU
+    path's accelerations.  Per row: the error relative to |a_i| and relative to the row's force
+    scale sum_j G m_j / r_ij^2 (what an FP32 sum of the row's terms rounds against)."""
+    import ctypes as _C
+    from oracle.oracle import Oracle
+    o = Oracle()
+    rows = np.sort(np.random.default_rng(seed).choice(len(m), n_rows, replace=False))
+    t0 = time.perf_counter()
+    want, gross = o.direct_acc_rows(m, x, _C.c_longdouble(6.674e-11), rows, threads=threads)
+    secs = time.perf_counter() - t0
+    amag = np.linalg.norm(want, axis=1)
+    out = {"rows": int(n_rows), "row_seed": seed, "oracle_s": secs, "threads": threads,
+           "force_scale_over_abs_a": {"median": float(np.median(gross / amag)), "max": float((gross / amag).max())}}
+    for name, a in accs.items():
+        err = np.linalg.norm(a[rows] - want, axis=1)
+        rel = err / amag
+        d = _dist_stats(rel)
+        d["max_over_force_scale"] = float((err / gross).max())
+        worst = np.argsort(rel)[-3:][::-1]
+        d["worst_rows"] = [{"row": int(rows[k]), "rel": float(rel[k]),
+                            "force_scale_over_abs_a": float(gross[k] / amag[k])} for k in worst]
+        out[name] = d
+    return out
+
+
+def measured_peaks(local):
+    """HBM denominator: the driver's MEASURED_PEAKS.json (a measured copy on this pool) where present,
+    else a device-to-device copy timed here.  The FMA peaks come from the library's microkernel."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]) * 1e9, "MEASURED_PEAKS.json hbm_gbs (measured copy on this pool)"
+    except Exception:
+        pass
+    import torch
+    nb = 2 << 30
+    a = torch.empty(nb // 4, dtype=torch.float32, device=f"cuda:{local}")
+    b = torch.empty_like(a)
+    b.copy_(a)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        b.copy_(a)
+    e1.record()
+    e1.synchronize()
+    return 5 * 2 * nb / (e0.elapsed_time(e1) * 1e-3), "device-to-device copy of 2 GiB timed in this run"
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -317,11 +381,13 @@ def run_ours(args, rank, world, local):
                        "force_ms": best_ms.value}
 
     stage("accuracy")
-    # --- accuracy of the mixed force against the FP64 one at the initial state (untimed)
+    # --- accelerations of both paths at the initial state (untimed); checked against the oracle
+    # beside the CPU baseline below, and against each other here
     a64, amx = np.zeros(3 * n), np.zeros(3 * n)
     check(L.gtd_system_accelerations(h64, 0, a64.ctypes.data))
     check(L.gtd_system_accelerations(hmx, 0, amx.ctypes.data))
-    rel = np.linalg.norm((amx - a64).reshape(n, 3), axis=1) / np.linalg.norm(a64.reshape(n, 3), axis=1)
+    a64, amx = a64.reshape(n, 3), amx.reshape(n, 3)
+    rel = np.linalg.norm(amx - a64, axis=1) / np.linalg.norm(a64, axis=1)
 
     stage("fp64 throughput")
     # --- FP64 GPU path throughput (same workload, fewer steps)
@@ -384,6 +450,7 @@ def run_ours(args, rank, world, local):
     check(L.gtd_measure_fma_peak(local, _lib.PREC_F64, C.byref(peak64)))
     avg_force_s = force_ms.value * 1e-3 / max(force_n.value, 1)
     achieved = FLOPS_PER_INTERACTION * pair / avg_force_s
+    hbm_peak, hbm_src = measured_peaks(local)
 
     stage("e2e")
     # --- end to end through the public C ABI with host buffers (upload, evolve, download)
@@ -408,14 +475,30 @@ def run_ours(args, rank, world, local):
     h2d = (m.nbytes + x3.nbytes + v3.nbytes) * args.e2e_calls / e2e_steps
     d2h = (xo.nbytes + vo.nbytes + ao.nbytes) * args.e2e_calls / e2e_steps
 
-    cpu = None
+    cpu, oracle_check = None, None
     if rank == 0 and world == 1 and args.cpu_sample_n > 0:
-        stage("cpu baseline sample")
+        stage("cpu baseline sample + oracle rows")
         cval, kind, secs = cpu_sample(args.cpu_sample_n, args.cpu_baseline_steps, args.seed, 1)
         cpu = {"value": cval, "unit": UNIT, "cores": 1, "kind": kind,
                "sample": f"the reference evolve(leapfrog_kdk) (single-threaded by design) on an N="
                          f"{args.cpu_sample_n} Plummer sphere, {args.cpu_baseline_steps} step(s) "
                          f"({args.cpu_baseline_steps + 1} force evaluations), {secs:.1f} s of evolve time"}
+        if args.oracle_rows > 0:
+            oracle_check = oracle_rows_check(m, x, {"fp64": a64, "mixed": amx}, args.oracle_rows, 5, host_threads())
+
+    drift_out, cfgs = None, None
+    if rank == 0 and world == 1 and args.drift_steps > 0:
+        stage(f"drift series ({args.drift_steps} steps, mixed and fp64)")
+        drift_out = drift_series(args, local, autotune=False)
+    if rank == 0 and world == 1 and args.configs == "all":
+        cfgs = {}
+        for name, fn in (("direct_fp64_1024", cfg_fp64_small), ("barnes_hut", cfg_bh), ("ensemble", cfg_ensemble),
+                         ("adjoint", cfg_adjoint)):
+            stage(f"config {name}")
+            try:
+                cfgs[name] = fn(args, local, peak.value, peak64.value, hbm_peak)
+            except Exception as exc:  # a failing secondary configuration must not hide the headline
+                cfgs[name] = {"error": f"{type(exc).__name__}: {exc}"}
 
     if rank == 0:
         line = {
@@ -427,9 +510,9 @@ def run_ours(args, rank, world, local):
                        "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
                        "l2": "flushed (512 MB write) between timed steps, outside the timed events"},
             "fp64_gpu": {"value": fp64_value, "unit": UNIT, "steps": args.fp64_steps,
-                         "mixed_over_fp64": value / world / fp64_value},
-            "accuracy": {"acc_rel_err_rms": float(np.sqrt((rel ** 2).mean())),
-                         "acc_rel_err_median": float(np.median(rel)), "acc_rel_err_max": float(rel.max()),
+                         "mixed_over_fp64": value / world / fp64_value,
+                         "frac_of_fp64_peak": FLOPS_PER_INTERACTION * fp64_value / peak64.value},
+            "accuracy": {"mixed_vs_fp64_all_bodies": _dist_stats(rel),
                          "energy_drift_rel": drift, "energy_drift_steps": W + K},
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
                          "unit": "TFLOP/s", "frac": achieved / peak.value,
@@ -438,20 +521,28 @@ def run_ours(args, rank, world, local):
                          "algorithmic_bytes": 32 * n,
                          "kernel": "force_mixed_kernel", "flops_per_interaction": FLOPS_PER_INTERACTION,
                          "peak_source": "measured FFMA/FFMA2 microkernel on this GPU (gtd_measure_fma_peak)",
-                         "fp64_peak": peak64.value / 1e12},
+                         "fp64_peak": peak64.value / 1e12, "hbm_peak_GBs": hbm_peak / 1e9,
+                         "hbm_peak_source": hbm_src},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "calls": args.e2e_calls, "iterations_per_call": iters},
             "gpu_launches": gpu_launches,
             "autotuned": tuned,
             "clocks": clk,
         }
+        if oracle_check is not None:
+            line["accuracy"]["vs_oracle_rows"] = oracle_check
+        if drift_out is not None:
+            line["drift"] = drift_out
+        if cfgs is not None:
+            line["configs"] = cfgs
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
 
 
-def run_drift(args, local):
-    """Energy and momentum conservation of the workload over a long run, mixed next to FP64."""
+def drift_series(args, local, autotune=True):
+    """Energy and momentum conservation of the workload over a long run, mixed next to FP64:
+    |dE/E| and |P|/(sum m|v|) every --drift-every steps (untimed; wall seconds reported)."""
     from gregpackagescpp_b200 import _lib
     from gregpackagescpp_b200._lib import check
     from gregpackagescpp_b200.ics import plummer
@@ -460,14 +551,16 @@ def run_drift(args, local):
     n = args.n
     m, x, v = plummer(n, args.seed)
     x3, v3 = np.ascontiguousarray(x.reshape(-1)), np.ascontiguousarray(v.reshape(-1))
-    out = {"workload": f"N={n} Plummer, leapfrog KDK dt=3600 s", "steps": args.drift_steps, "series": {}}
+    out = {"workload": f"N={n} Plummer, leapfrog KDK dt=3600 s", "steps": args.drift_steps,
+           "every": args.drift_every, "columns": ["step", "dE_over_E", "abs_P_over_sum_m_abs_v"], "series": {}}
     for name, prec in (("mixed", _lib.PREC_MIXED), ("fp64", _lib.PREC_F64)):
         h = C.c_void_p()
         check(L.gtd_system_create(C.byref(h), local, prec))
         check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, 1000, 0.0, 0.5))
         check(L.gtd_system_upload(h, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
-        best = C.c_int()
-        check(L.gtd_system_autotune_direct(h, 2, C.byref(best), None))
+        if autotune:
+            best = C.c_int()
+            check(L.gtd_system_autotune_direct(h, 2, C.byref(best), None))
         ke, pe, p = C.c_double(), C.c_double(), np.zeros(3)
         check(L.gtd_system_energy(h, C.byref(ke), C.byref(pe), p.ctypes.data, None))
         E0, pscale = ke.value + pe.value, float((m[:, None] * np.abs(v)).sum())
@@ -481,12 +574,13 @@ def run_drift(args, local):
             done += k
             check(L.gtd_system_energy(h, C.byref(ke), C.byref(pe), p.ctypes.data, None))
             rows.append((done, (ke.value + pe.value - E0) / abs(E0), float(np.linalg.norm(p)) / pscale))
-        out["series"][name] = {"wall_s": time.perf_counter() - t0, "step_dE_over_E_dP": rows}
+        out["series"][name] = {"wall_s": time.perf_counter() - t0, "rows": rows}
         check(L.gtd_system_destroy(h))
-    mx, fx = out["series"]["mixed"]["step_dE_over_E_dP"], out["series"]["fp64"]["step_dE_over_E_dP"]
+    mx, fx = out["series"]["mixed"]["rows"], out["series"]["fp64"]["rows"]
     out["max_abs_dE_over_E"] = {"mixed": max(abs(r[1]) for r in mx), "fp64": max(abs(r[1]) for r in fx)}
     out["max_abs_mixed_minus_fp64_dE_over_E"] = max(abs(a[1] - b[1]) for a, b in zip(mx, fx))
-    print(json.dumps(out), flush=True)
+    out["max_abs_P_over_sum_m_abs_v"] = {"mixed": max(r[2] for r in mx), "fp64": max(r[2] for r in fx)}
+    return out
 
 
 # ------------------------------------------------------------------------------------------------
@@ -498,7 +592,7 @@ def _events(stream):
     return a, b
 
 
-def run_fp64_small(args, local):
+def cfg_fp64_small(args, local, peak32=None, peak64=None, hbm=None):
     """Plain direct summation as the reference runs it: N=1024 Plummer, FP64, leapfrog KDK,
     dt=3600 s, 1000 steps; final state against the reference CPU run of the same call."""
     from gregpackagescpp_b200 import System
@@ -514,6 +608,8 @@ def run_fp64_small(args, local):
     inter = (steps + 1) * n * (n - 1)
     line = {"workload": "direct FP64, N=1024 Plummer, leapfrog KDK dt=3600 s, 1000 steps", "unit": UNIT,
             "device_value": inter / (ns * 1e-9), "e2e_value": inter / wall, "device_s": ns * 1e-9, "e2e_s": wall}
+    if peak64:
+        line["frac_of_fp64_peak"] = FLOPS_PER_INTERACTION * inter / (ns * 1e-9) / peak64
     try:
         from oracle.oracle import RefOracle
         if RefOracle.available():
@@ -523,10 +619,10 @@ def run_fp64_small(args, local):
                                            "v": float(np.abs(s.v - vo).max() / np.abs(vo).max())}
     except Exception as exc:  # the reference library is optional on a box
         line["reference_cpu"] = {"unavailable": str(exc)}
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_bh(args, local):
+def cfg_bh(args, local, peak32=None, peak64=None, hbm=None):
     """Barnes-Hut: two Plummer spheres of 2^21 bodies each on a parabolic approach, FP32 tree
     (T=float geometry, FP64 moments), theta=0.5, leapfrog KDK dt=3600 s; per-phase device times."""
     from gregpackagescpp_b200 import _lib
@@ -539,7 +635,7 @@ def run_bh(args, local):
     x3, v3 = np.ascontiguousarray(x.reshape(-1)), np.ascontiguousarray(v.reshape(-1))
     h = C.c_void_p()
     check(L.gtd_system_create(C.byref(h), local, _lib.PREC_F64))
-    check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, args.steps, 0.0, 0.5))
+    check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, args.bh_steps, 0.0, 0.5))
     check(L.gtd_system_upload(h, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
     check(L.gtd_bh_set_tree_float(h, 1))
     check(L.gtd_bh_set_walk_variant(h, args.bh_walk_variant))
@@ -567,9 +663,9 @@ def run_bh(args, local):
     nn, nl = C.c_int64(), C.c_int64()
     check(L.gtd_bh_tree_size(h, C.byref(nn), C.byref(nl), None))
     inter = float(cnt.astype(np.float64).sum())
-    # the reference schedule end to end: evolve(leapfrog_kdk | barnes_hut) for --steps steps
+    # the reference schedule end to end: evolve(leapfrog_kdk | barnes_hut) for --bh-steps steps
     ns = C.c_int64()
-    check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, args.steps, 0.0, 0.5))
+    check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, args.bh_steps, 0.0, 0.5))
     check(L.gtd_system_upload(h, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
     check(L.gtd_system_evolve(h, 16 | 65536, C.byref(ns)))
     check(L.gtd_system_destroy(h))
@@ -583,8 +679,12 @@ def run_bh(args, local):
             "walk_interactions_per_s": inter / (walk_ms * 1e-3),
             "walk_flops_20_per_interaction_TFLOPs": 20 * inter / (walk_ms * 1e-3) / 1e12,
             "build_algorithmic_GBs": build_bytes / (build_ms * 1e-3) / 1e9,
-            "walk_variant": args.bh_walk_variant, "evolve_steps": args.steps, "evolve_s": ns.value * 1e-9,
-            "steps_per_s": args.steps / (ns.value * 1e-9)}
+            "walk_variant": args.bh_walk_variant, "evolve_steps": args.bh_steps, "evolve_s": ns.value * 1e-9,
+            "steps_per_s": args.bh_steps / (ns.value * 1e-9)}
+    if peak32:
+        line["walk_frac_of_fp32_peak"] = 20 * inter / (walk_ms * 1e-3) / peak32
+    if hbm:
+        line["build_frac_of_hbm"] = build_bytes / (build_ms * 1e-3) / hbm
     try:
         from gregpackagescpp_b200.ics import two_plummer as tp
         from oracle.oracle import RefOracle
@@ -596,10 +696,10 @@ def run_bh(args, local):
                                      "walk_interactions_per_s": rcnt / (w_ns * 1e-9), "cores": 1}
     except Exception as exc:
         line["reference_cpu"] = {"unavailable": str(exc)}
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_ensemble(args, local):
+def cfg_ensemble(args, local, peak32=None, peak64=None, hbm=None):
     """4096 independent systems, N ~ U{3..2048}, log-uniform masses, radii from 1500 kg/m^3,
     positions in a 10 AU ball, sigma_v = 5 km/s; FP64 state, FP32 forces, merges; KDK dt=600 s."""
     from gregpackagescpp_b200.ensemble import Ensemble
@@ -616,7 +716,7 @@ def run_ensemble(args, local):
     # before the timed region
     e.evolve(max(args.warmup, 16))
     counts0, merges0, l0 = e.counts()
-    K = max(args.steps, 16)
+    K = max(args.ens_steps, 16)
     ns = e.evolve(K)
     counts, merges, l1 = e.counts()
     inter = float((counts.astype(np.float64) * (counts - 1)).sum())
@@ -627,6 +727,8 @@ def run_ensemble(args, local):
             "bodies": int(off[-1]), "merges_during_timed": int(merges - merges0), "autotuned_threads": threads,
             "bodies_per_thread": e.config()[1],
             "gpu_launches": int(l1 - l0), "launch": "one persistent launch per step, replayed from a CUDA graph"}
+    if peak32:
+        line["frac_of_fp32_peak"] = 20 * inter * K / secs / peak32
     try:
         from oracle.oracle import RefOracle
         if RefOracle.available():
@@ -649,10 +751,10 @@ def run_ensemble(args, local):
                                      "sample": "24 random systems, evolve(leapfrog_kdk) 4 steps, collisions off"}
     except Exception as exc:
         line["reference_cpu"] = {"unavailable": str(exc)}
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_adjoint(args, local):
+def cfg_adjoint(args, local, peak32=None, peak64=None, hbm=None):
     """Adjoint: N=16384 Plummer, FP64 KDK dt=3600 s, 2000 steps, checkpoints every 45 steps;
     loss = mean |x_T - x*|^2 with x* = forward final + N(0, (0.01 AU)^2)."""
     import torch
@@ -680,6 +782,8 @@ def run_adjoint(args, local):
     fwd, bwd = e0.elapsed_time(e1), e1.elapsed_time(e2)
     line = {"workload": f"adjoint KDK N={n}, {T} steps, checkpoints every {every}", "forward_ms": fwd,
             "backward_ms": bwd, "backward_over_forward": bwd / fwd, "total_over_forward": (fwd + bwd) / fwd}
+    if peak64:
+        line["forward_frac_of_fp64_peak"] = 20.0 * (T + 1) * n * (n - 1) / (fwd * 1e-3) / peak64
     if args.adj_fd > 0:
         # central differences of the library's own FP64 forward, h relative to the coordinate, at
         # two steps per group: the specified 1e-6 for positions and velocities (1e-4 for masses,
@@ -720,7 +824,7 @@ def run_adjoint(args, local):
                              f"h_rel_{10 * hrel:g}": summary(g, d2),
                              "fd_h_vs_10h_normwise": float(np.abs(d1 - d2).max() / np.abs(d2).max())}
         line["fd_check"] = fd_out
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_comet(args, local):
@@ -822,13 +926,17 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
-        elif args.drift_steps > 0:
+        elif args.drift_only:
             if rank == 0:
-                run_drift(args, local)
+                print(json.dumps(drift_series(args, local)), flush=True)
         elif args.workload != "direct-mixed":
             if rank == 0:
-                {"direct-fp64-1024": run_fp64_small, "bh": run_bh, "ensemble": run_ensemble,
-                 "adjoint": run_adjoint, "comet": run_comet}[args.workload](args, local)
+                if args.workload == "comet":
+                    run_comet(args, local)
+                else:
+                    fn = {"direct-fp64-1024": cfg_fp64_small, "bh": cfg_bh, "ensemble": cfg_ensemble,
+                          "adjoint": cfg_adjoint}[args.workload]
+                    print(json.dumps(fn(args, local)), flush=True)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "gtd_internal.cuh"
+#include "gtd_math.cuh"
 
 namespace gtd {
 
@@ -66,8 +67,7 @@ __global__ void __launch_bounds__(kVT) vjp_kernel(VjpArgs a) {
                 const double4 xj = tx[jj], wj = tw[jj];
                 const double dx = xj.x - xk.x, dy = xj.y - xk.y, dz = xj.z - xk.z;
                 const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-                double inv = rsqrt(r2);
-                inv = r2 > 0.0 ? inv : 0.0;  // j == k and padding contribute nothing
+                const double inv = r2 > 0.0 ? inv_r(r2) : 0.0;  // j == k and padding contribute nothing
                 const double inv2 = inv * inv, inv3 = inv2 * inv;
                 const double ux = xk.w * wj.x - xj.w * wk.x;
                 const double uy = xk.w * wj.y - xj.w * wk.y;

@@ -18,6 +18,7 @@
 #include <tuple>
 
 #include "gtd_internal.cuh"
+#include "gtd_math.cuh"
 
 namespace gtd {
 
@@ -27,6 +28,7 @@ struct ForceKArgs {
     const double4 *src;
     double G;
     double *part;
+    float near2;  // mixed kernel: a pair with r^2 < near2 |X_i|^2 sends its fold to the precise path
 };
 
 __device__ __forceinline__ void cta_range(const ForceKArgs &a, int g, int64_t &s, int64_t &e) {
@@ -36,8 +38,31 @@ __device__ __forceinline__ void cta_range(const ForceKArgs &a, int g, int64_t &s
 
 // -------------------------------------------------------------------------------------------
 // FP64: a_i = sum_j G m_j (x_j - x_i) / |x_j - x_i|^3, no softening (the reference's direct path
-// ignores eps).  The i == j term has r2 == 0 and is dropped by the select on inv.
+// ignores eps).  |r|^-3 comes from inv_r3 (a MUFU seed and a second-order binomial correction,
+// gtd_math.cuh): 16 FP64 operations per pair in all.  Tiles that hold the self pair (i == j,
+// r2 == 0) or padding bodies take the guarded loop, which selects their terms away; all others
+// run without a compare.
 // -------------------------------------------------------------------------------------------
+template <int I, int BJ, bool kGuard>
+__device__ __forceinline__ void f64_tile(const double4 *__restrict__ tile, const double (&xi)[I],
+                                         const double (&yi)[I], const double (&zi)[I], double (&ax)[I],
+                                         double (&ay)[I], double (&az)[I]) {
+#pragma unroll 4
+    for (int jj = 0; jj < BJ; ++jj) {
+        const double4 q = tile[jj];
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            const double dx = q.x - xi[k], dy = q.y - yi[k], dz = q.z - zi[k];
+            const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+            double sc = q.w * inv_r3(r2);
+            if (kGuard) sc = r2 > 0.0 ? sc : 0.0;
+            ax[k] = fma(sc, dx, ax[k]);
+            ay[k] = fma(sc, dy, ay[k]);
+            az[k] = fma(sc, dz, az[k]);
+        }
+    }
+}
+
 // BJ: j-bodies per work unit (a row of bi = 256 I bodies against BJ j-bodies).  Narrow units (BJ 32
 // or 64) let a small system spread over every SM: at N = 1024 the 256-wide units give 8 CTAs.
 template <int I, int BJ = kThreads>
@@ -53,10 +78,11 @@ __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
         const int64_t jt0 = s - r * a.tiles;
         const int64_t row_end = min(e, (r + 1) * a.tiles);
         const int64_t jt1 = row_end - r * a.tiles;
+        const int64_t row0 = r * a.bi;
         double xi[I], yi[I], zi[I], ax[I], ay[I], az[I];
 #pragma unroll
         for (int k = 0; k < I; ++k) {
-            const int64_t i = r * a.bi + k * kThreads + t;
+            const int64_t i = row0 + k * kThreads + t;
             const double4 p = i < a.n ? a.src[i] : zero;
             xi[k] = p.x; yi[k] = p.y; zi[k] = p.z;
             ax[k] = 0.0; ay[k] = 0.0; az[k] = 0.0;
@@ -76,21 +102,13 @@ __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
                 const int64_t j = (jt + 1) * BJ + t;
                 if (j < a.n) qn = a.src[j];
             }
-#pragma unroll 4
-            for (int jj = 0; jj < BJ; ++jj) {
-                const double4 q = tile[cur][jj];
-#pragma unroll
-                for (int k = 0; k < I; ++k) {
-                    const double dx = q.x - xi[k], dy = q.y - yi[k], dz = q.z - zi[k];
-                    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-                    double inv = rsqrt(r2);
-                    inv = r2 > 0.0 ? inv : 0.0;
-                    const double sc = (q.w * inv) * (inv * inv);
-                    ax[k] = fma(sc, dx, ax[k]);
-                    ay[k] = fma(sc, dy, ay[k]);
-                    az[k] = fma(sc, dz, az[k]);
-                }
-            }
+            const int64_t j0 = jt * BJ;
+            // the self pair lies in this tile, or the tile ends in padding bodies (mass 0 at the origin)
+            const bool guard = (j0 < row0 + a.bi && row0 < j0 + BJ) || j0 + BJ > a.n;
+            if (guard)
+                f64_tile<I, BJ, true>(tile[cur], xi, yi, zi, ax, ay, az);
+            else
+                f64_tile<I, BJ, false>(tile[cur], xi, yi, zi, ax, ay, az);
             if (more && t < BJ) {
                 qn.w *= a.G;
                 tile[cur ^ 1][t] = qn;
@@ -118,6 +136,16 @@ __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
 // FP32x2 pipe (add/mul/fma .f32x2) with one MUFU rsqrt per pair; each i keeps FP32 partial sums
 // for FOLD j-bodies, then folds them into FP64 Kahan-compensated accumulators.  Tiles that
 // overlap the row (where i == j occurs) take the guarded path; all others run without a compare.
+//
+// Close pairs far from the frame centre.  Rounding X = x - c to FP32 moves each body by up to
+// 2^-24 |X|, so a pair at distance r gets a relative error of up to 2^-24 (|X_i| + |X_j|) / r
+// <= 2^-24 (2 |X_i| + r) / r: a pair 0.002 AU apart in a row whose centre is 1.3 AU away loses
+// ~5e-5 of its force.  The fast loop therefore keeps, per i-body, the smallest r^2 of the fold
+// (one FMNMX per pair, on the ALU pipe beside the FMA pipe).  A warp in which some i-body met a
+// pair with r^2 < near2 |X_i|^2 recomputes that fold with the coordinate differences taken from
+// the split X = hi + lo of both bodies, dx = (hi_j - hi_i) + (lo_j - lo_i), which carries only
+// the rounding of dx itself, and a Newton step on the rsqrt.  With near2 = (2 / (K - 1))^2 every
+// pair left on the fast path keeps its coordinate error below K 2^-24 relative.
 // -------------------------------------------------------------------------------------------
 __device__ __forceinline__ float rsqrt_approx(float x) {
     float y;
@@ -170,20 +198,85 @@ struct KahanAcc<I, true> {
     __device__ __forceinline__ double result(int d, int k) const { return sm[d][k][t] - sm[3 + d][k][t]; }
 };
 
+// The staged j-tile: FP32 coordinates relative to the row centre (hi), their FP32 remainders (lo,
+// read only on the precise path) and G m.
+struct MixedTile {
+    const float *x, *y, *z, *m, *lx, *ly, *lz;
+};
+
+// Precise recomputation of one fold (see above): coordinate differences from the hi/lo splits,
+// rsqrt refined by one Newton step y <- y (3 - r2 y^2) / 2.  Padding bodies (hi = 1e30, r2 = inf)
+// and the self pair (r2 = 0) contribute exactly zero.
+template <int I, int FOLD>
+__device__ __forceinline__ void mixed_fold_precise(const MixedTile &T, int q0, const float2 (&nx)[I],
+                                                   const float2 (&ny)[I], const float2 (&nz)[I],
+                                                   const float *__restrict__ ilo, float2 (&fx)[I], float2 (&fy)[I],
+                                                   float2 (&fz)[I]) {
+    const float2 *X = reinterpret_cast<const float2 *>(T.x);
+    const float2 *Y = reinterpret_cast<const float2 *>(T.y);
+    const float2 *Z = reinterpret_cast<const float2 *>(T.z);
+    const float2 *M = reinterpret_cast<const float2 *>(T.m);
+    const float2 *LX = reinterpret_cast<const float2 *>(T.lx);
+    const float2 *LY = reinterpret_cast<const float2 *>(T.ly);
+    const float2 *LZ = reinterpret_cast<const float2 *>(T.lz);
+    const int t = threadIdx.x;
+    float2 lx[I], ly[I], lz[I];
+#pragma unroll
+    for (int k = 0; k < I; ++k) {
+        const float a = -ilo[(0 * I + k) * kThreads + t], b = -ilo[(1 * I + k) * kThreads + t],
+                    c = -ilo[(2 * I + k) * kThreads + t];
+        lx[k] = make_float2(a, a);
+        ly[k] = make_float2(b, b);
+        lz[k] = make_float2(c, c);
+        fx[k] = fy[k] = fz[k] = make_float2(0.f, 0.f);
+    }
+    const float kInf = __int_as_float(0x7f800000);
+#pragma unroll 1
+    for (int u = 0; u < FOLD / 2; ++u) {
+        const float2 xj = X[q0 + u], yj = Y[q0 + u], zj = Z[q0 + u], mj = M[q0 + u];
+        const float2 lxj = LX[q0 + u], lyj = LY[q0 + u], lzj = LZ[q0 + u];
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            const float2 dx = __fadd2_rn(__fadd2_rn(xj, nx[k]), __fadd2_rn(lxj, lx[k]));
+            const float2 dy = __fadd2_rn(__fadd2_rn(yj, ny[k]), __fadd2_rn(lyj, ly[k]));
+            const float2 dz = __fadd2_rn(__fadd2_rn(zj, nz[k]), __fadd2_rn(lzj, lz[k]));
+            float2 r2 = __fmul2_rn(dx, dx);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dz, dz, r2);
+            float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+            const float2 h = __ffma2_rn(__fmul2_rn(make_float2(-0.5f, -0.5f), r2), __fmul2_rn(inv, inv),
+                                        make_float2(1.5f, 1.5f));
+            inv = __fmul2_rn(inv, h);
+            inv.x = (r2.x > 0.f && r2.x < kInf) ? inv.x : 0.f;
+            inv.y = (r2.y > 0.f && r2.y < kInf) ? inv.y : 0.f;
+            const float2 inv2 = __fmul2_rn(inv, inv);
+            float2 sc = __fmul2_rn(mj, inv);
+            sc = __fmul2_rn(sc, inv2);
+            fx[k] = __ffma2_rn(dx, sc, fx[k]);
+            fy[k] = __ffma2_rn(dy, sc, fy[k]);
+            fz[k] = __ffma2_rn(dz, sc, fz[k]);
+        }
+    }
+}
+
 template <int I, int FOLD, int U, bool kGuard, class Acc>
-__device__ __forceinline__ void mixed_tile(const float *__restrict__ tx, const float *__restrict__ ty,
-                                           const float *__restrict__ tz, const float *__restrict__ tm,
-                                           const float2 (&nx)[I], const float2 (&ny)[I], const float2 (&nz)[I],
-                                           Acc &acc) {
-    const float2 *X = reinterpret_cast<const float2 *>(tx);
-    const float2 *Y = reinterpret_cast<const float2 *>(ty);
-    const float2 *Z = reinterpret_cast<const float2 *>(tz);
-    const float2 *M = reinterpret_cast<const float2 *>(tm);
+__device__ __forceinline__ void mixed_tile(const MixedTile &T, const float2 (&nx)[I], const float2 (&ny)[I],
+                                           const float2 (&nz)[I], const float (&thr2)[I],
+                                           const float *__restrict__ ilo, Acc &acc) {
+    const float2 *X = reinterpret_cast<const float2 *>(T.x);
+    const float2 *Y = reinterpret_cast<const float2 *>(T.y);
+    const float2 *Z = reinterpret_cast<const float2 *>(T.z);
+    const float2 *M = reinterpret_cast<const float2 *>(T.m);
+    const float kInf = __int_as_float(0x7f800000);
 #pragma unroll 1
     for (int q0 = 0; q0 < kThreads / 2; q0 += FOLD / 2) {
         float2 fx[I], fy[I], fz[I];
+        float mn[I];
 #pragma unroll
-        for (int k = 0; k < I; ++k) fx[k] = fy[k] = fz[k] = make_float2(0.f, 0.f);
+        for (int k = 0; k < I; ++k) {
+            fx[k] = fy[k] = fz[k] = make_float2(0.f, 0.f);
+            mn[k] = kInf;
+        }
 #pragma unroll U
         for (int u = 0; u < FOLD / 2; ++u) {
             const float2 xj = X[q0 + u], yj = Y[q0 + u], zj = Z[q0 + u], mj = M[q0 + u];
@@ -199,6 +292,9 @@ __device__ __forceinline__ void mixed_tile(const float *__restrict__ tx, const f
                 if (kGuard) {
                     inv.x = r2.x > 0.f ? inv.x : 0.f;
                     inv.y = r2.y > 0.f ? inv.y : 0.f;
+                    mn[k] = fminf(mn[k], fminf(r2.x > 0.f ? r2.x : kInf, r2.y > 0.f ? r2.y : kInf));
+                } else {
+                    mn[k] = fminf(mn[k], fminf(r2.x, r2.y));
                 }
                 const float2 inv2 = __fmul2_rn(inv, inv);
                 float2 sc = __fmul2_rn(mj, inv);
@@ -208,6 +304,10 @@ __device__ __forceinline__ void mixed_tile(const float *__restrict__ tx, const f
                 fz[k] = __ffma2_rn(dz, sc, fz[k]);
             }
         }
+        bool near = false;
+#pragma unroll
+        for (int k = 0; k < I; ++k) near |= mn[k] < thr2[k];
+        if (__any_sync(0xffffffffu, near)) mixed_fold_precise<I, FOLD>(T, q0, nx, ny, nz, ilo, fx, fy, fz);
 #pragma unroll
         for (int k = 0; k < I; ++k) {
             acc.add(0, k, (double)fx[k].x + (double)fx[k].y);
@@ -217,18 +317,44 @@ __device__ __forceinline__ void mixed_tile(const float *__restrict__ tx, const f
     }
 }
 
+// One staged body: FP32 hi part of x - c, its FP32 remainder lo, and G m.  Padding bodies are far
+// away and massless, so their terms are exactly 0 on both paths.
+__device__ __forceinline__ void stage_body(bool have, const double4 &q, const double3 &c, double G, int slot,
+                                           float *hx, float *hy, float *hz, float *hm, float *lx, float *ly,
+                                           float *lz) {
+    if (have) {
+        const double ex = q.x - c.x, ey = q.y - c.y, ez = q.z - c.z;
+        const float fx = (float)ex, fy = (float)ey, fz = (float)ez;
+        hx[slot] = fx;
+        hy[slot] = fy;
+        hz[slot] = fz;
+        lx[slot] = (float)(ex - (double)fx);
+        ly[slot] = (float)(ey - (double)fy);
+        lz[slot] = (float)(ez - (double)fz);
+        hm[slot] = (float)(G * q.w);
+    } else {
+        const float kFar = 1e30f;
+        hx[slot] = hy[slot] = hz[slot] = kFar;
+        lx[slot] = ly[slot] = lz[slot] = 0.f;
+        hm[slot] = 0.f;
+    }
+}
+
 template <int I, int FOLD, int MINB, bool SMK, int U>
 __global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs a) {
     __shared__ __align__(16) float tx[2][kThreads];
     __shared__ __align__(16) float ty[2][kThreads];
     __shared__ __align__(16) float tz[2][kThreads];
     __shared__ __align__(16) float tm[2][kThreads];
-    __shared__ double cred[3][kThreads];
+    __shared__ __align__(16) float tlx[2][kThreads];
+    __shared__ __align__(16) float tly[2][kThreads];
+    __shared__ __align__(16) float tlz[2][kThreads];
+    __shared__ float ilo[3 * I * kThreads];  // lo parts of the row's bodies, [dim][k][thread]
+    __shared__ double cred[3][kThreads / 32];
     __shared__ double kah[SMK ? 6 : 1][SMK ? I : 1][SMK ? kThreads : 1];
     const int t = threadIdx.x;
     int64_t s, e;
     cta_range(a, blockIdx.x, s, e);
-    const float kFar = 1e30f;  // padding bodies: far away and massless, their terms are exactly 0
     while (s < e) {
         const int64_t r = s / a.tiles;
         const int64_t jt0 = s - r * a.tiles;
@@ -248,54 +374,62 @@ __global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs 
                 msx += p.x; msy += p.y; msz += p.z;
             }
         }
-        cred[0][t] = msx;
-        cred[1][t] = msy;
-        cred[2][t] = msz;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            msx += __shfl_xor_sync(0xffffffffu, msx, o);
+            msy += __shfl_xor_sync(0xffffffffu, msy, o);
+            msz += __shfl_xor_sync(0xffffffffu, msz, o);
+        }
+        if ((t & 31) == 0) {
+            cred[0][t >> 5] = msx;
+            cred[1][t >> 5] = msy;
+            cred[2][t >> 5] = msz;
+        }
         __syncthreads();
-        for (int w = kThreads / 2; w > 0; w >>= 1) {
-            if (t < w) {
-                cred[0][t] += cred[0][t + w];
-                cred[1][t] += cred[1][t + w];
-                cred[2][t] += cred[2][t + w];
-            }
-            __syncthreads();
+        double3 c = make_double3(0.0, 0.0, 0.0);
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) {
+            c.x += cred[0][w];
+            c.y += cred[1][w];
+            c.z += cred[2][w];
         }
         const double inv_rows = 1.0 / (double)min((int64_t)a.bi, a.n - row0);
-        const double3 c = make_double3(cred[0][0] * inv_rows, cred[1][0] * inv_rows, cred[2][0] * inv_rows);
+        c.x *= inv_rows;
+        c.y *= inv_rows;
+        c.z *= inv_rows;
         __syncthreads();
         float2 nx[I], ny[I], nz[I];
+        float thr2[I];
         KahanAcc<I, SMK> acc;
         if constexpr (SMK) acc.sm = kah;
         acc.init(t);
 #pragma unroll
         for (int k = 0; k < I; ++k) {
             const int64_t i = row0 + k * kThreads + t;
-            float fx = 0.f, fy = 0.f, fz = 0.f;
-            if (i < a.n) {
-                fx = (float)(px[k] - c.x);
-                fy = (float)(py[k] - c.y);
-                fz = (float)(pz[k] - c.z);
+            float fx = 0.f, fy = 0.f, fz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+            if (i < a.n) {  // padding i-bodies sit at the centre with a zero threshold
+                const double ex = px[k] - c.x, ey = py[k] - c.y, ez = pz[k] - c.z;
+                fx = (float)ex;
+                fy = (float)ey;
+                fz = (float)ez;
+                lx = (float)(ex - (double)fx);
+                ly = (float)(ey - (double)fy);
+                lz = (float)(ez - (double)fz);
             }
             nx[k] = make_float2(-fx, -fx);
             ny[k] = make_float2(-fy, -fy);
             nz[k] = make_float2(-fz, -fz);
+            ilo[(0 * I + k) * kThreads + t] = lx;
+            ilo[(1 * I + k) * kThreads + t] = ly;
+            ilo[(2 * I + k) * kThreads + t] = lz;
+            thr2[k] = a.near2 * fmaf(fz, fz, fmaf(fy, fy, fx * fx));
         }
-        auto stage = [&](int64_t jt, int buf) {
-            const int64_t j = jt * kThreads + t;
-            if (j < a.n) {
-                const double4 q = a.src[j];
-                tx[buf][t] = (float)(q.x - c.x);
-                ty[buf][t] = (float)(q.y - c.y);
-                tz[buf][t] = (float)(q.z - c.z);
-                tm[buf][t] = (float)(a.G * q.w);
-            } else {
-                tx[buf][t] = kFar;
-                ty[buf][t] = kFar;
-                tz[buf][t] = kFar;
-                tm[buf][t] = 0.f;
-            }
-        };
-        stage(jt0, 0);
+        {
+            const int64_t j = jt0 * kThreads + t;
+            const bool have = j < a.n;
+            stage_body(have, have ? a.src[j] : make_double4(0.0, 0.0, 0.0, 0.0), c, a.G, t, tx[0], ty[0], tz[0],
+                       tm[0], tlx[0], tly[0], tlz[0]);
+        }
         __syncthreads();
         int cur = 0;
         for (int64_t jt = jt0; jt < jt1; ++jt) {
@@ -311,23 +445,14 @@ __global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs 
             }
             const int64_t j0 = jt * kThreads;
             const bool diag = j0 < row0 + a.bi && row0 < j0 + kThreads;
+            const MixedTile T{tx[cur], ty[cur], tz[cur], tm[cur], tlx[cur], tly[cur], tlz[cur]};
             if (diag)
-                mixed_tile<I, FOLD, U, true>(tx[cur], ty[cur], tz[cur], tm[cur], nx, ny, nz, acc);
+                mixed_tile<I, FOLD, U, true>(T, nx, ny, nz, thr2, ilo, acc);
             else
-                mixed_tile<I, FOLD, U, false>(tx[cur], ty[cur], tz[cur], tm[cur], nx, ny, nz, acc);
+                mixed_tile<I, FOLD, U, false>(T, nx, ny, nz, thr2, ilo, acc);
             if (more) {
                 const int nb = cur ^ 1;
-                if (have) {
-                    tx[nb][t] = (float)(qn.x - c.x);
-                    ty[nb][t] = (float)(qn.y - c.y);
-                    tz[nb][t] = (float)(qn.z - c.z);
-                    tm[nb][t] = (float)(a.G * qn.w);
-                } else {
-                    tx[nb][t] = kFar;
-                    ty[nb][t] = kFar;
-                    tz[nb][t] = kFar;
-                    tm[nb][t] = 0.f;
-                }
+                stage_body(have, qn, c, a.G, t, tx[nb], ty[nb], tz[nb], tm[nb], tlx[nb], tly[nb], tlz[nb]);
             }
             __syncthreads();
             cur ^= 1;
@@ -449,6 +574,7 @@ ForcePlan make_plan(int64_t n, int precision, int device, int variant) {
     if (grid > p.total) grid = p.total > 0 ? p.total : 1;
     p.grid = (int)grid;
     p.slots = p.grid + p.rows;
+    p.near2 = near2_of(kDefaultNearFactor);
     return p;
 }
 
@@ -457,7 +583,7 @@ size_t partial_bytes(const ForcePlan &p) { return (size_t)p.slots * 3 * p.bi * s
 int launch_force(int precision, const ForcePlan &p, const double4 *src, double G, double *partials,
                  cudaStream_t s) {
     if (p.n == 0) return GTD_OK;
-    ForceKArgs a{p.n, p.rows, p.tiles, p.total, p.grid, p.bi, src, G, partials};
+    ForceKArgs a{p.n, p.rows, p.tiles, p.total, p.grid, p.bi, src, G, partials, p.near2};
     if (precision == GTD_PREC_MIXED)
         with_mixed(p.variant, [&](auto k) { k<<<p.grid, kThreads, 0, s>>>(a); });
     else
@@ -611,9 +737,7 @@ __global__ void __launch_bounds__(kFusedBodies * kFusedSlices * 32)
             const double gm = q.w * G;
             const double dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
             const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-            double inv = rsqrt(r2);
-            inv = r2 > 0.0 ? inv : 0.0;
-            const double sc = (gm * inv) * (inv * inv);
+            const double sc = r2 > 0.0 ? gm * inv_r3(r2) : 0.0;
             ax = fma(sc, dx, ax);
             ay = fma(sc, dy, ay);
             az = fma(sc, dz, az);

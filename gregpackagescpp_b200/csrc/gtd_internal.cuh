@@ -38,7 +38,15 @@ struct ForcePlan {
     int grid = 0;            // CTAs of the force kernel
     int64_t slots = 0;       // partial-sum slots (grid + rows)
     int variant = 0;         // kernel variant (i-bodies per thread, fold length)
+    float near2 = 0.f;       // mixed kernel: precise-path threshold, near2_of(near factor)
 };
+
+// Mixed kernel: a fold that holds a pair closer than 2 |X_i| / (K - 1) to one of its i-bodies (X_i:
+// the body's coordinates in its row's FP32 frame) is recomputed on the precise path, so that the
+// FP32 rounding of the coordinates costs no pair more than K 2^-24 of its relative accuracy.
+// K <= 1 turns the check off.
+constexpr double kDefaultNearFactor = 8.0;
+inline float near2_of(double k) { return k > 1.0 ? (float)((2.0 / (k - 1.0)) * (2.0 / (k - 1.0))) : 0.f; }
 
 // Per-thread launch shape of the two force kernels.
 constexpr int kThreads = 256;

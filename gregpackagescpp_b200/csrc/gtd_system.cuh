@@ -53,6 +53,7 @@ struct gtd_system {
     int plan_prec = -1;
     int variant = 0;              // force-kernel variant in use
     bool variant_pinned = false;  // set by gtd_system_set_direct_variant; else the process-wide choice
+    double near_factor = gtd::kDefaultNearFactor;  // mixed kernel's precise-path factor K
     double *partials = nullptr;
     size_t part_bytes = 0;
     double *escratch = nullptr;

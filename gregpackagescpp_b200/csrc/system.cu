@@ -110,9 +110,12 @@ void release_bodies(gtd_system *s) {
 
 int ensure_plan(gtd_system *s) {
     if (!s->variant_pinned) s->variant = tuned_variant(s->device, s->precision, s->n);
-    if (s->plan.n == s->n && s->plan_prec == s->precision && s->plan.variant == s->variant && s->partials)
+    if (s->plan.n == s->n && s->plan_prec == s->precision && s->plan.variant == s->variant && s->partials) {
+        s->plan.near2 = near2_of(s->near_factor);
         return GTD_OK;
+    }
     s->plan = make_plan(s->n, s->precision, s->device, s->variant);
+    s->plan.near2 = near2_of(s->near_factor);
     s->plan_prec = s->precision;
     const size_t need = partial_bytes(s->plan);
     if (need > s->part_bytes) {
@@ -721,6 +724,14 @@ int gtd_system_set_direct_variant(gtd_system *s, int variant) {
     if (variant >= variant_count(s->precision)) return fail(GTD_ERR_INVALID_ARGUMENT, "variant %d out of range", variant);
     s->variant_pinned = variant >= 0;
     if (variant >= 0) s->variant = variant;
+    return GTD_OK;
+}
+
+int gtd_system_set_mixed_near_factor(gtd_system *s, double k) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (!(k == k)) return fail(GTD_ERR_INVALID_ARGUMENT, "near factor is NaN");
+    s->near_factor = k;
+    s->plan.near2 = near2_of(k);
     return GTD_OK;
 }
 

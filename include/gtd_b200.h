@@ -263,6 +263,13 @@ GTD_API int gtd_direct_variant_count(int precision, int *count);
 GTD_API int gtd_direct_variant_info(int precision, int variant, int *i_per_thread, int *fold);
 GTD_API int gtd_system_set_direct_variant(gtd_system *sys, int variant);
 GTD_API int gtd_system_autotune_direct(gtd_system *sys, int reps, int *best, double *best_ms);
+/* Accuracy control of the mixed-precision direct sum (no counterpart in the reference, whose
+ * evolve is FP64 throughout; it bounds the error of the FP32 form of cumulative_acc,
+ * gregsys.hpp:352-357).  The FP32 pair terms use coordinates relative to a per-row centre; a
+ * pair closer than 2|X_i|/(k - 1) to body i (X_i its offset from that centre) would lose more
+ * than k 2^-24 of its relative accuracy to their rounding, so the j-range holding it is summed
+ * again from hi/lo coordinate splits.  Default k = 8; k <= 1 turns the check off. */
+GTD_API int gtd_system_set_mixed_near_factor(gtd_system *sys, double k);
 /* Measured throughput of a dependent-FMA microkernel on `device` (all SMs): precision
  * GTD_PREC_MIXED gives FP32 FFMA FLOP/s, GTD_PREC_F64 gives FP64 DFMA FLOP/s (2 flops per FMA). */
 GTD_API int gtd_measure_fma_peak(int device, int precision, double *flops_per_s);

@@ -10,6 +10,7 @@
 #include "nbody_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -55,6 +56,79 @@ void orc_direct_acc(int n, const double *m, const double *x3, const long double 
     memset(a3, 0, sizeof(double) * 3 * (size_t)n);
     for (int o = 0; o < n; ++o)
         for (int i = o + 1; i < n; ++i) pair_acc(x3 + 3 * o, x3 + 3 * i, m[o], m[i], G, a3 + 3 * o, a3 + 3 * i);
+}
+
+/* orc_direct_acc restricted to the bodies rows[0..nrows): each row's acceleration is summed over
+ * the other bodies in ascending index order, with pair_acc's arithmetic for that body's side of
+ * each pair (a_i -= s r for the pairs (o < i) where the reference updates i as the second body,
+ * a_i += s r for o > i), so the rows agree bit for bit with orc_direct_acc.  gross (optional)
+ * receives sum_j |G m_j / r^2| per row, the scale of FP rounding in a summed force.  Rows are
+ * split over `threads` pthreads. */
+typedef struct {
+    int n, lo, hi;
+    const double *m, *x3;
+    ld G;
+    const int32_t *rows;
+    double *a3, *gross;
+} rows_job;
+
+static void *rows_worker(void *arg) {
+    const rows_job *J = (const rows_job *)arg;
+    for (int q = J->lo; q < J->hi; ++q) {
+        const int i = J->rows[q];
+        const double *xi = J->x3 + 3 * i;
+        double a[3] = {0.0, 0.0, 0.0};
+        ld g = 0.0L;
+        for (int o = 0; o < J->n; ++o) {
+            if (o == i) continue;
+            const double *xo = J->x3 + 3 * o;
+            if (o < i) { /* pair (o, i): r12 = x_i - x_o, body i is the second body */
+                double rx = xi[0] - xo[0], ry = xi[1] - xo[1], rz = xi[2] - xo[2];
+                double r2 = rx * rx + ry * ry + rz * rz;
+                ld r3 = mag_ld(r2 * rx, r2 * ry, r2 * rz);
+                ld sj = (J->G * (ld)J->m[o]) / r3;
+                a[0] = (double)((ld)a[0] - sj * (ld)rx);
+                a[1] = (double)((ld)a[1] - sj * (ld)ry);
+                a[2] = (double)((ld)a[2] - sj * (ld)rz);
+                g += (J->G * (ld)J->m[o]) / (ld)r2;
+            } else { /* pair (i, o): r12 = x_o - x_i, body i is the first body */
+                double rx = xo[0] - xi[0], ry = xo[1] - xi[1], rz = xo[2] - xi[2];
+                double r2 = rx * rx + ry * ry + rz * rz;
+                ld r3 = mag_ld(r2 * rx, r2 * ry, r2 * rz);
+                ld si = (J->G * (ld)J->m[o]) / r3;
+                a[0] = (double)((ld)a[0] + si * (ld)rx);
+                a[1] = (double)((ld)a[1] + si * (ld)ry);
+                a[2] = (double)((ld)a[2] + si * (ld)rz);
+                g += (J->G * (ld)J->m[o]) / (ld)r2;
+            }
+        }
+        J->a3[3 * q] = a[0];
+        J->a3[3 * q + 1] = a[1];
+        J->a3[3 * q + 2] = a[2];
+        if (J->gross) J->gross[q] = (double)g;
+    }
+    return NULL;
+}
+
+void orc_direct_acc_rows(int n, const double *m, const double *x3, const long double *Gp, const int32_t *rows,
+                         int nrows, double *a3, double *gross, int threads) {
+    enum { kMaxThreads = 256 };
+    if (threads > nrows) threads = nrows;
+    if (threads > kMaxThreads) threads = kMaxThreads;
+    if (threads < 1) threads = 1;
+    pthread_t tid[kMaxThreads];
+    rows_job job[kMaxThreads];
+    int started[kMaxThreads];
+    for (int k = 0; k < threads; ++k) {
+        job[k] = (rows_job){n, (int)((long)nrows * k / threads), (int)((long)nrows * (k + 1) / threads), m, x3, *Gp,
+                            rows, a3, gross};
+        started[k] = k > 0 && pthread_create(&tid[k], NULL, rows_worker, &job[k]) == 0;
+    }
+    rows_worker(&job[0]);
+    for (int k = 1; k < threads; ++k) {
+        if (started[k]) pthread_join(tid[k], NULL);
+        else rows_worker(&job[k]); /* a thread that could not start: its rows run here */
+    }
 }
 
 /* x += s * y with s long double and the sum rounded into double (vector3D += vector3D<long double>) */

@@ -32,6 +32,12 @@ void orc_G_units_into(uint64_t m_first, uint64_t m_second, uint64_t d_first, uin
  * a3 is zeroed first (MEM_LOOP, gregsys.hpp:107-122). */
 void orc_direct_acc(int n, const double *m, const double *x3, const long double *G, double *a3);
 
+/* orc_direct_acc for the bodies rows[0..nrows) only (bit for bit the same values), with
+ * gross[q] = sum_j G m_j / r^2 for each row when gross is not NULL; rows are split over
+ * `threads` pthreads.  a3 and gross are indexed by position in rows. */
+void orc_direct_acc_rows(int n, const double *m, const double *x3, const long double *G, const int32_t *rows,
+                         int nrows, double *a3, double *gross, int threads);
+
 /* gtd::system::evolve for the direct-summation methods (gregsys.hpp:2593-3071).  State is updated
  * in place; a3 holds the final accelerations as the reference leaves them.  coll is 0 or 3
  * (s_coll restitution, gregsys.hpp:690-914).  Returns 0, or -1 for an unsupported method. */

@@ -68,6 +68,8 @@ class Oracle:
         L.orc_G_units.argtypes = [C.c_uint64] * 6
         L.orc_G_units_into.argtypes = [C.c_uint64] * 6 + [C.POINTER(C.c_longdouble)]
         L.orc_direct_acc.argtypes = [C.c_int, _dp, _dp, C.POINTER(C.c_longdouble), _dp]
+        L.orc_direct_acc_rows.argtypes = [C.c_int, _dp, _dp, C.POINTER(C.c_longdouble), _ip, C.c_int, _dp,
+                                          C.c_void_p, C.c_int]
         L.orc_evolve.restype = C.c_int
         L.orc_evolve.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_longdouble,
                                  C.c_uint64, C.POINTER(C.c_longdouble)]
@@ -116,6 +118,16 @@ class Oracle:
         a = np.zeros(3 * n)
         self.lib.orc_direct_acc(n, _c3(m), _c3(x), C.byref(G), a)
         return a.reshape(n, 3)
+
+    def direct_acc_rows(self, m, x, G, rows, threads=1):
+        """orc_direct_acc for the bodies `rows` only (the same bits), and per row the scale
+        sum_j G m_j / r_ij^2 of the summed force.  Returns (a[len(rows), 3], gross[len(rows)])."""
+        rows = np.ascontiguousarray(np.asarray(rows, dtype=np.int32))
+        a = np.zeros(3 * len(rows))
+        gross = np.zeros(len(rows))
+        self.lib.orc_direct_acc_rows(len(m), _c3(m), _c3(x), C.byref(G), rows, len(rows), a,
+                                     gross.ctypes.data, int(threads))
+        return a.reshape(-1, 3), gross
 
     def evolve(self, method, m, x, v, dt, steps, G, r=None, rest=None, coll=0):
         n = len(m)
