@@ -29,6 +29,8 @@ struct ForceKArgs {
     double G;
     double *part;
     float near2;  // mixed kernel: a pair with r^2 < near2 |X_i|^2 sends its fold to the precise path
+    int64_t segs, seg_tiles, units;  // mixed kernel's work queue (ForcePlan)
+    unsigned *queue;                 // its counter, zeroed before each launch
 };
 
 __device__ __forceinline__ void cta_range(const ForceKArgs &a, int g, int64_t &s, int64_t &e) {
@@ -140,12 +142,13 @@ __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
 // Close pairs far from the frame centre.  Rounding X = x - c to FP32 moves each body by up to
 // 2^-24 |X|, so a pair at distance r gets a relative error of up to 2^-24 (|X_i| + |X_j|) / r
 // <= 2^-24 (2 |X_i| + r) / r: a pair 0.002 AU apart in a row whose centre is 1.3 AU away loses
-// ~5e-5 of its force.  The fast loop therefore keeps, per i-body, the smallest r^2 of the fold
-// (one FMNMX per pair, on the ALU pipe beside the FMA pipe).  A warp in which some i-body met a
-// pair with r^2 < near2 |X_i|^2 recomputes that fold with the coordinate differences taken from
-// the split X = hi + lo of both bodies, dx = (hi_j - hi_i) + (lo_j - lo_i), which carries only
-// the rounding of dx itself, and a Newton step on the rsqrt.  With near2 = (2 / (K - 1))^2 every
-// pair left on the fast path keeps its coordinate error below K 2^-24 relative.
+// ~5e-5 of its force.  Every staged tile therefore carries the FP32 remainders lo = X - hi of its
+// coordinates and the bounding box of each warp's 32 bodies; each warp of i-bodies (32 I bodies
+// consecutive in the spatial order) knows its box and its largest threshold near2 |X_i|^2.  A fold
+// whose j-box comes closer to the warp's i-box than that threshold is summed on the precise path,
+// dx = (hi_j - hi_i) + (lo_j - lo_i), which carries only the rounding of dx itself; every other
+// fold provably holds no pair with r^2 < near2 |X_i|^2.  With near2 = (2 / (K - 1))^2 every pair
+// on the fast path keeps its coordinate error below K 2^-24 relative.
 // -------------------------------------------------------------------------------------------
 __device__ __forceinline__ float rsqrt_approx(float x) {
     float y;
@@ -199,56 +202,78 @@ struct KahanAcc<I, true> {
 };
 
 // The staged j-tile: FP32 coordinates relative to the row centre (hi), their FP32 remainders (lo,
-// read only on the precise path) and G m.
+// read only on the precise path), G m, and the bounding box of each warp's 32 staged bodies.
 struct MixedTile {
     const float *x, *y, *z, *m, *lx, *ly, *lz;
+    const float *box;  // [kThreads / 32][6]: lo xyz, hi xyz
 };
 
-// Precise recomputation of one fold (see above): coordinate differences from the hi/lo splits,
-// rsqrt refined by one Newton step y <- y (3 - r2 y^2) / 2.  Padding bodies (hi = 1e30, r2 = inf)
-// and the self pair (r2 = 0) contribute exactly zero.
-template <int I, int FOLD>
-__device__ __forceinline__ void mixed_fold_precise(const MixedTile &T, int q0, const float2 (&nx)[I],
-                                                   const float2 (&ny)[I], const float2 (&nz)[I],
-                                                   const float *__restrict__ ilo, float2 (&fx)[I], float2 (&fy)[I],
-                                                   float2 (&fz)[I]) {
-    const float2 *X = reinterpret_cast<const float2 *>(T.x);
-    const float2 *Y = reinterpret_cast<const float2 *>(T.y);
-    const float2 *Z = reinterpret_cast<const float2 *>(T.z);
-    const float2 *M = reinterpret_cast<const float2 *>(T.m);
-    const float2 *LX = reinterpret_cast<const float2 *>(T.lx);
-    const float2 *LY = reinterpret_cast<const float2 *>(T.ly);
-    const float2 *LZ = reinterpret_cast<const float2 *>(T.lz);
-    const int t = threadIdx.x;
+// Order-preserving map of a float onto an unsigned int, so that warp minima and maxima of floats
+// are single REDUX operations (__reduce_min_sync / __reduce_max_sync).
+__device__ __forceinline__ unsigned f2key(float f) {
+    const unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key2f(unsigned k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+__device__ __forceinline__ float warp_minf(float v) { return key2f(__reduce_min_sync(0xffffffffu, f2key(v))); }
+__device__ __forceinline__ float warp_maxf(float v) { return key2f(__reduce_max_sync(0xffffffffu, f2key(v))); }
+
+// The loop over j-pairs [u0, u0 + LEN) of a staged tile.  kPrecise: the coordinate differences are
+// taken from the hi/lo splits, dx = (hi_j - hi_i) + (lo_j - lo_i), which carries only the rounding
+// of dx itself (three more packed adds per coordinate and pair of j-bodies); otherwise dx = hi_j -
+// hi_i.  Padding bodies (hi = 1e30, r2 = inf) contribute 0 on both paths.
+template <int I, int LEN, int U, bool kGuard, bool kPrecise>
+__device__ __forceinline__ void mixed_span(const MixedTile &T, int u0, const float2 (&nx)[I], const float2 (&ny)[I],
+                                           const float2 (&nz)[I], const float *__restrict__ ilo, float2 (&fx)[I],
+                                           float2 (&fy)[I], float2 (&fz)[I]) {
+    const float2 *X = reinterpret_cast<const float2 *>(T.x) + u0;
+    const float2 *Y = reinterpret_cast<const float2 *>(T.y) + u0;
+    const float2 *Z = reinterpret_cast<const float2 *>(T.z) + u0;
+    const float2 *M = reinterpret_cast<const float2 *>(T.m) + u0;
+    const float2 *LX = reinterpret_cast<const float2 *>(T.lx) + u0;
+    const float2 *LY = reinterpret_cast<const float2 *>(T.ly) + u0;
+    const float2 *LZ = reinterpret_cast<const float2 *>(T.lz) + u0;
     float2 lx[I], ly[I], lz[I];
-#pragma unroll
-    for (int k = 0; k < I; ++k) {
-        const float a = -ilo[(0 * I + k) * kThreads + t], b = -ilo[(1 * I + k) * kThreads + t],
-                    c = -ilo[(2 * I + k) * kThreads + t];
-        lx[k] = make_float2(a, a);
-        ly[k] = make_float2(b, b);
-        lz[k] = make_float2(c, c);
-        fx[k] = fy[k] = fz[k] = make_float2(0.f, 0.f);
-    }
-    const float kInf = __int_as_float(0x7f800000);
-#pragma unroll 1
-    for (int u = 0; u < FOLD / 2; ++u) {
-        const float2 xj = X[q0 + u], yj = Y[q0 + u], zj = Z[q0 + u], mj = M[q0 + u];
-        const float2 lxj = LX[q0 + u], lyj = LY[q0 + u], lzj = LZ[q0 + u];
+    if (kPrecise) {
+        const int t = threadIdx.x;
 #pragma unroll
         for (int k = 0; k < I; ++k) {
-            const float2 dx = __fadd2_rn(__fadd2_rn(xj, nx[k]), __fadd2_rn(lxj, lx[k]));
-            const float2 dy = __fadd2_rn(__fadd2_rn(yj, ny[k]), __fadd2_rn(lyj, ly[k]));
-            const float2 dz = __fadd2_rn(__fadd2_rn(zj, nz[k]), __fadd2_rn(lzj, lz[k]));
+            const float a = -ilo[(0 * I + k) * kThreads + t], b = -ilo[(1 * I + k) * kThreads + t],
+                        c = -ilo[(2 * I + k) * kThreads + t];
+            lx[k] = make_float2(a, a);
+            ly[k] = make_float2(b, b);
+            lz[k] = make_float2(c, c);
+        }
+    }
+#pragma unroll U
+    for (int u = 0; u < LEN; ++u) {
+        const float2 xj = X[u], yj = Y[u], zj = Z[u], mj = M[u];
+        float2 lxj, lyj, lzj;
+        if (kPrecise) {
+            lxj = LX[u];
+            lyj = LY[u];
+            lzj = LZ[u];
+        }
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            float2 dx = __fadd2_rn(xj, nx[k]);
+            float2 dy = __fadd2_rn(yj, ny[k]);
+            float2 dz = __fadd2_rn(zj, nz[k]);
+            if (kPrecise) {
+                dx = __fadd2_rn(dx, __fadd2_rn(lxj, lx[k]));
+                dy = __fadd2_rn(dy, __fadd2_rn(lyj, ly[k]));
+                dz = __fadd2_rn(dz, __fadd2_rn(lzj, lz[k]));
+            }
             float2 r2 = __fmul2_rn(dx, dx);
             r2 = __ffma2_rn(dy, dy, r2);
             r2 = __ffma2_rn(dz, dz, r2);
             float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-            const float2 h = __ffma2_rn(__fmul2_rn(make_float2(-0.5f, -0.5f), r2), __fmul2_rn(inv, inv),
-                                        make_float2(1.5f, 1.5f));
-            inv = __fmul2_rn(inv, h);
-            inv.x = (r2.x > 0.f && r2.x < kInf) ? inv.x : 0.f;
-            inv.y = (r2.y > 0.f && r2.y < kInf) ? inv.y : 0.f;
+            if (kGuard) {
+                inv.x = r2.x > 0.f ? inv.x : 0.f;
+                inv.y = r2.y > 0.f ? inv.y : 0.f;
+            }
             const float2 inv2 = __fmul2_rn(inv, inv);
             float2 sc = __fmul2_rn(mj, inv);
             sc = __fmul2_rn(sc, inv2);
@@ -259,55 +284,38 @@ __device__ __forceinline__ void mixed_fold_precise(const MixedTile &T, int q0, c
     }
 }
 
+// One staged tile against the thread's I i-bodies, in folds of FOLD j-bodies.  Before each fold,
+// the bounding boxes of the warp's i-bodies (iw: lo xyz, hi xyz, and the warp's largest threshold
+// near2 |X_i|^2) and of the fold's j-bodies decide whether any pair of the two can be closer than
+// its threshold; such a fold runs on the precise path, every other one on the fast path.
 template <int I, int FOLD, int U, bool kGuard, class Acc>
 __device__ __forceinline__ void mixed_tile(const MixedTile &T, const float2 (&nx)[I], const float2 (&ny)[I],
-                                           const float2 (&nz)[I], const float (&thr2)[I],
-                                           const float *__restrict__ ilo, Acc &acc) {
-    const float2 *X = reinterpret_cast<const float2 *>(T.x);
-    const float2 *Y = reinterpret_cast<const float2 *>(T.y);
-    const float2 *Z = reinterpret_cast<const float2 *>(T.z);
-    const float2 *M = reinterpret_cast<const float2 *>(T.m);
-    const float kInf = __int_as_float(0x7f800000);
+                                           const float2 (&nz)[I], const float *__restrict__ ilo,
+                                           const float *__restrict__ iw, Acc &acc) {
+    constexpr int kFoldWarps = FOLD / 32;
 #pragma unroll 1
     for (int q0 = 0; q0 < kThreads / 2; q0 += FOLD / 2) {
         float2 fx[I], fy[I], fz[I];
-        float mn[I];
 #pragma unroll
-        for (int k = 0; k < I; ++k) {
-            fx[k] = fy[k] = fz[k] = make_float2(0.f, 0.f);
-            mn[k] = kInf;
-        }
-#pragma unroll U
-        for (int u = 0; u < FOLD / 2; ++u) {
-            const float2 xj = X[q0 + u], yj = Y[q0 + u], zj = Z[q0 + u], mj = M[q0 + u];
+        for (int k = 0; k < I; ++k) fx[k] = fy[k] = fz[k] = make_float2(0.f, 0.f);
+        // smallest possible squared distance between the warp's i-bodies and the fold's j-bodies
+        const float *cb = T.box + (q0 / (FOLD / 2)) * kFoldWarps * 6;
+        float g2 = 0.f;
 #pragma unroll
-            for (int k = 0; k < I; ++k) {
-                const float2 dx = __fadd2_rn(xj, nx[k]);
-                const float2 dy = __fadd2_rn(yj, ny[k]);
-                const float2 dz = __fadd2_rn(zj, nz[k]);
-                float2 r2 = __fmul2_rn(dx, dx);
-                r2 = __ffma2_rn(dy, dy, r2);
-                r2 = __ffma2_rn(dz, dz, r2);
-                float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                if (kGuard) {
-                    inv.x = r2.x > 0.f ? inv.x : 0.f;
-                    inv.y = r2.y > 0.f ? inv.y : 0.f;
-                    mn[k] = fminf(mn[k], fminf(r2.x > 0.f ? r2.x : kInf, r2.y > 0.f ? r2.y : kInf));
-                } else {
-                    mn[k] = fminf(mn[k], fminf(r2.x, r2.y));
-                }
-                const float2 inv2 = __fmul2_rn(inv, inv);
-                float2 sc = __fmul2_rn(mj, inv);
-                sc = __fmul2_rn(sc, inv2);
-                fx[k] = __ffma2_rn(dx, sc, fx[k]);
-                fy[k] = __ffma2_rn(dy, sc, fy[k]);
-                fz[k] = __ffma2_rn(dz, sc, fz[k]);
+        for (int d = 0; d < 3; ++d) {
+            float lo = cb[d], hi = cb[3 + d];
+#pragma unroll
+            for (int w = 1; w < kFoldWarps; ++w) {
+                lo = fminf(lo, cb[w * 6 + d]);
+                hi = fmaxf(hi, cb[w * 6 + 3 + d]);
             }
+            const float g = fmaxf(0.f, fmaxf(lo - iw[3 + d], iw[d] - hi));
+            g2 = fmaf(g, g, g2);
         }
-        bool near = false;
-#pragma unroll
-        for (int k = 0; k < I; ++k) near |= mn[k] < thr2[k];
-        if (__any_sync(0xffffffffu, near)) mixed_fold_precise<I, FOLD>(T, q0, nx, ny, nz, ilo, fx, fy, fz);
+        if (g2 < iw[6])
+            mixed_span<I, FOLD / 2, U, kGuard, true>(T, q0, nx, ny, nz, ilo, fx, fy, fz);
+        else
+            mixed_span<I, FOLD / 2, U, kGuard, false>(T, q0, nx, ny, nz, ilo, fx, fy, fz);
 #pragma unroll
         for (int k = 0; k < I; ++k) {
             acc.add(0, k, (double)fx[k].x + (double)fx[k].y);
@@ -340,6 +348,21 @@ __device__ __forceinline__ void stage_body(bool have, const double4 &q, const do
     }
 }
 
+// Bounding box of the 32 bodies a warp just staged (padding bodies left out), written by lane 0 to
+// box[warp][6] of the buffer.  Every lane of the warp calls it.
+__device__ __forceinline__ void stage_box(bool have, const float *hx, const float *hy, const float *hz, int slot,
+                                          float *box) {
+    const float kInf = __int_as_float(0x7f800000);
+    const float x = hx[slot], y = hy[slot], z = hz[slot];
+    const float lx = warp_minf(have ? x : kInf), ly = warp_minf(have ? y : kInf), lz = warp_minf(have ? z : kInf);
+    const float ux = warp_maxf(have ? x : -kInf), uy = warp_maxf(have ? y : -kInf), uz = warp_maxf(have ? z : -kInf);
+    if ((threadIdx.x & 31) == 0) {
+        float *b = box + (threadIdx.x >> 5) * 6;
+        b[0] = lx; b[1] = ly; b[2] = lz;
+        b[3] = ux; b[4] = uy; b[5] = uz;
+    }
+}
+
 template <int I, int FOLD, int MINB, bool SMK, int U>
 __global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs a) {
     __shared__ __align__(16) float tx[2][kThreads];
@@ -350,23 +373,29 @@ __global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs 
     __shared__ __align__(16) float tly[2][kThreads];
     __shared__ __align__(16) float tlz[2][kThreads];
     __shared__ float ilo[3 * I * kThreads];  // lo parts of the row's bodies, [dim][k][thread]
+    __shared__ float jbox[2][kThreads / 32 * 6];  // per staged warp of j-bodies: lo xyz, hi xyz
+    __shared__ float ibox[kThreads / 32][7];      // per warp of i-bodies: lo xyz, hi xyz, max threshold
     __shared__ double cred[3][kThreads / 32];
     __shared__ double kah[SMK ? 6 : 1][SMK ? I : 1][SMK ? kThreads : 1];
+    __shared__ int64_t unit_sh;
     const int t = threadIdx.x;
-    int64_t s, e;
-    cta_range(a, blockIdx.x, s, e);
-    while (s < e) {
-        const int64_t r = s / a.tiles;
-        const int64_t jt0 = s - r * a.tiles;
-        const int64_t row_end = min(e, (r + 1) * a.tiles);
-        const int64_t jt1 = row_end - r * a.tiles;
+    // Work queue: units (row r, segment) are taken in turn, so that CTAs whose rows hold more
+    // precise-path folds take fewer units; each unit writes its own partial-sum slot.
+    for (;;) {
+        if (t == 0) unit_sh = (int64_t)atomicAdd(a.queue, 1u);
+        __syncthreads();
+        const int64_t unit = unit_sh;
+        if (unit >= a.units) break;
+        const int64_t r = unit / a.segs;
+        const int64_t jt0 = (unit - r * a.segs) * a.seg_tiles;
+        const int64_t jt1 = min(jt0 + a.seg_tiles, a.tiles);
         const int64_t row0 = r * a.bi;
         // the row's FP32 frame is centred on the mean position of its bodies
         double px[I], py[I], pz[I];
         double msx = 0.0, msy = 0.0, msz = 0.0;
 #pragma unroll
         for (int k = 0; k < I; ++k) {
-            const int64_t i = row0 + k * kThreads + t;
+            const int64_t i = row0 + t * I + k;  // a warp holds 32 I consecutive bodies
             px[k] = py[k] = pz[k] = 0.0;
             if (i < a.n) {
                 const double4 p = a.src[i];
@@ -399,13 +428,14 @@ __global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs 
         c.z *= inv_rows;
         __syncthreads();
         float2 nx[I], ny[I], nz[I];
-        float thr2[I];
+        const float kInf = __int_as_float(0x7f800000);
+        float blo[3] = {kInf, kInf, kInf}, bhi[3] = {-kInf, -kInf, -kInf}, bth = 0.f;
         KahanAcc<I, SMK> acc;
         if constexpr (SMK) acc.sm = kah;
         acc.init(t);
 #pragma unroll
         for (int k = 0; k < I; ++k) {
-            const int64_t i = row0 + k * kThreads + t;
+            const int64_t i = row0 + t * I + k;  // a warp holds 32 I consecutive bodies
             float fx = 0.f, fy = 0.f, fz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
             if (i < a.n) {  // padding i-bodies sit at the centre with a zero threshold
                 const double ex = px[k] - c.x, ey = py[k] - c.y, ez = pz[k] - c.z;
@@ -422,13 +452,30 @@ __global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs 
             ilo[(0 * I + k) * kThreads + t] = lx;
             ilo[(1 * I + k) * kThreads + t] = ly;
             ilo[(2 * I + k) * kThreads + t] = lz;
-            thr2[k] = a.near2 * fmaf(fz, fz, fmaf(fy, fy, fx * fx));
+            const bool real = i < a.n;
+            blo[0] = fminf(blo[0], real ? fx : kInf);
+            blo[1] = fminf(blo[1], real ? fy : kInf);
+            blo[2] = fminf(blo[2], real ? fz : kInf);
+            bhi[0] = fmaxf(bhi[0], real ? fx : -kInf);
+            bhi[1] = fmaxf(bhi[1], real ? fy : -kInf);
+            bhi[2] = fmaxf(bhi[2], real ? fz : -kInf);
+            bth = fmaxf(bth, a.near2 * fmaf(fz, fz, fmaf(fy, fy, fx * fx)));
+        }
+        {
+            const float v0 = warp_minf(blo[0]), v1 = warp_minf(blo[1]), v2 = warp_minf(blo[2]);
+            const float v3 = warp_maxf(bhi[0]), v4 = warp_maxf(bhi[1]), v5 = warp_maxf(bhi[2]);
+            const float v6 = warp_maxf(bth);
+            if ((t & 31) == 0) {
+                float *b = ibox[t >> 5];
+                b[0] = v0; b[1] = v1; b[2] = v2; b[3] = v3; b[4] = v4; b[5] = v5; b[6] = v6;
+            }
         }
         {
             const int64_t j = jt0 * kThreads + t;
             const bool have = j < a.n;
             stage_body(have, have ? a.src[j] : make_double4(0.0, 0.0, 0.0, 0.0), c, a.G, t, tx[0], ty[0], tz[0],
                        tm[0], tlx[0], tly[0], tlz[0]);
+            stage_box(have, tx[0], ty[0], tz[0], t, jbox[0]);
         }
         __syncthreads();
         int cur = 0;
@@ -445,28 +492,29 @@ __global__ void __launch_bounds__(kThreads, MINB) force_mixed_kernel(ForceKArgs 
             }
             const int64_t j0 = jt * kThreads;
             const bool diag = j0 < row0 + a.bi && row0 < j0 + kThreads;
-            const MixedTile T{tx[cur], ty[cur], tz[cur], tm[cur], tlx[cur], tly[cur], tlz[cur]};
+            const MixedTile T{tx[cur], ty[cur], tz[cur], tm[cur], tlx[cur], tly[cur], tlz[cur], jbox[cur]};
+            const float *iw = ibox[t >> 5];
             if (diag)
-                mixed_tile<I, FOLD, U, true>(T, nx, ny, nz, thr2, ilo, acc);
+                mixed_tile<I, FOLD, U, true>(T, nx, ny, nz, ilo, iw, acc);
             else
-                mixed_tile<I, FOLD, U, false>(T, nx, ny, nz, thr2, ilo, acc);
+                mixed_tile<I, FOLD, U, false>(T, nx, ny, nz, ilo, iw, acc);
             if (more) {
                 const int nb = cur ^ 1;
                 stage_body(have, qn, c, a.G, t, tx[nb], ty[nb], tz[nb], tm[nb], tlx[nb], tly[nb], tlz[nb]);
+                stage_box(have, tx[nb], ty[nb], tz[nb], t, jbox[nb]);
             }
             __syncthreads();
             cur ^= 1;
         }
-        double *slot = a.part + (size_t)(blockIdx.x + r) * 3 * a.bi;
+        double *slot = a.part + (size_t)unit * 3 * a.bi;
 #pragma unroll
         for (int k = 0; k < I; ++k) {
-            const int l = k * kThreads + t;
+            const int l = t * I + k;
             slot[l] = acc.result(0, k);
             slot[a.bi + l] = acc.result(1, k);
             slot[2 * a.bi + l] = acc.result(2, k);
         }
-        s = row_end;
-        __syncthreads();
+        __syncthreads();  // also orders every read of unit_sh before thread 0 takes the next unit
     }
 }
 
@@ -481,8 +529,8 @@ struct VariantInfo {
     int bj = kThreads;  // j-bodies per work unit
 };
 // mixed: {I, FOLD}; the launch bound (blocks per SM) and where the Kahan sums live are in with_mixed
-static const VariantInfo kMixedVariants[] = {{2, 64}, {4, 128}, {2, 64}, {2, 128}, {2, 64},
-                                             {2, 128}, {1, 64},  {2, 64},  {4, 128}};
+static const VariantInfo kMixedVariants[] = {{2, 64}, {4, 128}, {2, 128}, {2, 128}, {1, 64},
+                                             {4, 64}, {2, 64},  {2, 64},  {4, 128}};
 static const VariantInfo kF64Variants[] = {{2, 0}, {1, 0}, {4, 0}, {1, 0, 64}, {1, 0, 32}};
 constexpr int kNumMixed = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
 constexpr int kNumF64 = sizeof(kF64Variants) / sizeof(kF64Variants[0]);
@@ -531,11 +579,11 @@ template <typename F>
 static void with_mixed(int v, F &&f) {
     switch (v) {
         case 1: f(force_mixed_kernel<4, 128, 1, false, 8>); break;
-        case 2: f(force_mixed_kernel<2, 64, 3, true, 4>); break;
-        case 3: f(force_mixed_kernel<2, 128, 3, true, 4>); break;
-        case 4: f(force_mixed_kernel<2, 64, 4, true, 2>); break;
-        case 5: f(force_mixed_kernel<2, 128, 4, true, 2>); break;
-        case 6: f(force_mixed_kernel<1, 64, 4, true, 4>); break;
+        case 2: f(force_mixed_kernel<2, 128, 2, false, 4>); break;
+        case 3: f(force_mixed_kernel<2, 128, 2, false, 8>); break;
+        case 4: f(force_mixed_kernel<1, 64, 3, false, 4>); break;
+        case 5: f(force_mixed_kernel<4, 64, 1, false, 4>); break;
+        case 6: f(force_mixed_kernel<2, 64, 2, true, 4>); break;
         case 7: f(force_mixed_kernel<2, 64, 2, false, 4>); break;
         case 8: f(force_mixed_kernel<4, 128, 1, false, 4>); break;
         default: f(force_mixed_kernel<2, 64, 2, false, 8>); break;
@@ -551,6 +599,14 @@ static void with_f64(int v, F &&f) {
         case 4: f(force_f64_kernel<1, 32>); break;
         default: f(force_f64_kernel<2>); break;
     }
+}
+
+// Cuts each row's tiles into at most `segs` segments of equal tile count.
+static void set_segments(ForcePlan &p, int64_t segs) {
+    p.seg_tiles = (p.tiles + segs - 1) / segs;
+    p.segs = (p.tiles + p.seg_tiles - 1) / p.seg_tiles;
+    p.units = p.rows * p.segs;
+    p.slots = p.units;
 }
 
 ForcePlan make_plan(int64_t n, int precision, int device, int variant) {
@@ -571,21 +627,61 @@ ForcePlan make_plan(int64_t n, int precision, int device, int variant) {
         with_f64(p.variant, [&](auto k) { cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, 0); });
     if (per_sm < 1) per_sm = 1;
     int64_t grid = (int64_t)sms * per_sm;
-    if (grid > p.total) grid = p.total > 0 ? p.total : 1;
-    p.grid = (int)grid;
-    p.slots = p.grid + p.rows;
+    if (precision == GTD_PREC_MIXED) {
+        // about 32 units per CTA: the last units to finish leave a tail of ~3 % at most
+        const int64_t target = 32 * grid;
+        int64_t segs = std::max<int64_t>(1, std::min<int64_t>(p.tiles, (target + p.rows - 1) / p.rows));
+        set_segments(p, segs);
+        if (grid > p.units) grid = p.units > 0 ? p.units : 1;
+        p.grid = (int)grid;
+    } else {
+        if (grid > p.total) grid = p.total > 0 ? p.total : 1;
+        p.grid = (int)grid;
+        p.slots = p.grid + p.rows;
+    }
     p.near2 = near2_of(kDefaultNearFactor);
     return p;
 }
 
-size_t partial_bytes(const ForcePlan &p) { return (size_t)p.slots * 3 * p.bi * sizeof(double); }
+// The queue counter sits after the partial sums, on its own 256-byte line.
+static size_t queue_offset(const ForcePlan &p) {
+    return ((size_t)p.slots * 3 * p.bi * sizeof(double) + 255) / 256 * 256;
+}
+
+size_t partial_bytes(const ForcePlan &p) { return queue_offset(p) + (p.segs > 0 ? 256 : 0); }
+
+int fit_plan_partials(ForcePlan &p, size_t max_bytes) {
+    if (partial_bytes(p) <= max_bytes) return GTD_OK;
+    const size_t per_slot = (size_t)3 * p.bi * sizeof(double);
+    const int64_t max_slots = max_bytes > 512 ? (int64_t)((max_bytes - 512) / per_slot) : 0;
+    if (p.segs > 0) {
+        const int64_t segs = max_slots / std::max<int64_t>(p.rows, 1);
+        if (segs < 1) return fail(GTD_ERR_CAPACITY, "%lld rows need more partial sums than %zu bytes hold",
+                                  (long long)p.rows, max_bytes);
+        set_segments(p, segs);
+        if (p.grid > p.units) p.grid = (int)p.units;
+    } else {
+        const int64_t grid = max_slots - p.rows;
+        if (grid < 1) return fail(GTD_ERR_CAPACITY, "%lld rows need more partial sums than %zu bytes hold",
+                                  (long long)p.rows, max_bytes);
+        if (p.grid > grid) p.grid = (int)grid;
+        p.slots = p.grid + p.rows;
+    }
+    return partial_bytes(p) <= max_bytes ? GTD_OK : fail(GTD_ERR_CAPACITY, "partial sums do not fit %zu bytes", max_bytes);
+}
 
 int launch_force(int precision, const ForcePlan &p, const double4 *src, double G, double *partials,
                  cudaStream_t s) {
     if (p.n == 0) return GTD_OK;
-    ForceKArgs a{p.n, p.rows, p.tiles, p.total, p.grid, p.bi, src, G, partials, p.near2};
-    if (precision == GTD_PREC_MIXED)
+    unsigned *queue = p.segs > 0 ? reinterpret_cast<unsigned *>(reinterpret_cast<char *>(partials) + queue_offset(p))
+                                 : nullptr;
+    ForceKArgs a{p.n, p.rows, p.tiles, p.total, p.grid, p.bi, src, G, partials, p.near2, p.segs, p.seg_tiles,
+                 p.units, queue};
+    if (precision == GTD_PREC_MIXED) {
+        if (!queue) return fail(GTD_ERR_INVALID_ARGUMENT, "mixed-precision plan without a work queue");
+        GTD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned), s));
         with_mixed(p.variant, [&](auto k) { k<<<p.grid, kThreads, 0, s>>>(a); });
+    }
     else
         with_f64(p.variant, [&](auto k) { k<<<p.grid, kThreads, 0, s>>>(a); });
     GTD_CHECK_LAUNCH();
@@ -600,10 +696,22 @@ struct IntArgs {
     int grid, bi, epi;
     const double *part;
     StepArgs st;
+    int64_t segs;  // > 0: work-queue slots r * segs .. r * segs + segs - 1
 };
 
 __device__ __forceinline__ int64_t cta_of(int64_t pos, int grid, int64_t total) {
     return ((pos + 1) * (int64_t)grid - 1) / total;
+}
+
+// The partial-sum slots of row r, first to last (fixed order: the sums are reproducible).
+__device__ __forceinline__ void row_slots(const IntArgs &a, int64_t r, int64_t &first, int64_t &last) {
+    if (a.segs > 0) {
+        first = r * a.segs;
+        last = first + a.segs - 1;
+    } else {
+        first = cta_of(r * a.tiles, a.grid, a.total) + r;
+        last = cta_of((r + 1) * a.tiles - 1, a.grid, a.total) + r;
+    }
 }
 
 // The method's update of body i from its summed force (ax, ay, az), in FP64.
@@ -676,11 +784,11 @@ __global__ void integrate_kernel(IntArgs a) {
     if (i >= a.n) return;
     const int64_t r = i / a.bi;
     const int l = (int)(i - r * a.bi);
-    const int64_t g0 = cta_of(r * a.tiles, a.grid, a.total);
-    const int64_t g1 = cta_of((r + 1) * a.tiles - 1, a.grid, a.total);
+    int64_t g0, g1;
+    row_slots(a, r, g0, g1);
     double ax = 0.0, ay = 0.0, az = 0.0;
     for (int64_t g = g0; g <= g1; ++g) {
-        const double *slot = a.part + (size_t)(g + r) * 3 * a.bi;
+        const double *slot = a.part + (size_t)g * 3 * a.bi;
         ax += slot[l];
         ay += slot[a.bi + l];
         az += slot[2 * a.bi + l];
@@ -696,11 +804,11 @@ __global__ void integrate_warp_kernel(IntArgs a) {
     if (i >= a.n) return;  // whole warps leave together
     const int64_t r = i / a.bi;
     const int l = (int)(i - r * a.bi);
-    const int64_t g0 = cta_of(r * a.tiles, a.grid, a.total);
-    const int64_t g1 = cta_of((r + 1) * a.tiles - 1, a.grid, a.total);
+    int64_t g0, g1;
+    row_slots(a, r, g0, g1);
     double ax = 0.0, ay = 0.0, az = 0.0;
     for (int64_t g = g0 + lane; g <= g1; g += 32) {
-        const double *slot = a.part + (size_t)(g + r) * 3 * a.bi;
+        const double *slot = a.part + (size_t)g * 3 * a.bi;
         ax += slot[l];
         ay += slot[a.bi + l];
         az += slot[2 * a.bi + l];
@@ -769,7 +877,7 @@ __global__ void __launch_bounds__(kFusedBodies * kFusedSlices * 32)
 
 int launch_fused_small(int64_t n, const double4 *src, double G, int epi, const StepArgs &st, cudaStream_t s) {
     if (n == 0) return GTD_OK;
-    IntArgs a{n, 0, 0, 0, 0, epi, nullptr, st};
+    IntArgs a{n, 0, 0, 0, 0, epi, nullptr, st, 0};
     fused_small_kernel<<<(unsigned)((n + kFusedBodies - 1) / kFusedBodies), kFusedBodies * kFusedSlices * 32, 0, s>>>(
         a, src, G);
     GTD_CHECK_LAUNCH();
@@ -778,12 +886,40 @@ int launch_fused_small(int64_t n, const double4 *src, double G, int epi, const S
 
 int launch_integrate(const ForcePlan &p, const double *partials, int epi, const StepArgs &st, cudaStream_t s) {
     if (p.n == 0) return GTD_OK;
-    IntArgs a{p.n, p.tiles, p.total, p.grid, p.bi, epi, partials, st};
+    IntArgs a{p.n, p.tiles, p.total, p.grid, p.bi, epi, partials, st, p.segs};
     const int threads = 256;
-    if ((int64_t)p.grid > 4 * p.rows)  // a row's force is spread over more than ~4 CTAs
+    if (p.slots > 4 * p.rows)  // a row's force is spread over more than ~4 slots
         integrate_warp_kernel<<<(unsigned)((p.n * 32 + threads - 1) / threads), threads, 0, s>>>(a);
     else
         integrate_kernel<<<(unsigned)((p.n + threads - 1) / threads), threads, 0, s>>>(a);
+    GTD_CHECK_LAUNCH();
+    return GTD_OK;
+}
+
+// Thread per body: the summed partials written as a triple (the force alone).
+__global__ void sum_partials_kernel(IntArgs a, double *acc3) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int64_t r = i / a.bi;
+    const int l = (int)(i - r * a.bi);
+    int64_t g0, g1;
+    row_slots(a, r, g0, g1);
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int64_t g = g0; g <= g1; ++g) {
+        const double *slot = a.part + (size_t)g * 3 * a.bi;
+        ax += slot[l];
+        ay += slot[a.bi + l];
+        az += slot[2 * a.bi + l];
+    }
+    acc3[3 * i] = ax;
+    acc3[3 * i + 1] = ay;
+    acc3[3 * i + 2] = az;
+}
+
+int launch_sum_partials(const ForcePlan &p, const double *partials, double *acc3, cudaStream_t s) {
+    if (p.n == 0) return GTD_OK;
+    IntArgs a{p.n, p.tiles, p.total, p.grid, p.bi, EPI_ACC, partials, StepArgs{}, p.segs};
+    sum_partials_kernel<<<(unsigned)((p.n + 255) / 256), 256, 0, s>>>(a, acc3);
     GTD_CHECK_LAUNCH();
     return GTD_OK;
 }

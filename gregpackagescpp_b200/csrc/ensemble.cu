@@ -652,12 +652,21 @@ int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
     cudaSetDevice(e->device);
     const int64_t nb = e->n_bodies;
     const size_t b4 = sizeof(double4) * (size_t)nb;
-    double4 *sp, *sv, *sa;
-    double *sr, *se;
-    int32_t *si, *sc;
-    GTD_CUDA(cudaMalloc(&sp, b4)); GTD_CUDA(cudaMalloc(&sv, b4)); GTD_CUDA(cudaMalloc(&sa, b4));
-    GTD_CUDA(cudaMalloc(&sr, 8 * (size_t)nb)); GTD_CUDA(cudaMalloc(&se, 8 * (size_t)nb));
-    GTD_CUDA(cudaMalloc(&si, 4 * (size_t)nb)); GTD_CUDA(cudaMalloc(&sc, 4 * (size_t)e->n_sys));
+    // copies of the state, freed on every return path
+    struct Saved {
+        double4 *sp = nullptr, *sv = nullptr, *sa = nullptr;
+        double *sr = nullptr, *se = nullptr;
+        int32_t *si = nullptr, *sc = nullptr;
+        ~Saved() {
+            cudaFree(sp); cudaFree(sv); cudaFree(sa); cudaFree(sr); cudaFree(se); cudaFree(si); cudaFree(sc);
+        }
+    } S;
+    GTD_CUDA(cudaMalloc(&S.sp, b4)); GTD_CUDA(cudaMalloc(&S.sv, b4)); GTD_CUDA(cudaMalloc(&S.sa, b4));
+    GTD_CUDA(cudaMalloc(&S.sr, 8 * (size_t)nb)); GTD_CUDA(cudaMalloc(&S.se, 8 * (size_t)nb));
+    GTD_CUDA(cudaMalloc(&S.si, 4 * (size_t)nb)); GTD_CUDA(cudaMalloc(&S.sc, 4 * (size_t)e->n_sys));
+    double4 *sp = S.sp, *sv = S.sv, *sa = S.sa;
+    double *sr = S.sr, *se = S.se;
+    int32_t *si = S.si, *sc = S.sc;
     auto save = [&](bool back) -> int {
         auto cp = [&](void *dst, void *src, size_t bytes) { return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, e->stream); };
         cudaError_t c = cudaSuccess;
@@ -698,6 +707,13 @@ int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
             rc = save(true);
         }
     }
+    if (rc) {  // a failed copy or launch: leave the configuration as it was
+        e->threads = orig_threads;
+        e->ib = orig_ib;
+        e->begun = was_begun;
+        cudaStreamSynchronize(e->stream);
+        return rc;
+    }
     int best = orig_threads, best_ib = orig_ib;  // kept if no timing completed
     double bestv = 1e300;
     for (int k = 0; k < kCands; ++k)
@@ -709,9 +725,7 @@ int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
     e->threads = best;
     e->ib = best_ib;
     e->begun = was_begun;
-    cudaStreamSynchronize(e->stream);
-    cudaFree(sp); cudaFree(sv); cudaFree(sa); cudaFree(sr); cudaFree(se); cudaFree(si); cudaFree(sc);
-    if (rc) return rc;
+    GTD_CUDA(cudaStreamSynchronize(e->stream));
     GTD_CUDA(cudaMemset(e->work, 0, 4 * sizeof(unsigned)));
     if (best_threads) *best_threads = best;
     if (best_ms) *best_ms = bestv;

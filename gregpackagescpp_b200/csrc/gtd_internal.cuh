@@ -36,7 +36,11 @@ struct ForcePlan {
     int bi = 0, bj = 0;      // bodies per i-block, per j-tile
     int64_t rows = 0, tiles = 0, total = 0;
     int grid = 0;            // CTAs of the force kernel
-    int64_t slots = 0;       // partial-sum slots (grid + rows)
+    int64_t slots = 0;       // partial-sum slots: grid + rows (stream-K), rows * segs (work queue)
+    // Work queue (mixed kernel): each row's tiles are cut into segs segments of seg_tiles tiles; the
+    // rows * segs units are taken in turn from a counter by the CTAs, each unit writing its own slot.
+    // segs == 0: the stream-K split above.
+    int64_t segs = 0, seg_tiles = 0, units = 0;
     int variant = 0;         // kernel variant (i-bodies per thread, fold length)
     float near2 = 0.f;       // mixed kernel: precise-path threshold, near2_of(near factor)
 };
@@ -86,6 +90,11 @@ int launch_fused_small(int64_t n, const double4 *src, double G, int epi, const S
 void remember_variant(int device, int precision, int64_t n, int variant);
 int tuned_variant(int device, int precision, int64_t n);
 size_t partial_bytes(const ForcePlan &p);
+// Shrinks the plan's partial-sum footprint to at most max_bytes (fewer queue segments, or a smaller
+// stream-K grid); GTD_ERR_CAPACITY when even the smallest split does not fit.
+int fit_plan_partials(ForcePlan &p, size_t max_bytes);
+// acc3[3 i + d] = the summed partials of body i (the force alone, in the bodies' order).
+int launch_sum_partials(const ForcePlan &p, const double *partials, double *acc3, cudaStream_t s);
 // Force on every body of `src` (positions + G-free masses), written as partial sums.
 int launch_force(int precision, const ForcePlan &p, const double4 *src, double G, double *partials,
                  cudaStream_t s);

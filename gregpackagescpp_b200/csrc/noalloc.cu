@@ -6,7 +6,8 @@
 // all its memory once at start-up) may not be able to get more, and in a running loop cudaMalloc /
 // cudaFree synchronise the whole device, stalling every other stream.  This entry point takes the
 // caller's device buffers for input and output and keeps the only scratch the force needs - the
-// stream-K partial sums - in one fixed array compiled into the library.
+// force kernel's partial sums (and, in mixed precision, its work-queue counter, zeroed on the
+// stream before every launch) - in one fixed array compiled into the library.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -21,8 +22,6 @@ namespace gtd {
 constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double)];
 
-// The stream-K grid is capped so the partial sums of N = 65536 bodies fit the scratch.
-constexpr int kNoAllocMaxGrid = 296;
 constexpr int64_t kNoAllocMaxBodies = 65536;
 constexpr int kMaxDevices = 64;
 
@@ -33,28 +32,21 @@ struct ScratchAddr {
 static ScratchAddr g_scratch_addr[kMaxDevices];
 static std::mutex g_scratch_mu;
 
-// Sums the partials of body i (CTA order, as the integrate kernel does) into acc3[3 i .. 3 i + 2].
-__global__ void noalloc_combine_kernel(int64_t n, int64_t tiles, int64_t total, int grid, int bi,
-                                       const double *part, double *acc3) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t r = i / bi;
-    const int l = (int)(i - r * bi);
-    const int64_t g0 = ((r * tiles + 1) * (int64_t)grid - 1) / total;
-    const int64_t g1 = (((r + 1) * tiles) * (int64_t)grid - 1) / total;
-    double ax = 0.0, ay = 0.0, az = 0.0;
-    for (int64_t g = g0; g <= g1; ++g) {
-        const double *slot = part + (size_t)(g + r) * 3 * bi;
-        ax += slot[l];
-        ay += slot[bi + l];
-        az += slot[2 * bi + l];
+// Whether p is memory the current device can read and write: device or managed memory of that
+// device.  A host pointer, or another device's buffer, is rejected before any launch.
+static bool on_current_device(const void *p, int dev) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();  // the failed query leaves its error as the last error: clear it
+        return false;
     }
-    acc3[3 * i] = ax;
-    acc3[3 * i + 1] = ay;
-    acc3[3 * i + 2] = az;
+    if (at.type == cudaMemoryTypeManaged) return true;
+    return at.type == cudaMemoryTypeDevice && at.device == dev;
 }
 
-// Device address of the scratch on the current device; looked up on the first call per device.
+// Device address of the scratch on the current device; looked up on the first call per device and
+// kept for the life of the process.  cudaDeviceReset discards the module and with it the array, so
+// the kept address is not valid across a device reset: do not use this entry point after one.
 static int scratch_on_current_device(void **out) {
     int dev = 0;
     GTD_CUDA(cudaGetDevice(&dev));
@@ -90,24 +82,20 @@ extern "C" int gtd_direct_accelerations_noalloc(int64_t n, const double *pm4, do
                     "gtd_direct_accelerations_noalloc holds its partial sums in a fixed %zu-byte device array and "
                     "accepts at most %lld bodies; got %lld (use gtd_system_accelerations for larger systems)",
                     kNoAllocScratchBytes, (long long)kNoAllocMaxBodies, (long long)n);
+    int dev = 0;
+    GTD_CUDA(cudaGetDevice(&dev));
+    if (!on_current_device(pm4, dev) || !on_current_device(acc3, dev))
+        return fail(GTD_ERR_INVALID_ARGUMENT,
+                    "pm4 and acc3 must be device (or managed) memory of the current device %d", dev);
     void *scratch = nullptr;
     int rc = scratch_on_current_device(&scratch);
     if (rc) return rc;
-    int dev = 0;
-    GTD_CUDA(cudaGetDevice(&dev));
+    // the split of the force into partial sums is narrowed until they fit the fixed scratch
     ForcePlan p = make_plan(n, precision, dev, 0);
-    if (p.grid > kNoAllocMaxGrid) {
-        p.grid = kNoAllocMaxGrid;
-        p.slots = p.grid + p.rows;
-    }
-    if (partial_bytes(p) > kNoAllocScratchBytes)
-        return fail(GTD_ERR_CAPACITY, "%lld bodies need %zu bytes of partial sums; the fixed scratch holds %zu",
-                    (long long)n, partial_bytes(p), kNoAllocScratchBytes);
+    rc = fit_plan_partials(p, kNoAllocScratchBytes);
+    if (rc) return rc;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     rc = launch_force(precision, p, reinterpret_cast<const double4 *>(pm4), G, static_cast<double *>(scratch), st);
     if (rc) return rc;
-    noalloc_combine_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, p.tiles, p.total, p.grid, p.bi,
-                                                                         static_cast<const double *>(scratch), acc3);
-    GTD_CHECK_LAUNCH();
-    return GTD_OK;
+    return launch_sum_partials(p, static_cast<const double *>(scratch), acc3, st);
 }

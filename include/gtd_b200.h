@@ -313,8 +313,13 @@ GTD_API int gtd_bh_accelerations(gtd_system *sys, double *a3, uint32_t *n_inter)
  * (cudaGetSymbolAddress), so make the first call on each device before any stream capture.  All
  * calls share the array: calls whose work overlaps on the GPU (different streams, or different
  * host threads) race on it and must be serialised by the caller.  Nothing in it needs clearing
- * between calls (every partial sum read is written first by the same call).  stream: a
- * cudaStream_t or NULL; the call returns after enqueueing. */
+ * between calls (every partial sum read is written first by the same call).  The array's address
+ * is kept per device after the first call; cudaDeviceReset discards the array, so the entry point
+ * must not be used after a device reset.  pm4 and acc3 that are not device (or managed) memory of
+ * the current device are rejected with GTD_ERR_INVALID_ARGUMENT before anything is launched.
+ * GTD_PREC_MIXED sums the bodies in the order given (gtd_system reorders them spatially first);
+ * its test bar against the FP64 result is 1e-6 RMS relative.  stream: a cudaStream_t or NULL; the
+ * call returns after enqueueing. */
 GTD_API int gtd_direct_accelerations_noalloc(int64_t n, const double *pm4, double G, int precision, double *acc3,
                                              void *stream);
 

@@ -20,13 +20,23 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REFLIB = os.path.join(HERE, "_ref", "libgtdref.so")
-REF_TREE = "/root/reference"
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _up = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 
 EULER, MODIFIED_EULER, MIDPOINT, LEAPFROG_KDK, LEAPFROG_DKD = 2, 4, 8, 16, 32
+
+
+def reference_tree() -> str | None:
+    """The reference checkout the Makefile reads (GTD_REFERENCE_DIR, else the Makefile's default),
+    or None when it is not present on this machine."""
+    try:
+        r = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True, timeout=60)
+        path = r.stdout.strip()
+    except Exception:
+        return None
+    return path if path and os.path.isdir(path) else None
 
 
 def ensure_built(ref: bool = False) -> None:
@@ -37,10 +47,11 @@ def ensure_built(ref: bool = False) -> None:
         os.path.getmtime(os.path.join(HERE, f)) for f in ("nbody_oracle.c", "nbody_oracle.h"))
     if need:
         subprocess.run(["make", "-s", "-C", HERE, LIB], check=True)
-    if ref and os.path.isdir(REF_TREE):
+    tree = reference_tree() if ref else None
+    if tree:
         if (not os.path.exists(REFLIB) or
                 os.path.getmtime(REFLIB) < os.path.getmtime(os.path.join(HERE, "ref_oracle.cpp"))):
-            subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
+            subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={tree}"], check=True)
     del targets
 
 

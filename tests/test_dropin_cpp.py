@@ -35,10 +35,16 @@ def test_dropin_program_runs_on_gpu(gpu, tmp_path):
     assert run.returncode == 0, run.stdout + run.stderr
 
 
-REF_DRIVER = "/root/reference/nrg.cpp"
+def _ref_driver():
+    from oracle.oracle import reference_tree
+    tree = reference_tree()
+    return os.path.join(tree, "nrg.cpp") if tree else None
 
 
-@pytest.mark.skipif(not os.path.exists(REF_DRIVER), reason="the reference tree is not mounted here")
+REF_DRIVER = _ref_driver()
+
+
+@pytest.mark.skipif(REF_DRIVER is None or not os.path.exists(REF_DRIVER), reason="the reference tree is not here")
 def test_reference_driver_compiles_unchanged(tmp_path):
     """nrg.cpp, one of the reference's own drivers (it loads .nsys files into
     gtd::system<T,T,T,true,false,3,0,0,false> for three T and sums their energies through body and

@@ -54,7 +54,7 @@ def test_noalloc_mixed_precision_close_to_fp64(gpu):
     torch.cuda.synchronize()
     want = System(m, x, v, units_format=UNITS_G6674).accelerations()
     rel = np.linalg.norm(acc3.cpu().numpy() - want, axis=1) / np.linalg.norm(want, axis=1)
-    assert np.sqrt((rel ** 2).mean()) < 1e-5
+    assert np.sqrt((rel ** 2).mean()) < 1e-6, float(np.sqrt((rel ** 2).mean()))
 
 
 def test_noalloc_rejects_more_bodies_than_its_scratch_holds(gpu):
@@ -64,3 +64,17 @@ def test_noalloc_rejects_more_bodies_than_its_scratch_holds(gpu):
     rc = _noalloc(pm4, acc3)
     assert rc == _lib.ERR_CAPACITY
     assert b"65536" in _lib.load().gtd_last_error()
+
+
+def test_noalloc_rejects_host_memory(gpu):
+    """A host array where device memory is expected is turned into an error before any launch."""
+    import torch
+    L = _lib.load()
+    L.gtd_direct_accelerations_noalloc.argtypes = [C.c_int64, C.c_void_p, C.c_double, C.c_int, C.c_void_p,
+                                                   C.c_void_p]
+    L.gtd_direct_accelerations_noalloc.restype = C.c_int
+    host_pm4 = np.zeros((64, 4))
+    acc3 = torch.zeros((64, 3), dtype=torch.float64, device="cuda:0")
+    rc = L.gtd_direct_accelerations_noalloc(64, host_pm4.ctypes.data, G, _lib.PREC_F64, acc3.data_ptr(), None)
+    assert rc == _lib.ERR_INVALID_ARGUMENT
+    assert b"device" in L.gtd_last_error()
