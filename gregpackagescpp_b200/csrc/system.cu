@@ -460,6 +460,12 @@ const char *gtd_last_error(void) { return gtd::last_error(); }
 
 int gtd_abi_version(void) { return GTD_ABI_VERSION; }
 
+int gtd_check_option(int option, int *accepted) {
+    if (!accepted) return fail(GTD_ERR_INVALID_ARGUMENT, "accepted is NULL");
+    *accepted = check_option(option) ? 1 : 0;
+    return GTD_OK;
+}
+
 int gtd_device_count(int *count) {
     if (!count) return fail(GTD_ERR_INVALID_ARGUMENT, "count is NULL");
     *count = 0;

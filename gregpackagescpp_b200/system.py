@@ -6,6 +6,7 @@ std::vector<body>) and is uploaded to the device for each evolve() and read back
 from __future__ import annotations
 
 import ctypes as C
+import math
 import re
 from dataclasses import dataclass, field
 from fractions import Fraction
@@ -20,7 +21,7 @@ PI = 3.14159265358979323846
 _UNITS_RE = re.compile(
     r"^\s*(m|M)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(d|D)\s*(?=\d{1,18}\s*:)"
     r"\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(t|T)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*"
-    r"(?=\d{1,18}\s*$)\d*[1-9]+\d*\s*$")
+    r"(?=\d{1,18}\s*$)\d*[1-9]+\d*\s*$", re.ASCII)  # std::regex's \d and \s are ASCII
 
 
 def _ke(m, v):
@@ -49,9 +50,11 @@ def parse_units(units: str) -> float:
     b = mass numerator, c/d = distance numerator/denominator, x/y = time denominator/numerator;
     G = 66743e-15 * b c^3 y^2 / (a d^3 x^2).  Raises ValueError on a malformed string, as the
     reference throws std::invalid_argument."""
-    if not _UNITS_RE.match(units):
+    if not _UNITS_RE.fullmatch(units):
         raise ValueError(f'The units_format string passed, "{units}", does not match the format required:\n'
-                         '"Ma:b,Dc:x,Ty:z"')
+                         '"Ma:b,Dc:x,Ty:z", where \'a\', \'b\', \'c\', \'x\', \'y\', and \'z\' represent any '
+                         'positive integer number of 1-18 characters starting with at least one non-zero '
+                         'character.\n')
     s = units.strip("MmDdTt ").replace(" ", "")
     nums = [int(x) for x in re.findall(r"\d+", s)]
     m_den, m_num, d_num, d_den, t_den, t_num = nums
@@ -256,13 +259,16 @@ class System:
 
     def set_softening(self, epsilon: float) -> bool:
         # the reference rejects eps < sqrt(LDBL_MIN) (~1.8e-2466): for a double that is eps <= 0
-        if not epsilon > 0:
+        # (NaN compares false and is accepted, as there)
+        if epsilon <= 0:
             return False
         self.eps = float(epsilon)
         return True
 
     def set_bh_opening_angle(self, theta: float) -> bool:
-        if theta < 0 or theta >= PI:
+        # the reference compares with its long double pi: the double nearest pi lies below it and is
+        # accepted, every larger double is not
+        if theta < 0 or theta > math.pi:
             return False
         self.theta = float(theta)
         return True

@@ -104,7 +104,9 @@ private:
         static const std::regex re{R"(^\s*(m|M)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(d|D)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*,)\d*[1-9]+\d*\s*,\s*(t|T)\s*(?=\d{1,18}\s*:)\d*[1-9]+\d*\s*:\s*(?=\d{1,18}\s*$)\d*[1-9]+\d*\s*$)"};
         if (!std::regex_match(str, re))
             throw std::invalid_argument{"The units_format string passed, \"" + str +
-                                        "\", does not match the format required:\n\"Ma:b,Dc:x,Ty:z\"."};
+                                        "\", does not match the format required:\n\"Ma:b,Dc:x,Ty:z\", where "
+                                        "'a', 'b', 'c', 'x', 'y', and 'z' represent any positive integer number of "
+                                        "1-18 characters starting with at least one non-zero character.\n"};
         uint64_t v[6];
         int k = 0;
         static const std::regex digits{R"(\d+)"};

@@ -67,6 +67,9 @@ extern "C" {
 typedef struct gtd_system gtd_system;
 
 GTD_API const char *gtd_last_error(void);
+/* *accepted = whether evolve() accepts the method value, by gtd::system::check_option
+ * (gregsys.hpp:1406-1411; its word tests let nearly every value through).  Host-only. */
+GTD_API int gtd_check_option(int option, int *accepted);
 GTD_API int gtd_abi_version(void);
 GTD_API int gtd_device_count(int *count);
 

@@ -234,6 +234,12 @@ class RefOracle:
                                  C.c_char_p, _dp, _dp, _dp, C.POINTER(C.c_longlong)]
         L.ref_G.restype = C.c_int
         L.ref_G.argtypes = [C.c_char_p, C.POINTER(C.c_longdouble)]
+        L.ref_setters.restype = C.c_int
+        L.ref_setters.argtypes = [C.c_longdouble, C.c_uint64, C.c_longdouble, C.c_longdouble, _ip]
+        L.ref_check_option.restype = C.c_int
+        L.ref_check_option.argtypes = [C.c_int]
+        L.ref_construct_dt.restype = C.c_int
+        L.ref_construct_dt.argtypes = [C.c_longdouble]
         L.ref_energy.restype = C.c_int
         L.ref_energy.argtypes = [C.c_int, _dp, _dp, _dp, C.c_char_p, C.POINTER(C.c_longdouble),
                                  C.POINTER(C.c_longdouble)]
@@ -307,6 +313,29 @@ class RefOracle:
         g = C.c_longdouble()
         self._chk(self.lib.ref_G(units.encode(), C.byref(g)))
         return g.value
+
+    def units(self, units: str):
+        """(True, G as ctypes long double) when the reference accepts the units format, else
+        (False, the message of its std::invalid_argument)."""
+        g = C.c_longdouble()
+        if self.lib.ref_G(units.encode(), C.byref(g)) == 0:
+            return True, g
+        return False, self.lib.ref_last_error().decode()
+
+    def setters(self, dt, iterations, eps, theta):
+        """The reference's set_timestep, set_iterations, set_softening, set_bh_opening_angle results."""
+        out = np.zeros(4, np.int32)
+        self._chk(self.lib.ref_setters(dt, iterations, eps, theta, out))
+        return tuple(bool(b) for b in out)
+
+    def check_option(self, option: int) -> bool:
+        return bool(self.lib.ref_check_option(option))
+
+    def construct_dt(self, dt):
+        """None when a system with time step dt constructs, else the exception message."""
+        if self.lib.ref_construct_dt(dt) == 0:
+            return None
+        return self.lib.ref_last_error().decode()
 
     def bench_kdk(self, m, x, v, dt, steps, threads, units="M66743:66740,D1:1,T1:1"):
         """Wall seconds for `threads` concurrent reference evolve(leapfrog_kdk) calls."""

@@ -46,6 +46,11 @@ public:
 
     template <typename S>
     static long double G(const S &s) { return s.G; }
+
+    /* gtd::system's private static check_option (gregsys.hpp:1406-1411). */
+    static bool check_option(int option) {
+        return gtd::system<double, double, double, false, false, 0, 0, 0, false>::check_option(option);
+    }
     template <typename S>
     static long double time_elapsed(const S &s) { return s.time_elapsed; }
     template <typename S>
@@ -361,6 +366,32 @@ int ref_G(const char *units, long double *G) {
     REF_TRY
     gtd::system<double, double, double, false, false, 0, 0, 0, false> s{1.0L, 1, units};
     *G = ref_access::G(s);
+    return 0;
+    REF_CATCH
+}
+
+/* The reference's setters (gregsys.hpp:1636-1672) on a default system: out4 = the results of
+ * set_timestep(dt), set_iterations(iterations), set_softening(eps), set_bh_opening_angle(theta).
+ * dt, eps and theta arrive as long double so that values between two doubles can be tried. */
+int ref_setters(long double dt, uint64_t iterations, long double eps, long double theta, int *out4) {
+    REF_TRY
+    gtd::system<double, double, double, false, false, 0, 0, 0, false> s{1.0L, 1, "M1:1,D1:1,T1:1"};
+    out4[0] = s.set_timestep(dt) ? 1 : 0;
+    out4[1] = s.set_iterations(iterations) ? 1 : 0;
+    out4[2] = s.set_softening(eps) ? 1 : 0;
+    out4[3] = s.set_bh_opening_angle(theta) ? 1 : 0;
+    return 0;
+    REF_CATCH
+}
+
+/* check_option (gregsys.hpp:1406-1411): 1 when evolve() accepts the method value, else 0. */
+int ref_check_option(int option) { return ref_access::check_option(option) ? 1 : 0; }
+
+/* Constructs a system with time step dt (the constructor's check_dt, gregsys.hpp:1401-1405):
+ * 0, or -1 with the exception's message in ref_last_error(). */
+int ref_construct_dt(long double dt) {
+    REF_TRY
+    gtd::system<double, double, double, false, false, 0, 0, 0, false> s{dt, 1, "M1:1,D1:1,T1:1"};
     return 0;
     REF_CATCH
 }

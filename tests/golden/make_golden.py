@@ -2,7 +2,8 @@
 (through oracle/_ref/libgtdref.so, built from the reference tree by oracle/Makefile).
 
 Run here, where the reference tree is mounted:  python tests/golden/make_golden.py
-The fixtures are small .npz files; the tests read them, never the reference tree.
+(``python tests/golden/make_golden.py tree`` regenerates only the tree-walk fixture.)
+The fixtures are small .npz / text files; the tests read them, never the reference tree.
 """
 from __future__ import annotations
 
@@ -223,7 +224,36 @@ def callback_fixtures(r, out):
     out["cbp_cases"] = np.array(cases)
 
 
+TREE_WALK_N = 2000
+
+
+def tree_walk_fixture():
+    """tests/cpp/tree_walk_main.cpp - a program written against the reference's bh_tree API -
+    compiled against the reference headers and run on TREE_WALK_N bodies; its output (leaf order,
+    per-leaf cell_iterator counts and long-double force sums, nn_iterator counts, the children of
+    the first yielded cells via operator[]) is the fixture tree_walk_ref.txt."""
+    import subprocess
+    import tempfile
+    from oracle.oracle import reference_tree
+    tree = reference_tree()
+    if tree is None:
+        raise SystemExit("the reference tree is not present here")
+    src = os.path.join(ROOT, "tests", "cpp", "tree_walk_main.cpp")
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = os.path.join(tmp, "tree_walk_ref")
+        subprocess.run(["g++", "-std=c++20", "-O2", "-include", "cstdint", "-w", "-I", tree, src, "-o", exe],
+                       check=True)
+        outp = subprocess.run([exe, str(TREE_WALK_N)], check=True, capture_output=True, text=True).stdout
+    path = os.path.join(HERE, "tree_walk_ref.txt")
+    with open(path, "w") as f:
+        f.write(outp)
+    print(path, os.path.getsize(path), "bytes")
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "tree":
+        tree_walk_fixture()
+        return
     ensure_built(ref=True)
     r = RefOracle()
     out = {}
@@ -309,6 +339,7 @@ def main():
     path = os.path.join(HERE, "reference_golden.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes,", len(out), "arrays")
+    tree_walk_fixture()
 
 
 if __name__ == "__main__":

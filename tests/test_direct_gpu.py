@@ -59,6 +59,30 @@ def test_kdk_1024_thousand_steps_energy(gpu, oracle):
     assert abs((ke1 + pe1) - (ke0 + pe0)) / abs(ke0 + pe0) < 1e-6
 
 
+def test_energy_over_1000_steps_vs_reference(gpu):
+    """The reference's own evolve(leapfrog_kdk) and calc_energy (gregsys.hpp:608-630) next to the
+    FP64 GPU path over 1000 steps of dt = 3600 s at N = 2048: the two energies agree at step 0 and
+    at step 1000, so the drift |dE/E| the GPU path shows is the integrator's (the reference drifts
+    by the same amount), not an error of the GPU arithmetic."""
+    from oracle.oracle import RefOracle
+    if not RefOracle.available():
+        pytest.skip("the reference-backed oracle library was not built here")
+    ref = RefOracle()
+    m, x, v = plummer(2048, 2)
+    s = System(m, x, v, timestep=3600.0, num_iterations=1000, units_format=UNITS_G6674)
+    ke0, pe0, _, _ = s.energy()
+    rk0, rp0 = ref.energy(m, x, v, UNITS_G6674)
+    s.evolve(16)
+    ke1, pe1, _, _ = s.energy()
+    xr, vr, _, _ = ref.evolve(16, m, x, v, 3600.0, 1000, UNITS_G6674)
+    rk1, rp1 = ref.energy(m, xr, vr, UNITS_G6674)
+    e0, e1, r0, r1 = ke0 + pe0, ke1 + pe1, rk0 + rp0, rk1 + rp1
+    assert abs(e0 - r0) <= 1e-13 * abs(r0), (e0, r0)
+    drift_gpu, drift_ref = (e1 - e0) / abs(e0), (r1 - r0) / abs(r0)
+    print(f"|dE/E| over 1000 steps: GPU {drift_gpu:.6e}, reference {drift_ref:.6e}")
+    assert abs(e1 - r1) <= 1e-9 * abs(r1), (drift_gpu, drift_ref)
+
+
 def test_energy_diagnostic_vs_oracle(gpu, oracle, golden):
     g = golden
     s = System(g["direct_m"], g["direct_x"], g["direct_v"], units_format=UNITS_G6674)

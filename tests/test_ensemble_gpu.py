@@ -120,3 +120,26 @@ def test_capacity_limit(gpu):
     x = np.random.default_rng(0).normal(size=(9000, 3))
     with pytest.raises(Exception):
         Ensemble(off, m, x)
+
+
+def test_config_size_sampled_systems_vs_oracle(gpu, oracle):
+    """The ensemble configuration itself: 4096 systems with N ~ U{3..2048} (seed 4, 4.24 M bodies),
+    merges on, 20 KDK steps in one batch; 32 seeded systems re-run one by one on the oracle (the
+    reference's KDK and check_overlap merge after each step) at the bars of test_merges_vs_oracle."""
+    off, m, r, x, v = ensemble(4096, 4)
+    e = Ensemble(off, m, x, v, r, merge=True, dt=DT)
+    e.evolve(20)
+    st = e.state()
+    counts, merges, _ = e.counts()
+    pick = np.random.default_rng(11).choice(4096, 32, replace=False)
+    for s in pick:
+        b, k = off[s], off[s + 1]
+        rows = np.concatenate([m[b:k, None], r[b:k, None], np.ones((k - b, 1)), x[b:k], v[b:k],
+                               np.zeros((k - b, 3))], 1)
+        rows = oracle.merge_overlapping(rows)
+        mo, ro, xo, vo = oracle_run(oracle, rows[:, 0].copy(), rows[:, 1].copy(), rows[:, 2].copy(),
+                                    rows[:, 3:6].copy(), rows[:, 6:9].copy(), 20, True)
+        assert counts[s] == len(mo), (s, counts[s], len(mo))
+        np.testing.assert_allclose(st[s]["m"], mo, rtol=1e-15)
+        assert np.abs(st[s]["x"] - xo).max() / np.abs(xo).max() < 1e-10, s
+        assert np.abs(st[s]["v"] - vo).max() / np.abs(vo).max() < 1e-7, s
