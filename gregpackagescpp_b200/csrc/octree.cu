@@ -502,26 +502,26 @@ __global__ void __launch_bounds__(kTT, sizeof(T) == 4 ? 8 : 1) walk_kernel(int64
         if (leaf) {
             if (count == 1) {
                 if ((int32_t)node != ol) {
-                    const T dx = A.x - p.x, dy = A.y - p.y, dz = A.z - p.z;
-                    const T r2 = SOFT ? dx * dx + dy * dy + dz * dz + eps2 : dx * dx + dy * dy + dz * dz;
-                    const T inv = rsqrt_t(r2);
-                    const T sc = A.w * inv * inv * inv;
-                    ax += sc * dx;
-                    ay += sc * dy;
-                    az += sc * dz;
+                    const T dx = sub_t(A.x, p.x), dy = sub_t(A.y, p.y), dz = sub_t(A.z, p.z);
+                    const T r2 = fma_t(dz, dz, fma_t(dy, dy, mul_t(dx, dx)));
+                    const T inv = rsqrt_t(SOFT ? r2 + eps2 : r2);
+                    const T sc = mul_t(mul_t(mul_t(A.w, inv), inv), inv);
+                    ax = fma_t(sc, dx, ax);
+                    ay = fma_t(sc, dy, ay);
+                    az = fma_t(sc, dz, az);
                     if constexpr (COUNT) ++cnt;
                 }
             } else {
                 for (int q = B.y; q < B.y + count; ++q) {
                     if (q == (int)s) continue;
                     const V Q = bodies[q];
-                    const T dx = Q.x - p.x, dy = Q.y - p.y, dz = Q.z - p.z;
-                    const T r2 = SOFT ? dx * dx + dy * dy + dz * dz + eps2 : dx * dx + dy * dy + dz * dz;
-                    const T inv = rsqrt_t(r2);
-                    const T sc = Q.w * inv * inv * inv;
-                    ax += sc * dx;
-                    ay += sc * dy;
-                    az += sc * dz;
+                    const T dx = sub_t(Q.x, p.x), dy = sub_t(Q.y, p.y), dz = sub_t(Q.z, p.z);
+                    const T r2 = fma_t(dz, dz, fma_t(dy, dy, mul_t(dx, dx)));
+                    const T inv = rsqrt_t(SOFT ? r2 + eps2 : r2);
+                    const T sc = mul_t(mul_t(mul_t(Q.w, inv), inv), inv);
+                    ax = fma_t(sc, dx, ax);
+                    ay = fma_t(sc, dy, ay);
+                    az = fma_t(sc, dz, az);
                     if constexpr (COUNT) ++cnt;
                 }
             }
@@ -531,12 +531,11 @@ __global__ void __launch_bounds__(kTT, sizeof(T) == 4 ? 8 : 1) walk_kernel(int64
             const T r2 = fma_t(dz, dz, fma_t(dy, dy, mul_t(dx, dx)));
             const T w2 = sizeof(T) == 4 ? (T)__int_as_float(B.w) : (T)w2_64[node];
             if (w2 < mul_t(th2, r2)) {
-                const T r2e = SOFT ? r2 + eps2 : r2;
-                const T inv = rsqrt_t(r2e);
-                const T sc = A.w * inv * inv * inv;
-                ax += sc * dx;
-                ay += sc * dy;
-                az += sc * dz;
+                const T inv = rsqrt_t(SOFT ? r2 + eps2 : r2);
+                const T sc = mul_t(mul_t(mul_t(A.w, inv), inv), inv);
+                ax = fma_t(sc, dx, ax);
+                ay = fma_t(sc, dy, ay);
+                az = fma_t(sc, dz, az);
                 if constexpr (COUNT) ++cnt;
                 next = (uint32_t)B.x;
             } else {
