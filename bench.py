@@ -785,14 +785,22 @@ def cfg_adjoint(args, local, peak32=None, peak64=None, hbm=None):
     if peak64:
         line["forward_frac_of_fp64_peak"] = 20.0 * (T + 1) * n * (n - 1) / (fwd * 1e-3) / peak64
     if args.adj_fd > 0:
-        # central differences of the library's own FP64 forward, h relative to the coordinate, at
-        # two steps per group: the specified 1e-6 for positions and velocities (1e-4 for masses,
-        # whose derivatives are small next to the loss) and 10x that.  Both carry roundoff of the
-        # FP64 loss divided by h, which at the small step is ~1e-5 of the components that are small
-        # next to the largest one; the larger step divides it by ten while the truncation error
-        # stays below it (|D(h) - D(10h)| is reported as the quotients' own disagreement).
+        # FP64 central differences of the library's own forward on args.adj_fd seeded coordinates,
+        # split over positions, velocities and masses.  The forward is chaotic at this size (2000
+        # steps with close encounters), so a quotient D(h) carries, besides its O(h^2) truncation,
+        # the amplified FP64 roundoff of the two loss values divided by h.  Rule: each coordinate
+        # takes D at h = 1e-6, 1e-5 and 1e-4 relative; of the adjacent pairs (1e-6, 1e-5) and
+        # (1e-5, 1e-4) the one whose quotients agree best gives the reference D_ref (its smaller
+        # step) and the resolution |D(h_a) - D(h_b)|; a component agrees when
+        # |g - D_ref| <= max(1e-5 |D_ref|, resolution).  The specified h = 1e-6 is reported on its
+        # own beside it.
         rng = np.random.default_rng(8)
-        fd_out = {}
+        steps_rel = (1e-6, 1e-5, 1e-4)
+
+        def loss_at(args3):
+            with torch.no_grad():
+                y, _ = leapfrog_final_state(*args3, 6.674e-11, 3600.0, T, every)
+                return float(((y - target) ** 2).sum(-1).mean())
 
         def fd_at(which, idx, hrel):
             base = {"x": tx, "v": tv, "m": tm}[which].reshape(-1)
@@ -801,28 +809,42 @@ def cfg_adjoint(args, local, peak32=None, peak64=None, hbm=None):
             for sgn in (1, -1):
                 args3 = [tx.clone(), tv.clone(), tm.clone()]
                 args3["xvm".index(which)].reshape(-1)[idx] += sgn * hs
-                with torch.no_grad():
-                    y, _ = leapfrog_final_state(*args3, 6.674e-11, 3600.0, T, every)
-                    vals.append(float(((y - target) ** 2).sum(-1).mean()))
+                vals.append(loss_at(args3))
             return (vals[0] - vals[1]) / (2 * hs)
 
-        def summary(g, d):
-            err = np.abs(g - d)
-            rel = err / np.maximum(np.abs(d), 1e-300)
-            return {"max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
-                    "normwise_rel_err": float(err.max() / np.abs(d).max()), "within_1e-5": int((rel <= 1e-5).sum())}
-
-        for which, grad, hrel in (("x", xa.grad, 1e-6), ("v", va.grad, 1e-6), ("m", ma.grad, 1e-4)):
+        per = [len(c) for c in np.array_split(np.arange(args.adj_fd), 3)]  # e.g. 64 = 22 + 21 + 21
+        fd_out = {"steps_rel": list(steps_rel),
+                  "rule": "D_ref, res = best-agreeing adjacent pair of D(1e-6), D(1e-5), D(1e-4); agree if "
+                          "|g - D_ref| <= max(1e-5 |D_ref|, res)"}
+        t0 = time.perf_counter()
+        for k, (which, grad) in enumerate((("x", xa.grad), ("v", va.grad), ("m", ma.grad))):
             flat = grad.reshape(-1)
-            g, d1, d2 = [], [], []
-            for idx in rng.choice(flat.numel(), max(1, args.adj_fd // 3), replace=False):
-                g.append(float(flat[idx]))
-                d1.append(fd_at(which, idx, hrel))
-                d2.append(fd_at(which, idx, 10 * hrel))
-            g, d1, d2 = np.array(g), np.array(d1), np.array(d2)
-            fd_out[which] = {"coords": len(g), f"h_rel_{hrel:g}": summary(g, d1),
-                             f"h_rel_{10 * hrel:g}": summary(g, d2),
-                             "fd_h_vs_10h_normwise": float(np.abs(d1 - d2).max() / np.abs(d2).max())}
+            rows = []
+            for idx in rng.choice(flat.numel(), per[k], replace=False):
+                g = float(flat[idx])
+                d = [fd_at(which, int(idx), h) for h in steps_rel]
+                pairs = [(abs(d[0] - d[1]) / abs(d[0]), 0), (abs(d[1] - d[2]) / abs(d[1]), 1)]
+                _, j = min(pairs)
+                ref, res = d[j], abs(d[j] - d[j + 1])
+                rows.append({"index": int(idx), "g": g, "D": d, "ref_step": steps_rel[j],
+                             "rel": abs(g - ref) / abs(ref), "res_rel": res / abs(ref),
+                             "agree": abs(g - ref) <= max(1e-5 * abs(ref), res),
+                             "rel_h1e-6": abs(g - d[0]) / abs(d[0]), "res_h1e-6": abs(d[0] - d[1]) / abs(d[0])})
+            rel = np.array([r["rel"] for r in rows])
+            rel6 = np.array([r["rel_h1e-6"] for r in rows])
+            gv = np.array([r["g"] for r in rows])
+            dref = np.array([r["D"][int(np.log10(r["ref_step"])) + 6] for r in rows])
+            fd_out[which] = {
+                "coords": len(rows), "agree_by_rule": int(sum(r["agree"] for r in rows)),
+                "within_1e-5_of_D_ref": int((rel <= 1e-5).sum()), "median_rel_vs_D_ref": float(np.median(rel)),
+                "max_rel_vs_D_ref": float(rel.max()),
+                "normwise_rel_vs_D_ref": float(np.abs(gv - dref).max() / np.abs(dref).max()),
+                "h1e-6": {"within_1e-5": int((rel6 <= 1e-5).sum()), "median_rel": float(np.median(rel6)),
+                          "max_rel": float(rel6.max())},
+                "ref_step_counts": {str(h): int(sum(r["ref_step"] == h for r in rows)) for h in steps_rel[:2]},
+                "disagreeing": [r for r in rows if not r["agree"]],
+            }
+        fd_out["wall_s"] = time.perf_counter() - t0
         line["fd_check"] = fd_out
     return line
 
