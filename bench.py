@@ -38,9 +38,10 @@ METRIC = "pair-interactions/s mixed vs FP64 GPU at |ΔE/E|≤1e-6; ensemble step
 UNIT = "pair-interactions/s"
 FLOPS_PER_INTERACTION = 20
 # dram__bytes_read.sum + dram__bytes_write.sum of one force_mixed_kernel launch, from an ncu capture
-# (--metrics dram__bytes_read.sum,dram__bytes_write.sum) of this workload: (N, variant) -> bytes.
-# The positions (N x 32 B = 8.39 MB at N = 262144) are read once; the partial sums stay in L2.
-NCU_FORCE_TRAFFIC = {(262144, 8): 8688384 + 5120}
+# (--metrics dram__bytes_read.sum,dram__bytes_write.sum, one launch at N = 262144): (N, variant) ->
+# (read, write).  The positions (N x 32 B = 8.39 MB) are read about once; the writes are the work
+# units' FP64 partial sums (units x 3 x 8 B per i-body), of which part stays in L2.
+NCU_FORCE_TRAFFIC = {(262144, 2): (12063744, 179496448), (262144, 8): (11524096, 177701888)}
 
 
 def parse_args():
@@ -68,7 +69,11 @@ def parse_args():
                    help="rows of the N-body force checked against the CPU oracle (untimed)")
     p.add_argument("--configs", choices=["all", "none"], default="all",
                    help="after the headline (untimed, one GPU): the other configurations of the path")
-    p.add_argument("--workload", choices=["direct-mixed", "direct-fp64-1024", "bh", "ensemble", "adjoint", "comet"],
+    p.add_argument("--force-prec", choices=["mixed", "f64"], default="mixed",
+                   help="--workload force: precision of the force evaluations")
+    p.add_argument("--force-calls", type=int, default=3, help="--workload force: evaluations (profiling driver)")
+    p.add_argument("--workload", choices=["direct-mixed", "direct-fp64-1024", "bh", "ensemble", "adjoint", "comet",
+                                          "force"],
                    default="direct-mixed", help="direct-mixed is the headline; the others print their own line")
     p.add_argument("--bh-n", type=int, default=4194304)
     p.add_argument("--bh-cpu-n", type=int, default=10000)
@@ -90,7 +95,8 @@ def parse_args():
                    help="eager: the device-callback loop with one launch per kernel and a host read of the "
                         "verdict per step (the form ncu can profile kernel by kernel)")
     p.add_argument("--mixed-variant", type=int, default=-1,
-                   help="use this mixed force-kernel variant instead of the autotuner's choice")
+                   help="use this mixed force-kernel variant instead of the autotuner's choice (with "
+                        "--workload force: the variant of --force-prec)")
     return p.parse_args()
 
 
@@ -380,6 +386,9 @@ def run_ours(args, rank, world, local):
         tuned[name] = {"variant": best.value, "i_per_thread": ii.value, "fold": fold.value,
                        "force_ms": best_ms.value}
 
+    units, part_bytes = C.c_int64(), C.c_int64()
+    check(L.gtd_system_direct_plan_info(hmx, C.byref(units), C.byref(part_bytes)))
+
     stage("accuracy")
     # --- accelerations of both paths at the initial state (untimed); checked against the oracle
     # beside the CPU baseline below, and against each other here
@@ -516,9 +525,13 @@ def run_ours(args, rank, world, local):
                          "energy_drift_rel": drift, "energy_drift_steps": W + K},
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
                          "unit": "TFLOP/s", "frac": achieved / peak.value,
-                         "traffic": NCU_FORCE_TRAFFIC.get((n, tuned["mixed"]["variant"])),
+                         "traffic": (sum(NCU_FORCE_TRAFFIC[(n, tuned["mixed"]["variant"])])
+                                     if (n, tuned["mixed"]["variant"]) in NCU_FORCE_TRAFFIC else None),
+                         "traffic_read_write": NCU_FORCE_TRAFFIC.get((n, tuned["mixed"]["variant"])),
                          "traffic_unit": "bytes per launch (ncu dram read + write)",
-                         "algorithmic_bytes": 32 * n,
+                         "algorithmic_bytes": 32 * n + part_bytes.value,
+                         "algorithmic_bytes_note": "positions 32 B per body read once + the work units' FP64 "
+                                                   f"partial sums ({units.value} units)",
                          "kernel": "force_mixed_kernel", "flops_per_interaction": FLOPS_PER_INTERACTION,
                          "peak_source": "measured FFMA/FFMA2 microkernel on this GPU (gtd_measure_fma_peak)",
                          "fp64_peak": peak64.value / 1e12, "hbm_peak_GBs": hbm_peak / 1e9,
@@ -849,6 +862,40 @@ def cfg_adjoint(args, local, peak32=None, peak64=None, hbm=None):
     return line
 
 
+def run_force(args, local):
+    """Profiling driver: --force-calls direct-sum force evaluations (gtd_system_accelerations) of the
+    seeded N = --n Plummer sphere in --force-prec, force-kernel variant --mixed-variant (the
+    process default when < 0), near factor 8; prints the CUDA-event time of each call."""
+    import torch
+
+    from gregpackagescpp_b200 import _lib
+    from gregpackagescpp_b200._lib import check
+    from gregpackagescpp_b200.ics import plummer
+    L = _lib.load()
+    n = args.n
+    m, x, v = plummer(n, args.seed)
+    x3, v3 = np.ascontiguousarray(x.reshape(-1)), np.ascontiguousarray(v.reshape(-1))
+    prec = _lib.PREC_MIXED if args.force_prec == "mixed" else _lib.PREC_F64
+    h = C.c_void_p()
+    check(L.gtd_system_create(C.byref(h), local, prec))
+    check(L.gtd_system_set_params(h, 6.674e-11, 3600.0, 10, 0.0, 0.5))
+    check(L.gtd_system_upload(h, n, m.ctypes.data, None, None, x3.ctypes.data, v3.ctypes.data))
+    if args.mixed_variant >= 0:
+        check(L.gtd_system_set_direct_variant(h, args.mixed_variant))
+    a = np.zeros(3 * n)
+    ms = []
+    for _ in range(args.force_calls):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        check(L.gtd_system_accelerations(h, 0, a.ctypes.data))
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    check(L.gtd_system_destroy(h))
+    print(json.dumps({"workload": f"{args.force_prec} force evaluations, N={n}", "variant": args.mixed_variant,
+                      "call_ms": ms}), flush=True)
+
+
 def run_comet(args, local):
     """random_comet's evolve stage as rsl9.cpp drives it (gregsys.hpp:1881-1984): N=727 bodies of
     75 m and 4.197e9 kg at rest in a 1600 m ball, n_exp = 3, d_scale = 1200 m, restitution 0.5..0.95,
@@ -955,6 +1002,8 @@ def main():
             if rank == 0:
                 if args.workload == "comet":
                     run_comet(args, local)
+                elif args.workload == "force":
+                    run_force(args, local)
                 else:
                     fn = {"direct-fp64-1024": cfg_fp64_small, "bh": cfg_bh, "ensemble": cfg_ensemble,
                           "adjoint": cfg_adjoint}[args.workload]

@@ -151,6 +151,7 @@ def load():
     L.gtd_system_set_direct_variant.argtypes = [vp, ip]
     L.gtd_system_autotune_direct.argtypes = [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.gtd_system_set_mixed_near_factor.argtypes = [vp, C.c_double]
+    L.gtd_system_direct_plan_info.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
     L.gtd_bh_build.argtypes = [vp, ip]
     L.gtd_bh_set_tree_float.argtypes = [vp, ip]
     L.gtd_bh_set_walk_variant.argtypes = [vp, ip]

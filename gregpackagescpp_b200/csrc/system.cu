@@ -733,6 +733,17 @@ int gtd_system_set_direct_variant(gtd_system *s, int variant) {
     return GTD_OK;
 }
 
+int gtd_system_direct_plan_info(gtd_system *s, int64_t *units, int64_t *partial_bytes_out) {
+    if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
+    if (s->n == 0) return fail(GTD_ERR_INVALID_ARGUMENT, "no bodies");
+    DeviceGuard g(s->device);
+    int rc = ensure_plan(s);
+    if (rc) return rc;
+    if (units) *units = s->plan.segs > 0 ? s->plan.units : s->plan.total;
+    if (partial_bytes_out) *partial_bytes_out = (int64_t)partial_bytes(s->plan);
+    return GTD_OK;
+}
+
 int gtd_system_set_mixed_near_factor(gtd_system *s, double k) {
     if (!s) return fail(GTD_ERR_INVALID_ARGUMENT, "system is NULL");
     if (!(k == k)) return fail(GTD_ERR_INVALID_ARGUMENT, "near factor is NaN");

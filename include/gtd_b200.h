@@ -273,6 +273,10 @@ GTD_API int gtd_system_autotune_direct(gtd_system *sys, int reps, int *best, dou
  * than k 2^-24 of its relative accuracy to their rounding, so the j-range holding it is summed
  * again from hi/lo coordinate splits.  Default k = 8; k <= 1 turns the check off. */
 GTD_API int gtd_system_set_mixed_near_factor(gtd_system *sys, double k);
+/* The split of the handle's direct-sum force (no counterpart in the reference): the work units of
+ * one force evaluation (mixed: (row, segment) units taken from a work queue; FP64: (row, tile)
+ * pairs) and the bytes of partial sums they write. */
+GTD_API int gtd_system_direct_plan_info(gtd_system *sys, int64_t *units, int64_t *partial_bytes);
 /* Measured throughput of a dependent-FMA microkernel on `device` (all SMs): precision
  * GTD_PREC_MIXED gives FP32 FFMA FLOP/s, GTD_PREC_F64 gives FP64 DFMA FLOP/s (2 flops per FMA). */
 GTD_API int gtd_measure_fma_peak(int device, int precision, double *flops_per_s);
