@@ -8,8 +8,9 @@
 // caller's own kernels.  The predicate's verdict stays on the device: the loop is a CUDA graph whose
 // WHILE node runs up to kChunkSteps steps, each behind IF nodes that the predicate kernel opens or
 // closes, so the host waits once per chunk.  Cases the graph cannot hold (merging collisions, the
-// periodic Morton reorder of the mixed path, force timing) run the same kernels eagerly with one
-// 64-byte read of the verdict per step; the bodies never cross PCIe in either form.
+// periodic spatial reorder of the mixed path, force timing, memFreq recording) run the same kernels
+// eagerly with one 64-byte read of the verdict per step; the bodies never cross PCIe in either form
+// (a recorded frame is read back when it is made, every memFreq-th step).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -222,6 +223,10 @@ static int callback_step(gtd_system *s, bool capture, const cudaGraphConditional
         }
         rc = enqueue_collisions(s, &hk);
         if (rc) return rc;
+    }
+    if (!capture && s->rec_every) {  // s_coll<true> records after the collision pass, before for_each_bod
+        s->rec_step += 1;
+        if (s->rec_step % s->rec_every == 0 && (rc = record_frame(s, s->rec_step))) return rc;
     }
     if (s->cb.each_fn) return run_hook(s, s->cb.each_fn, s->cb.each_user, "for_each_bod");
     return GTD_OK;
@@ -498,7 +503,6 @@ int gtd_system_evolve_callbacks(gtd_system *s, int method, uint64_t max_steps, u
         return rc;
     }
     if (branch == GTD_TWO_BODY || branch == GTD_RK4 || branch == GTD_RK3_8) return gtd_system_evolve(s, method, elapsed_ns);
-    if (s->rec_every) return fail(GTD_ERR_UNSUPPORTED, "trajectory recording with device callbacks is not supported");
     DeviceGuard g(s->device);
     int rc = ensure_ctl(s);
     if (rc) return rc;
@@ -509,8 +513,9 @@ int gtd_system_evolve_callbacks(gtd_system *s, int method, uint64_t max_steps, u
     GTD_CHECK_LAUNCH();
     s->launches += 1;
     uint64_t waits = 0;
+    // recorded frames are read back as they are made: a recording evolve runs eagerly
     const bool graphable = s->coll != GTD_MERGE_COLL && !(s->precision == GTD_PREC_MIXED && s->coll == GTD_NO_COLL) &&
-                           !s->time_force;
+                           !s->time_force && !s->rec_every;
     cudaGraphExec_t exec = nullptr;
     int flips = 0, verdicts_apart = 0;
     uint64_t per_step = 0;

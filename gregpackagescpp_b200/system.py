@@ -317,18 +317,15 @@ class System:
             x0, v0 = self.x.copy(), self.v.copy()
             check(self._L.gtd_system_evolve(self._h, integration_method, C.byref(ns)))
             self._pull()
-            if self.mem_freq and len(self.m):
-                self.x, self.v, cur = x0, v0, (self.x, self.v)
-                self._collect_recordings(integration_method)
-                self.x, self.v = cur
+            self._recordings_from(x0, v0, integration_method)
             self.time_elapsed = self.iterations * self.dt
             return ns.value
-        if self.mem_freq:
-            raise NotImplementedError("memFreq recordings with evolve callbacks are not supported")
+        x0, v0 = self.x.copy(), self.v.copy()
         if (integration_method & System.barnes_hut) == System.barnes_hut:
             # the Barnes-Hut branch calls no callback (gregsys.hpp:2893-2945)
             check(self._L.gtd_system_evolve(self._h, integration_method, C.byref(ns)))
             self._pull()
+            self._recordings_from(x0, v0, integration_method)
             self.time_elapsed = self.iterations * self.dt
             return ns.value
         err = []
@@ -365,6 +362,7 @@ class System:
             if hook is not None:
                 L.gtd_system_set_step_hook(self._h, None, None)
         self._pull()
+        self._recordings_from(x0, v0, integration_method)
         self.time_elapsed = self.iterations * self.dt  # gregsys.hpp:3069, whatever the steps taken
         self.steps_taken = steps
         return 0
@@ -383,6 +381,7 @@ class System:
 
     def _evolve_device(self, method, cont, each, all_, max_steps) -> int:
         L, h = self._L, self._h
+        x0, v0 = self.x.copy(), self.v.copy()
         self._push()
         hooks = []
         for cb in (cont, each, all_):
@@ -406,6 +405,7 @@ class System:
         finally:
             L.gtd_system_set_device_callbacks(h, None, None, None, None, None, None)
         self._pull()
+        self._recordings_from(x0, v0, method)
         if isinstance(all_, RestFromCom):
             c = np.zeros(3)
             check(L.gtd_system_rest_from_com_centre(h, ptr(c)))
@@ -432,6 +432,13 @@ class System:
         self.pe = np.zeros((0, n))
         self.energies = np.zeros((0, n))
         self.tot_pe, self.tot_ke, self.tot_e = np.zeros(0), np.zeros(0), np.zeros(0)
+
+    def _recordings_from(self, x0, v0, method: int) -> None:
+        """The last evolve's records, its first frame the state (x0, v0) it started from."""
+        if self.mem_freq and len(self.m):
+            self.x, self.v, cur = x0, v0, (self.x, self.v)
+            self._collect_recordings(method)
+            self.x, self.v = cur
 
     def _collect_recordings(self, method: int) -> None:
         """The records the reference keeps (fileFreq = 0, the only setting with which its evolve

@@ -4,8 +4,9 @@
 // calls and is gathered to the device SoA at evolve() entry and scattered back at exit.
 //
 // Differences, all documented in the engine: no long double arithmetic on the device (FP64 is used
-// for every T); trajectory recording (memFreq), file output (fileFreq) and progress printing are
-// not performed; evolve-time merges use check_overlap's scan as that routine intends.  .nsys files
+// for every T); per-step file output (fileFreq) and progress printing are not performed (memFreq
+// recordings are, from frames computed on the device); evolve-time merges use check_overlap's scan
+// as that routine intends.  .nsys files
 // (to_nsys and the path constructor) are written and read by the engine, for floating-point M, R
 // and T.
 #ifndef GTD_B200_GREGSYS_HPP
@@ -461,7 +462,6 @@ public:
                               (std::same_as<bodFuncT, std::nullptr_t> || device::is_callback<bodFuncT>::value) &&
                               (std::same_as<bodsFuncT, std::nullptr_t> || device::is_callback<bodsFuncT>::value),
                           "device callbacks and host callables cannot be mixed in one evolve");
-            static_assert(memFreq == 0, "memFreq recordings with evolve callbacks are not supported by the engine");
             gtd_device_hook cf = nullptr, ef = nullptr, af = nullptr;
             void *cu = nullptr, *eu = nullptr, *au = nullptr;
             if constexpr (std::same_as<evFuncT, device::hook>) { cf = continue_ev_if.fn; cu = continue_ev_if.user; }
@@ -482,6 +482,7 @@ public:
             int64_t ns = 0;
             throw_status(gtd_system_evolve_callbacks(dev, integration_method, callback_step_limit, &steps, &ns));
             pull();
+            if constexpr (memFreq != 0) collect_recordings(integration_method);
             if constexpr (device::is_rest_from_com<bodsFuncT>::value) {
                 double c[3];
                 throw_status(gtd_system_rest_from_com_centre(dev, c));
@@ -493,7 +494,6 @@ public:
             time_elapsed = iterations * dt;  // gregsys.hpp:3069, whatever the steps taken
             return std::chrono::nanoseconds{ns};
         } else {
-            static_assert(memFreq == 0, "memFreq recordings with evolve callbacks are not supported by the engine");
             // host callables see the bodies every step: the state makes a host round trip for them.
             // Order per step (gregsys.hpp:16-106, 2970-2987): continue_ev_if, the update, for_all_bods
             // (inside the step, before the collision pass), the collision pass, for_each_bod.
@@ -502,6 +502,7 @@ public:
                 int64_t ns = 0;
                 throw_status(gtd_system_evolve(dev, integration_method, &ns));
                 pull();
+                if constexpr (memFreq != 0) collect_recordings(integration_method);
                 time_elapsed = iterations * dt;
                 return std::chrono::nanoseconds{ns};
             }
@@ -547,6 +548,7 @@ public:
                 }
             }
             pull();
+            if constexpr (memFreq != 0) collect_recordings(integration_method);
             time_elapsed = iterations * dt;  // gregsys.hpp:3069, whatever the steps taken
             return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - start);
         }

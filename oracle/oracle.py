@@ -282,6 +282,12 @@ class RefOracle:
                                            C.c_char_p, C.c_int, C.c_double, C.c_uint64, C.c_int, C.c_double,
                                            C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double,
                                            C.c_uint64, _dp, _dp, _dp, _dp, C.POINTER(C.c_uint64)]
+        L.ref_evolve_record_callbacks.restype = C.c_int
+        L.ref_evolve_record_callbacks.argtypes = (
+            [C.c_int, C.c_int, C.c_uint64, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_uint64, C.c_char_p,
+             C.c_int, C.c_double, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+             C.c_int, C.c_double, C.c_uint64, _dp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+            + [_dp] * 9 + [C.POINTER(C.c_uint64)])
 
     def _chk(self, rc):
         if rc < 0:
@@ -308,6 +314,35 @@ class RefOracle:
             int(mw), 1 if each_factor is not None else 0, each_factor or 1.0, max_steps, com, xo, vo, ro,
             C.byref(steps)))
         return xo.reshape(n, 3), vo.reshape(n, 3), ro, steps.value, com
+
+    def evolve_record_callbacks(self, method, m, x, v, dt, iterations, units, mem_freq, r=None, rest=None, coll=0,
+                                cont=None, rest_from_com=None, each_factor=None, max_steps=0, max_frames=None):
+        """evolve_callbacks of a system with memFreq = mem_freq (1, 2 or 3): the recordings as
+        evolve_record, plus x, v, rest, steps and the carried centre (com)."""
+        n = len(m)
+        F = max_frames or (max(iterations, max_steps) + 2)
+        pos, vel = np.zeros(F * n * 3), np.zeros(F * n * 3)
+        ke, pe, en, tot = np.zeros(F * n), np.zeros(F * n), np.zeros(F * n), np.zeros(F * 3)
+        xo, vo, ro = np.zeros(3 * n), np.zeros(3 * n), np.zeros(n)
+        pf, ef = C.c_int(), C.c_int()
+        r = _c3(np.zeros(n) if r is None else r)
+        rest = _c3(np.ones(n) if rest is None else rest)
+        mmc, probing = cont if cont is not None else (0.0, 0)
+        mn, mx, sc, ne, com, mw = rest_from_com if rest_from_com is not None else (0.0, 1.0, 1.0, 1.0, (0, 0, 0), 0)
+        com = np.ascontiguousarray(np.asarray(com, dtype=np.float64).copy())
+        steps = C.c_uint64()
+        self._chk(self.lib.ref_evolve_record_callbacks(
+            method, coll, mem_freq, n, _c3(m), r, rest, _c3(x), _c3(v), dt, iterations, units.encode(),
+            1 if cont is not None else 0, mmc, probing, 1 if rest_from_com is not None else 0, mn, mx, sc, ne,
+            int(mw), 1 if each_factor is not None else 0, each_factor or 1.0, max_steps, com, F, C.byref(pf),
+            C.byref(ef), pos, vel, ke, pe, en, tot, xo, vo, ro, C.byref(steps)))
+        p, e = pf.value, ef.value
+        if max(p, e) > F:
+            raise RuntimeError(f"{max(p, e)} frames recorded, room for {F}")
+        return dict(pos=pos[:p * n * 3].reshape(p, n, 3), vel=vel[:p * n * 3].reshape(p, n, 3),
+                    ke=ke[:p * n].reshape(p, n), pe=pe[:e * n].reshape(e, n), energy=en[:e * n].reshape(e, n),
+                    tot=tot[:e * 3].reshape(e, 3), x=xo.reshape(n, 3), v=vo.reshape(n, 3), rest=ro,
+                    steps=steps.value, com=com)
 
     def G(self, units="M66743:66740,D1:1,T1:1"):
         g = C.c_longdouble()

@@ -625,23 +625,48 @@ int ref_load_nsys(int kind, const char *path, int alloc, int check, int max_n, i
 /* evolve with trajectory recording: gtd::system<double,double,double,false,false,coll,MF,FF,false>,
  * evolve(method) called `calls` times (a second call clears the first one's recordings,
  * gregsys.hpp:2615-2619, 2569-2586); the recordings of the last call and the final state. */
+template <uint64_t MF>
+static std::vector<gtd::body<double, double, double, MF>> rec_bodies(int n, const double *m, const double *r,
+                                                                     const double *rest, const double *x3,
+                                                                     const double *v3) {
+    std::vector<gtd::body<double, double, double, MF>> v;
+    v.reserve(n);
+    for (int i = 0; i < n; ++i)
+        v.emplace_back(m[i], r ? r[i] : 0.0, gtd::vector3D<double>{x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]},
+                       gtd::vector3D<double>{v3[3 * i], v3[3 * i + 1], v3[3 * i + 2]},
+                       rest ? (long double)rest[i] : 1.0L);
+    return v;
+}
+
 template <int coll, uint64_t MF, uint64_t FF>
 static int evolve_rec_impl(int method, int n, const double *m, const double *r, const double *rest, const double *x3,
                            const double *v3, double dt, uint64_t steps, const char *units, int calls, int max_frames,
                            int *pos_frames, int *pe_frames, double *pos3, double *vel3, double *ke, double *pe,
                            double *energy, double *tot3, double *x3o, double *v3o) {
     using sys_t = gtd::system<double, double, double, false, false, coll, MF, FF, false>;
-    using bod_t = gtd::body<double, double, double, MF>;
-    std::vector<bod_t> v;
-    v.reserve(n);
-    for (int i = 0; i < n; ++i)
-        v.emplace_back(m[i], r ? r[i] : 0.0, gtd::vector3D<double>{x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]},
-                       gtd::vector3D<double>{v3[3 * i], v3[3 * i + 1], v3[3 * i + 2]},
-                       rest ? (long double)rest[i] : 1.0L);
-    sys_t s{std::move(v), (long double)dt, steps, units, true};
+    sys_t s{rec_bodies<MF>(n, m, r, rest, x3, v3), (long double)dt, steps, units, true};
     for (int c = 0; c < calls; ++c) s.evolve(method);
     ref_access::recordings(s, max_frames, pos_frames, pe_frames, pos3, vel3, ke, pe, energy, tot3);
     read_back(s, x3o, v3o, nullptr, nullptr, nullptr);
+    return 0;
+}
+
+/* evolve(method, continue_ev_if, for_each_bod, for_all_bods) of a system with memFreq = MF (fileFreq
+ * 0), the callbacks of ref_access::evolve_callbacks: the recordings (FUNC_TEMPL_SELECT,
+ * gregsys.hpp:16-106, inside the callback loops), the final state, every rest_c and the steps. */
+template <int coll, uint64_t MF>
+static int evolve_rec_cb_impl(int method, int n, const double *m, const double *r, const double *rest,
+                              const double *x3, const double *v3, double dt, uint64_t iterations, const char *units,
+                              const ref_access::cb_args &p, double *com_io, int max_frames, int *pos_frames,
+                              int *pe_frames, double *pos3, double *vel3, double *ke, double *pe, double *energy,
+                              double *tot3, double *x3o, double *v3o, double *rest_o, uint64_t *steps) {
+    using sys_t = gtd::system<double, double, double, false, false, coll, MF, 0, false>;
+    sys_t s{rec_bodies<MF>(n, m, r, rest, x3, v3), (long double)dt, iterations, units, true};
+    *steps = ref_access::evolve_callbacks(s, method, p, com_io);
+    ref_access::recordings(s, max_frames, pos_frames, pe_frames, pos3, vel3, ke, pe, energy, tot3);
+    read_back(s, x3o, v3o, nullptr, nullptr, nullptr);
+    auto &b = ref_access::bodies(s);
+    for (size_t i = 0; i < b.size(); ++i) rest_o[i] = (double)ref_access::rest(b[i]);
     return 0;
 }
 
@@ -664,6 +689,32 @@ int ref_evolve_record(int method, int coll, uint64_t mem_freq, uint64_t file_fre
 #undef REC_CASE
     std::snprintf(g_err, sizeof g_err, "unsupported coll %d / mem_freq %llu / file_freq %llu", coll,
                   (unsigned long long)mem_freq, (unsigned long long)file_freq);
+    return -1;
+    REF_CATCH
+}
+
+/* mem_freq 1, 2 or 3; coll 0 or 3; the callback arguments as ref_evolve_callbacks. */
+int ref_evolve_record_callbacks(int method, int coll, uint64_t mem_freq, int n, const double *m, const double *r,
+                                const double *rest, const double *x3, const double *v3, double dt,
+                                uint64_t iterations, const char *units, int cont_mode, double min_max_cor,
+                                uint64_t probing_iters, int all_mode, double min_cor, double max_cor,
+                                double scale_factor, double n_exp, int mass_weighted, int each_mode,
+                                double each_factor, uint64_t max_steps, double *com_io, int max_frames,
+                                int *pos_frames, int *pe_frames, double *pos3, double *vel3, double *ke, double *pe,
+                                double *energy, double *tot3, double *x3o, double *v3o, double *rest_o,
+                                uint64_t *steps) {
+    REF_TRY
+    const ref_access::cb_args p{cont_mode, all_mode, each_mode, mass_weighted, (long double)min_max_cor,
+                                (long double)min_cor, (long double)max_cor, (long double)scale_factor,
+                                (long double)n_exp, probing_iters, max_steps, each_factor};
+#define REC_CB_CASE(C, F)                                                                                      \
+    if (coll == C && mem_freq == F)                                                                            \
+        return evolve_rec_cb_impl<C, F>(method, n, m, r, rest, x3, v3, dt, iterations, units, p, com_io,       \
+                                        max_frames, pos_frames, pe_frames, pos3, vel3, ke, pe, energy, tot3, x3o, \
+                                        v3o, rest_o, steps);
+    REC_CB_CASE(0, 1) REC_CB_CASE(0, 2) REC_CB_CASE(0, 3) REC_CB_CASE(3, 1) REC_CB_CASE(3, 2) REC_CB_CASE(3, 3)
+#undef REC_CB_CASE
+    std::snprintf(g_err, sizeof g_err, "unsupported coll %d / mem_freq %llu", coll, (unsigned long long)mem_freq);
     return -1;
     REF_CATCH
 }

@@ -165,6 +165,52 @@ int main() {
                     cerr, perr / scale);
         fails += !(err / scale < 1e-12 && rerr < 1e-12 && cerr < 1e-13 && perr == 0.0);
     }
+    {  // memFreq recordings with evolve callbacks: a host for_all_bods lambda and the device functor
+       // record the same frames; a predicate true 6 times records what 6 iterations record
+        using rsys_t = gtd::system<double, double, double, false, false, 3, 2, 0, false>;
+        const auto ci = make(64, 29, 1.5e10);
+        const int n = (int)ci.size();
+        std::vector<rsys_t::bod_t> rb;
+        for (const auto &b : ci) rb.emplace_back(b.mass(), b.rad(), b.pos(), b.vel(), b.restitution());
+        gtd::vector3D<double> mean{};
+        for (const bod &b : ci) mean += b.pos();
+        mean = gtd::vector3D<double>{mean.x / n, mean.y / n, mean.z / n};
+        const long double sf = 1e22L, min_cor = 0.5L, max_cor = 1.0L;
+        rsys_t h{rb, 3600, 6, "M66743:66740,D1:1,T1:1", true};
+        gtd::vector3D<double> hcom = mean;
+        h.evolve(rsys_t::leapfrog_kdk, nullptr, nullptr, [&](std::vector<rsys_t::bod_t> &bs) {
+            for (const auto &b : bs) hcom += b.pos();
+            hcom = gtd::vector3D<double>{hcom.x / n, hcom.y / n, hcom.z / n};
+            for (auto &b : bs) {
+                const long double de = powl((b.pos() - hcom).magnitude(), 2.0L);
+                b.set_restitution(max_cor - (max_cor - min_cor) * (de / (de + sf)));
+            }
+        });
+        rsys_t d{rb, 3600, 6, "M66743:66740,D1:1,T1:1", true};
+        gtd::vector3D<double> dcom = mean;
+        d.evolve(rsys_t::leapfrog_kdk, nullptr, nullptr,
+                 gtd::device::rest_from_com<double>{min_cor, max_cor, sf, 2.0L, &dcom});
+        uint64_t k = 0;
+        rsys_t p{rb, 3600, 100, "M66743:66740,D1:1,T1:1", true};
+        p.evolve(rsys_t::leapfrog_kdk, [&]() { return k++ < 6; });
+        rsys_t q{rb, 3600, 6, "M66743:66740,D1:1,T1:1", true};
+        q.evolve(rsys_t::leapfrog_kdk);
+        bool ok = h[0].get_positions().size() == 4 && d[0].get_positions().size() == 4 &&
+                  p[0].get_positions().size() == 4 && h.recorded_total_e().size() == 4 &&
+                  d.recorded_total_e().size() == 4 && p.recorded_total_e().size() == 4;
+        double err = 0, scale = 0, perr = 0;
+        for (int i = 0; ok && i < n; ++i)
+            for (size_t f = 0; f < 4; ++f) {
+                const auto &a = h[i].get_positions()[f], &b = d[i].get_positions()[f];
+                err = std::fmax(err, std::fabs(a.x - b.x) + std::fabs(a.y - b.y) + std::fabs(a.z - b.z));
+                scale = std::fmax(scale, std::fabs(a.x));
+                perr = std::fmax(perr, std::fabs(p[i].get_positions()[f].z - q[i].get_positions()[f].z));
+            }
+        for (size_t f = 0; ok && f < 4; ++f) perr = std::fmax(perr, std::fabs(p.recorded_total_e()[f] - q.recorded_total_e()[f]));
+        std::printf("memFreq with callbacks: frames %d, host vs device %.3e, predicate vs iterations %.3e\n",
+                    (int)ok, ok ? err / scale : -1.0, perr);
+        fails += !(ok && err / scale < 1e-12 && perr == 0.0);
+    }
     std::printf(fails ? "FAIL\n" : "OK\n");
     return fails ? 1 : 0;
 }

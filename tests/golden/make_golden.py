@@ -224,6 +224,30 @@ def callback_fixtures(r, out):
     out["cbp_cases"] = np.array(cases)
 
 
+def record_callback_fixtures(r, out):
+    """memFreq recordings of evolve(method, callbacks) (FUNC_TEMPL_SELECT inside the callback loops,
+    gregsys.hpp:16-106): (1) the 8 collisional steps of callback_fixtures (2) with for_all_bods and
+    for_each_bod, memFreq 1 and 3, every method; (2) the predicate alone on the collisionless
+    Plummer sphere, 7 probing steps, memFreq 2, the leapfrogs and Euler."""
+    c = comet_setup(n=48, R=5.0, b=1.0, mass=4e9, seed=5)
+    for name, meth in METHODS.items():
+        for f in (1, 3):
+            d = r.evolve_record_callbacks(meth, c["m"], c["x"], c["v"], 0.25, 8, CB_UNITS, f, r=c["r"], rest=c["rest"],
+                                          coll=3, rest_from_com=(0.5, 1.0, c["sf"], 2.0, c["com"], False),
+                                          each_factor=0.999)
+            key = f"rcb_{name}_{f}"
+            for k in ("pos", "vel", "ke", "pe", "energy", "tot", "x", "v", "rest", "com"):
+                out[f"{key}_{k}"] = d[k]
+    m, x, v = plummer(40, 11)
+    for name in ("leapfrog_kdk", "leapfrog_dkd", "euler"):
+        d = r.evolve_record_callbacks(METHODS[name], m, x, v, 3600.0, 1000, UNITS_G6674, 2, rest=np.full(40, 0.9),
+                                      cont=(0.5, 7), max_frames=64)
+        key = f"rcp_{name}"
+        for k in ("pos", "vel", "ke", "pe", "energy", "tot", "x", "v"):
+            out[f"{key}_{k}"] = d[k]
+        out[f"{key}_steps"] = np.array(d["steps"])
+
+
 TREE_WALK_N = 2000
 
 
@@ -336,6 +360,7 @@ def main():
     nsys_fixtures(r, out)
     record_fixtures(r, out)
     callback_fixtures(r, out)
+    record_callback_fixtures(r, out)
     path = os.path.join(HERE, "reference_golden.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes,", len(out), "arrays")

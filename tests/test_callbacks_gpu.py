@@ -15,9 +15,6 @@ perturbations out of 24, so its end step is checked exactly; the m-weighted one 
 step 244 to 368 under them (263 unperturbed), so its full run is checked for an end in that range
 only.  The engine's per-step differences are FP64 rounding against the reference's long-double
 intermediates."""
-import ctypes as C
-import os
-import subprocess
 
 import numpy as np
 import pytest
@@ -27,33 +24,12 @@ from gregpackagescpp_b200.ics import UNITS_G6674
 
 pytestmark = pytest.mark.gpu
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 METHODS = {"euler": 2, "modified_euler": 4, "midpoint": 8, "leapfrog_kdk": 16, "leapfrog_dkd": 32}
 CB_UNITS = "M1:1,D1:1,T1:1"
 
 
 def _rel(a, b):
     return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))
-
-
-@pytest.fixture(scope="module")
-def hooks(tmp_path_factory):
-    """tests/cpp/device_hooks.cu compiled with nvcc into a scratch library."""
-    out = str(tmp_path_factory.mktemp("hooks") / "device_hooks.so")
-    nvcc = "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc"
-    r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-shared", "-Xcompiler", "-fPIC",
-                        "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "device_hooks.cu"),
-                        "-o", out], capture_output=True, text=True)
-    assert r.returncode == 0, r.stderr[-3000:]
-    lib = C.CDLL(out)
-    lib.make_scale_args.restype = C.c_void_p
-    lib.make_scale_args.argtypes = [C.c_double]
-    lib.make_count_args.restype = C.c_void_p
-    lib.make_count_args.argtypes = [C.c_uint64]
-    lib.reset_count_args.argtypes = [C.c_void_p]
-    lib.free_args.argtypes = [C.c_void_p, C.c_int]
-    lib.addr = lambda name: C.cast(getattr(lib, name), C.c_void_p).value
-    return lib
 
 
 def _comet_system(g, tag, iterations=1000):

@@ -62,3 +62,100 @@ def test_frames_in_upload_order_after_mixed_reordering(gpu):
     assert a.positions.shape == b.positions.shape == (4, 3000, 3)
     assert rel(b.positions, a.positions) < 1e-9
     assert rel(b.pe, a.pe) < 1e-9
+
+
+# ---- recordings with evolve callbacks (FUNC_TEMPL_SELECT inside the callback loops) -----------
+CB_UNITS = "M1:1,D1:1,T1:1"
+
+
+def _check_records(s, g, key):
+    assert s.positions.shape == g[f"{key}_pos"].shape, key
+    assert s.pe.shape == g[f"{key}_pe"].shape, key
+    assert rel(s.positions, g[f"{key}_pos"]) < 1e-12, key
+    assert rel(s.velocities, g[f"{key}_vel"]) < 1e-10, key
+    assert rel(s.kinetic_energies, g[f"{key}_ke"]) < 1e-10, key
+    assert rel(s.pe, g[f"{key}_pe"]) < 1e-12, key
+    assert rel(s.energies, g[f"{key}_energy"]) < 1e-10, key
+    tot = np.stack([s.tot_pe, s.tot_ke, s.tot_e], 1) if len(s.tot_pe) else np.zeros((0, 3))
+    assert rel(tot, g[f"{key}_tot"]) < 1e-10, key
+    assert rel(s.x, g[f"{key}_x"]) < 1e-12 and rel(s.v, g[f"{key}_v"]) < 1e-10, key
+
+
+def _cbs_system(g, f):
+    return System(g["cbs_m"], g["cbs_x"], g["cbs_v"], r=g["cbs_r"], rest=g["cbs_rest"], timestep=0.25,
+                  num_iterations=8, units_format=CB_UNITS, collisions=3, mem_freq=f)
+
+
+@pytest.mark.parametrize("f", [1, 3])
+@pytest.mark.parametrize("name", list(METHODS))
+def test_recordings_with_host_callbacks(gpu, golden, name, f):
+    """8 collisional steps with host for_all_bods (restitution from the carried centre) and
+    for_each_bod (velocities x 0.999): the frames are taken after the collision pass and before
+    for_each_bod, every f-th step, as the reference's."""
+    g = golden
+    _, sf = g["cbs_par"]
+    s = _cbs_system(g, f)
+    com = g["cbs_com"].copy()
+    n = len(g["cbs_m"])
+
+    def for_all(sys_):
+        nonlocal com
+        acc = com.copy()
+        for i in range(n):
+            acc = acc + sys_.x[i]
+        com = acc / n
+        de = np.sum((sys_.x - com) ** 2, axis=1)
+        sys_.rest = 1.0 - (1.0 - 0.5) * (de / (de + sf))
+
+    def for_each(sys_, i):
+        sys_.v[i] = sys_.v[i] * 0.999
+
+    s.evolve(METHODS[name], None, for_each, for_all)
+    _check_records(s, g, f"rcb_{name}_{f}")
+    assert rel(s.rest, g[f"rcb_{name}_{f}_rest"]) < 1e-12
+
+
+@pytest.mark.parametrize("f", [1, 3])
+@pytest.mark.parametrize("name", list(METHODS))
+def test_recordings_with_device_callbacks(gpu, golden, hooks, name, f):
+    """The same steps with the built-in for_all_bods and a user for_each_bod hook on the device: a
+    recording evolve runs the callback loop eagerly and reads each frame back when it is made."""
+    from gregpackagescpp_b200 import DeviceHook, RestFromCom
+    g = golden
+    _, sf = g["cbs_par"]
+    s = _cbs_system(g, f)
+    args = hooks.make_scale_args(0.999)
+    try:
+        fab = RestFromCom(0.5, 1.0, sf, 2.0, g["cbs_com"])
+        s.evolve(METHODS[name], None, DeviceHook(hooks.addr("hook_scale_velocities"), args), fab)
+    finally:
+        hooks.free_args(args, 0)
+    assert s.steps_taken == 8 and not s.callback_stats()["graph_loop"]
+    _check_records(s, g, f"rcb_{name}_{f}")
+    assert rel(s.rest, g[f"rcb_{name}_{f}_rest"]) < 1e-12
+    assert rel(fab.com, g[f"rcb_{name}_{f}_com"]) < 1e-14
+
+
+@pytest.mark.parametrize("name", ["leapfrog_kdk", "leapfrog_dkd", "euler"])
+def test_recordings_with_predicate(gpu, golden, name):
+    """continue_ev_if alone (7 probing steps of the rest-below predicate, collisions off), memFreq 2:
+    as a host callable and as the device predicate, the reference's records."""
+    from gregpackagescpp_b200 import WhileRestBelow
+    g = golden
+    key = f"rcp_{name}"
+    assert int(g[f"{key}_steps"]) == 7
+    for device in (False, True):
+        s = System(g["cbp_m"], g["cbp_x"], g["cbp_v"], rest=g["cbp_rest_hi"], timestep=3600.0, num_iterations=1000,
+                   units_format=UNITS_G6674, mem_freq=2)
+        if device:
+            s.evolve(METHODS[name], WhileRestBelow(0.5, 7))
+        else:
+            k = [0]
+
+            def cont():
+                k[0] += 1
+                return k[0] <= 7
+
+            s.evolve(METHODS[name], cont)
+        assert s.steps_taken == 7
+        _check_records(s, g, key)
