@@ -82,6 +82,8 @@ def parse_args():
                    help="node records of the float-tree walk: -1 default, 0 separate arrays, 1 interleaved")
     p.add_argument("--ens-systems", type=int, default=4096)
     p.add_argument("--ens-steps", type=int, default=128, help="ensemble steps timed (after the warm-up chunk)")
+    p.add_argument("--ens-check-systems", type=int, default=12,
+                   help="ensemble systems re-run on the oracle after the timed steps (untimed)")
     p.add_argument("--ens-config", type=str, default="",
                    help="THREADS,BODIES_PER_THREAD for the ensemble kernel instead of the autotuner's choice")
     p.add_argument("--adj-n", type=int, default=16384)
@@ -764,7 +766,52 @@ def cfg_ensemble(args, local, peak32=None, peak64=None, hbm=None):
                                      "sample": "24 random systems, evolve(leapfrog_kdk) 4 steps, collisions off"}
     except Exception as exc:
         line["reference_cpu"] = {"unavailable": str(exc)}
+    if args.ens_check_systems > 0:
+        line["vs_oracle"] = ensemble_oracle_check(off, m, r, x, v, e.config(), local, args.ens_check_systems)
     return line
+
+
+def ensemble_oracle_check(off, m, r, x, v, config, local, n_check, steps=20, seed=11):
+    """The checker beside the ensemble line (untimed): the same ICs, 20 KDK steps with merges in one
+    batch on the GPU (the timed configuration), and n_check seeded systems re-run one by one on the
+    oracle (the reference's KDK, then its check_overlap merge scan after each step).  Survivors and
+    masses must match exactly; positions and velocities are reported relative to each system's
+    largest value (the FP32 pair forces carry the mixed bar of 1e-6 relative acceleration)."""
+    from gregpackagescpp_b200.ensemble import Ensemble
+    from oracle.oracle import Oracle
+    o = Oracle()
+    Gl = o.G("M66743:66740,D1:1,T1:1")
+    e = Ensemble(off, m, x, v, r, merge=True, dt=600.0, device=local)
+    e.set_threads(config[0])
+    e.set_bodies_per_thread(config[1])
+    e.evolve(steps)
+    st = e.state()
+    counts, merges, _ = e.counts()
+    pick = np.random.default_rng(seed).choice(len(off) - 1, n_check, replace=False)
+    t0 = time.perf_counter()
+    worst_x = worst_v = 0.0
+    same_survivors = same_mass = True
+    gpu_merges = oracle_merges = 0
+    for s in pick:
+        b, k = off[s], off[s + 1]
+        rows = np.concatenate([m[b:k, None], r[b:k, None], np.ones((k - b, 1)), x[b:k], v[b:k],
+                               np.zeros((k - b, 3))], 1)
+        rows = o.merge_overlapping(rows)
+        for _ in range(steps):
+            xo, vo, ao = o.evolve(16, rows[:, 0].copy(), rows[:, 3:6].copy(), rows[:, 6:9].copy(), 600.0, 1, Gl)
+            rows = o.merge_overlapping(np.concatenate([rows[:, 0:3], xo, vo, ao], axis=1))
+        gpu_merges += int((k - b) - counts[s])
+        oracle_merges += int((k - b) - len(rows))
+        if counts[s] != len(rows):
+            same_survivors = False
+            continue
+        same_mass &= bool(np.array_equal(st[s]["m"], rows[:, 0]))
+        worst_x = max(worst_x, float(np.abs(st[s]["x"] - rows[:, 3:6]).max() / np.abs(rows[:, 3:6]).max()))
+        worst_v = max(worst_v, float(np.abs(st[s]["v"] - rows[:, 6:9]).max() / np.abs(rows[:, 6:9]).max()))
+    return {"systems": int(n_check), "steps": steps, "bodies": int(sum(off[s + 1] - off[s] for s in pick)),
+            "same_survivors": same_survivors, "same_masses": same_mass, "merges_gpu": gpu_merges,
+            "merges_oracle": oracle_merges, "merges_all_systems_gpu": int(merges),
+            "x_rel_max": worst_x, "v_rel_max": worst_v, "oracle_s": time.perf_counter() - t0}
 
 
 def cfg_adjoint(args, local, peak32=None, peak64=None, hbm=None):

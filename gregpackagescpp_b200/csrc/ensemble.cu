@@ -9,11 +9,13 @@
 // from an atomic work counter (longest-processing-time order), so the 680x spread in per-system
 // work (N = 3 .. 2048) balances across the persistent grid.  A system's bodies are staged once per
 // step in shared memory as FP32 coordinates relative to the system's mean position, with G m and
-// the radius; each thread owns bodies i = t, t + T, ... and sums its forces two j-bodies per
-// packed FP32x2 instruction, folding every 64 j-bodies into FP64.  Alongside the force it keeps the
-// smallest separation to any other body (integer min on the ALU pipe); a body closer to another
-// than its radius plus the system's largest radius flags the system, and only flagged systems run
-// the exact FP64 merge scan.
+// the radius; the rows are spread over the CTA in passes of IB rows per thread (IB = 1, 2 or 4),
+// and each thread sums its rows' forces two j-bodies per packed FP32x2 instruction, folding every
+// 64 j-bodies into FP64.  Alongside the force it keeps the smallest separation to any other body (a
+// 3-input float minimum; the one fold holding the row's own body excludes the self pair by its bit
+// pattern); a body closer to another than its radius plus the system's largest radius, plus a
+// bound on the FP32 staging error, flags the system, and only flagged systems run the exact FP64
+// merge scan.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,7 +33,7 @@ struct gtd_ensemble {
     double G = 6.6743e-11, dt = 1.0;
     int merge = 1;
     int threads = 256;   // CTA size (autotuned)
-    int ib = 1;          // bodies per thread in the force loop (autotuned; 2 needs threads <= 256)
+    int ib = 1;          // bodies per thread in the force loop (autotuned; 2 and 4 need threads <= 256)
     int blocks_per_sm = 0;
     int64_t n_sys = 0, n_bodies = 0;
     int max_n = 0;
@@ -108,17 +110,36 @@ __device__ __forceinline__ bool ens_overlaps(const double4 &a, double ra, const 
     return d < __dadd_rn(ra, rb);
 }
 
-// The check_overlap scan (merges, restart from index 0 after each) over one system, by one CTA.
-__device__ int ens_merge_scan(int n, double4 *pos, double4 *vel, double4 *acc, double *rad, double *rest,
-                              int32_t *ids, int *sh) {
+// Removes row i of a system of num rows (the vector erase of the reference's scan): rows i+1 .. num-1
+// move down by one, in passes of T rows.
+__device__ __noinline__ void ens_erase_row(int i, int num, double4 *pos, double4 *vel, double4 *acc, double *rad, double *rest,
+                              int32_t *ids) {
+    const int t = threadIdx.x, T = blockDim.x;
+    for (int base = i; base < num - 1; base += T) {
+        const int k = base + t;
+        const bool act = k < num - 1;
+        double4 p, v, a;
+        double r = 0, e = 0;
+        int32_t id = 0;
+        if (act) { p = pos[k + 1]; v = vel[k + 1]; a = acc[k + 1]; r = rad[k + 1]; e = rest[k + 1]; id = ids[k + 1]; }
+        __syncthreads();
+        if (act) { pos[k] = p; vel[k] = v; acc[k] = a; rad[k] = r; rest[k] = e; ids[k] = id; }
+        __syncthreads();
+    }
+}
+
+// The check_overlap scan (merges, restart from index 0 after each) over one system, by one CTA,
+// from scan state (n rows, at row o0, restarted0: the last step merged into o0).
+__device__ __noinline__ int ens_merge_scan(int n, int o0, bool restarted0, double4 *pos, double4 *vel, double4 *acc, double *rad,
+                              double *rest, int32_t *ids, int *sh) {
     // sh[0] = best, sh[1] = num, sh[2] = o
     const int t = threadIdx.x, T = blockDim.x;
     if (t == 0) {
         sh[1] = n;
-        sh[2] = 0;
+        sh[2] = o0;
     }
     __syncthreads();
-    bool restarted = false;
+    bool restarted = restarted0;
     while (true) {
         const int num = sh[1], o = sh[2];
         if (o >= num) break;
@@ -144,17 +165,7 @@ __device__ int ens_merge_scan(int n, double4 *pos, double4 *vel, double4 *acc, d
             pos[o] = p; vel[o] = v; acc[o] = a; rad[o] = r; rest[o] = e;
         }
         __syncthreads();
-        for (int base = i; base < num - 1; base += T) {
-            const int k = base + t;
-            const bool act = k < num - 1;
-            double4 p, v, a;
-            double r = 0, e = 0;
-            int32_t id = 0;
-            if (act) { p = pos[k + 1]; v = vel[k + 1]; a = acc[k + 1]; r = rad[k + 1]; e = rest[k + 1]; id = ids[k + 1]; }
-            __syncthreads();
-            if (act) { pos[k] = p; vel[k] = v; acc[k] = a; rad[k] = r; rest[k] = e; ids[k] = id; }
-            __syncthreads();
-        }
+        ens_erase_row(i, num, pos, vel, acc, rad, rest, ids);
         if (t == 0) {
             sh[1] = num - 1;
             sh[2] = i < o ? o - 1 : o;
@@ -167,60 +178,222 @@ __device__ int ens_merge_scan(int n, double4 *pos, double4 *vel, double4 *acc, d
     return out;
 }
 
-// Forces on the IB bodies i0, i0 + T, ... (those below nc) of a staged system: each staged j pair is
-// read from shared memory once for all IB bodies.  Returns whether any of them may overlap another.
-// floor2 is added to every r2 inside its first FMA (no extra instruction): the self pair gets
-// r2 = floor2 exactly, a finite 1/r and a zero term (dx = 0), and the overlap minimum skips it by
-// its bit pattern.  floor2 is far below the staged coordinates' resolution (ens_r2_floor).
+constexpr int kEnsCand = 256;  // candidate rows a system's scan tracks before it falls back to the full scan
+
+struct EnsCand {
+    int n;                 // candidates listed (may exceed kEnsCand: then the list is incomplete)
+    int o, num, next;      // scan state: current row, rows, the partner found (-1: none, -2: done)
+    int restarted;
+    int row[kEnsCand];
+};
+
+// One step of the candidate scan, by one thread: sorts and de-duplicates the list, finds the next
+// (row, partner) pair in scan order from the state in c and merges the partner into the row
+// (c.next = the partner), or ends the scan (c.next = -2).
+__device__ __noinline__ void ens_cand_next(double4 *pos, double4 *vel, double4 *acc, double *rad, double *rest,
+                                           EnsCand &c) {
+    // sort the list (few entries; insertion sort) and drop duplicates
+    int k = 0;
+    for (int a = 0; a < c.n; ++a) {
+        const int v = c.row[a];
+        int b = k;
+        while (b > 0 && c.row[b - 1] > v) { c.row[b] = c.row[b - 1]; --b; }
+        c.row[b] = v;
+        ++k;
+    }
+    int u = 0;
+    for (int a = 0; a < k; ++a)
+        if (u == 0 || c.row[u - 1] != c.row[a]) c.row[u++] = c.row[a];
+    c.n = u;
+    int o = c.o;
+    bool restarted = c.restarted != 0;
+    int found = -2;
+    while (true) {
+        if (!restarted) {  // jump to the first candidate at or after o
+            int a = 0;
+            while (a < c.n && c.row[a] < o) ++a;
+            if (a == c.n) break;
+            o = c.row[a];
+        }
+        const int lo = restarted ? 0 : o + 1;
+        const double4 po = pos[o];
+        const double ro = rad[o];
+        int best = -1;
+        for (int a = 0; a < c.n; ++a) {
+            const int i = c.row[a];
+            if (i >= lo && i != o && ens_overlaps(po, ro, pos[i], rad[i])) {
+                best = i;  // the list is sorted: the first partner is the smallest
+                break;
+            }
+        }
+        if (best >= 0) {
+            found = best;
+            break;
+        }
+        ++o;
+        restarted = false;
+    }
+    c.o = o;
+    c.next = found;
+    if (found >= 0) {
+        double4 p = pos[o], v = vel[o], a = acc[o];
+        double r = rad[o], e = rest[o];
+        ens_merge_into(p, v, a, r, e, pos[found], vel[found], acc[found], rad[found], rest[found]);
+        pos[o] = p; vel[o] = v; acc[o] = a; rad[o] = r; rest[o] = e;
+    }
+}
+
+// The same scan restricted to candidate rows.  Every row with an FP64 overlap partner was flagged
+// by the force loop's FP32 separation test (a bound that covers the staging error), and overlap is
+// symmetric, so a row outside the list overlaps nothing and its partners are all listed: the scan
+// can jump from candidate to candidate and search the list alone, taking the same merges in the same
+// order as the full scan.  After a merge only the merged row has moved; it is tested against every
+// row and its new partners join the list.  Returns the rows left; if the list overflows, the full
+// scan continues from the state reached.
+__device__ __noinline__ int ens_merge_scan_cand(int n, double4 *pos, double4 *vel, double4 *acc, double *rad, double *rest,
+                                   int32_t *ids, EnsCand &c, int *sh) {
+    const int t = threadIdx.x;
+    if (t == 0) {
+        c.o = 0;
+        c.num = n;
+        c.restarted = 0;
+    }
+    while (true) {
+        if (t == 0) ens_cand_next(pos, vel, acc, rad, rest, c);
+        __syncthreads();
+        const int i = c.next, num = c.num;
+        __syncthreads();  // every thread has read the state before thread 0 changes it
+        if (i < 0) break;
+        ens_erase_row(i, num, pos, vel, acc, rad, rest, ids);
+        if (t == 0) {
+            // the list after the erase: i leaves, later rows move down by one
+            int u = 0;
+            for (int a = 0; a < c.n; ++a) {
+                const int r = c.row[a];
+                if (r != i) c.row[u++] = r > i ? r - 1 : r;
+            }
+            c.n = u;
+            c.o = i < c.o ? c.o - 1 : c.o;
+            c.num = num - 1;
+            c.restarted = 1;
+        }
+        __syncthreads();
+        // the merged row's partners join the list (with the merged row itself)
+        const int o = c.o, nm = c.num;
+        const double4 po = pos[o];
+        const double ro = rad[o];
+        bool any = false;
+        for (int k = t; k < nm; k += blockDim.x)
+            if (k != o && ens_overlaps(po, ro, pos[k], rad[k])) {
+                const int s = atomicAdd(&c.n, 1);
+                if (s < kEnsCand) c.row[s] = k;
+                any = true;
+            }
+        if (__syncthreads_or(any) && t == 0) {
+            const int s = atomicAdd(&c.n, 1);
+            if (s < kEnsCand) c.row[s] = o;
+        }
+        __syncthreads();
+        const bool overflow = c.n > kEnsCand;
+        const int o1 = c.o, n1 = c.num;
+        __syncthreads();
+        if (overflow)  // too many to track: the full scan from here
+            return ens_merge_scan(n1, o1, true, pos, vel, acc, rad, rest, ids, sh);
+    }
+    const int out = c.num;
+    __syncthreads();
+    return out;
+}
+
+__device__ __forceinline__ float ens_min3(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// One fold (j pairs q0 .. q1-1) of the force loop for IB rows.  kOwn: the fold holds one of the
+// rows' own bodies, whose self pair (r2 = floor2 exactly) must stay out of the minimum: the
+// separation minimum is then taken on the integer bits offset past floor2 (2 ALU operations per
+// value); every other fold takes a plain 3-input float minimum (1 operation per two values).
+template <int IB, bool kOwn>
+__device__ __forceinline__ void ens_fold(int q0, int q1, const float2 *X2, const float2 *Y2, const float2 *Z2,
+                                         const float2 *M2, const float2 (&nx)[IB], const float2 (&ny)[IB],
+                                         const float2 (&nz)[IB], float2 fl2, unsigned fbits, float2 (&fx)[IB],
+                                         float2 (&fy)[IB], float2 (&fz)[IB], float (&mnf)[IB], unsigned (&mnr)[IB]) {
+#pragma unroll 4
+    for (int q = q0; q < q1; ++q) {
+        const float2 X = X2[q], Y = Y2[q], Z = Z2[q], M = M2[q];
+#pragma unroll
+        for (int b = 0; b < IB; ++b) {
+            const float2 dx = __fadd2_rn(X, nx[b]), dy = __fadd2_rn(Y, ny[b]), dz = __fadd2_rn(Z, nz[b]);
+            float2 r2 = __ffma2_rn(dx, dx, fl2);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dz, dz, r2);
+            if constexpr (kOwn) {
+                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.x) - fbits);
+                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.y) - fbits);
+            } else {
+                mnf[b] = ens_min3(mnf[b], r2.x, r2.y);
+            }
+            const float2 inv = make_float2(ens_rsqrt(r2.x), ens_rsqrt(r2.y));
+            const float2 inv2 = __fmul2_rn(inv, inv);
+            float2 sc = __fmul2_rn(M, inv);
+            sc = __fmul2_rn(sc, inv2);
+            fx[b] = __ffma2_rn(dx, sc, fx[b]);
+            fy[b] = __ffma2_rn(dy, sc, fy[b]);
+            fz[b] = __ffma2_rn(dz, sc, fz[b]);
+        }
+    }
+}
+
+// Forces on the IB rows r0, r0 + s, ..., r0 + (IB-1) s (those below nc) of a staged system: each
+// staged j pair is read from shared memory once for all IB rows.  Returns whether any of them may
+// overlap another body.  floor2 is added to every r2 inside its first FMA (no extra instruction):
+// the self pair gets r2 = floor2 exactly, a finite 1/r and a zero term (dx = 0).  floor2 is far
+// below the staged coordinates' resolution (ens_r2_floor).  r0 - t and s are multiples of 32, so
+// the 32 rows of a warp share one fold of kEnsFold j-bodies for each b, and the choice of fold form
+// (ens_fold's kOwn) is uniform across the warp.
 template <int IB>
-__device__ __forceinline__ int ens_force_rows(int i0, int T, int nc, int npad, const float *sx, const float *sy,
+__device__ __forceinline__ int ens_force_rows(int r0, int s, int nc, int npad, const float *sx, const float *sy,
                                               const float *sz, const float *sm, double4 *pos, double4 *vel,
-                                              double4 *acc, const double *rad, float rmx, bool kick, double h2,
-                                              float floor2) {
+                                              double4 *acc, const double *rad, float rmx, float slack, bool kick,
+                                              double h2, float floor2, EnsCand &cand) {
     const float2 *X2 = reinterpret_cast<const float2 *>(sx);
     const float2 *Y2 = reinterpret_cast<const float2 *>(sy);
     const float2 *Z2 = reinterpret_cast<const float2 *>(sz);
     const float2 *M2 = reinterpret_cast<const float2 *>(sm);
     float2 nx[IB], ny[IB], nz[IB];
     double ax[IB], ay[IB], az[IB];
-    unsigned mnr[IB];
+    float mnf[IB];      // min r2 over the folds without the row's own body
+    unsigned mnr[IB];   // min over the own fold's j != i of r2 bits, offset past floor2
+    int own[IB];        // fold of the row's own body
 #pragma unroll
     for (int b = 0; b < IB; ++b) {
-        const int i = i0 + b * T;
-        const int ic = i < nc ? i : i0;  // a missing second body repeats the first; its result is dropped
+        const int i = r0 + b * s;
+        const int ic = i < nc ? i : r0;  // a missing row repeats the first; its result is dropped
         nx[b] = make_float2(-sx[ic], -sx[ic]);
         ny[b] = make_float2(-sy[ic], -sy[ic]);
         nz[b] = make_float2(-sz[ic], -sz[ic]);
         ax[b] = ay[b] = az[b] = 0.0;
-        mnr[b] = 0xffffffffu;  // min over j != i of r2 bits, the self pair (r2 = floor2) excluded
+        mnf[b] = INFINITY;
+        mnr[b] = 0xffffffffu;
+        own[b] = ic / kEnsFold;
     }
     const float2 fl2 = make_float2(floor2, floor2);
     const unsigned fbits = (unsigned)__float_as_int(floor2) + 1u;
     for (int q0 = 0; q0 < npad / 2; q0 += kEnsFold / 2) {
         const int q1 = min(q0 + kEnsFold / 2, npad / 2);
+        const int fold = q0 / (kEnsFold / 2);
         float2 fx[IB], fy[IB], fz[IB];
 #pragma unroll
         for (int b = 0; b < IB; ++b) fx[b] = fy[b] = fz[b] = make_float2(0.f, 0.f);
-#pragma unroll 4
-        for (int q = q0; q < q1; ++q) {
-            const float2 X = X2[q], Y = Y2[q], Z = Z2[q], M = M2[q];
+        bool mine = false;
 #pragma unroll
-            for (int b = 0; b < IB; ++b) {
-                const float2 dx = __fadd2_rn(X, nx[b]), dy = __fadd2_rn(Y, ny[b]), dz = __fadd2_rn(Z, nz[b]);
-                float2 r2 = __ffma2_rn(dx, dx, fl2);
-                r2 = __ffma2_rn(dy, dy, r2);
-                r2 = __ffma2_rn(dz, dz, r2);
-                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.x) - fbits);
-                mnr[b] = min(mnr[b], (unsigned)__float_as_int(r2.y) - fbits);
-                const float2 inv = make_float2(ens_rsqrt(r2.x), ens_rsqrt(r2.y));
-                const float2 inv2 = __fmul2_rn(inv, inv);
-                float2 sc = __fmul2_rn(M, inv);
-                sc = __fmul2_rn(sc, inv2);
-                fx[b] = __ffma2_rn(dx, sc, fx[b]);
-                fy[b] = __ffma2_rn(dy, sc, fy[b]);
-                fz[b] = __ffma2_rn(dz, sc, fz[b]);
-            }
-        }
+        for (int b = 0; b < IB; ++b) mine |= own[b] == fold;
+        if (__any_sync(0xffffffffu, mine))
+            ens_fold<IB, true>(q0, q1, X2, Y2, Z2, M2, nx, ny, nz, fl2, fbits, fx, fy, fz, mnf, mnr);
+        else
+            ens_fold<IB, false>(q0, q1, X2, Y2, Z2, M2, nx, ny, nz, fl2, fbits, fx, fy, fz, mnf, mnr);
 #pragma unroll
         for (int b = 0; b < IB; ++b) {
             ax[b] += (double)fx[b].x + (double)fx[b].y;
@@ -231,12 +404,17 @@ __device__ __forceinline__ int ens_force_rows(int i0, int T, int nc, int npad, c
     int flagged = 0;
 #pragma unroll
     for (int b = 0; b < IB; ++b) {
-        const int i = i0 + b * T;
+        const int i = r0 + b * s;
         if (i >= nc) continue;
-        if (mnr[b] != 0xffffffffu) {  // some other body exists
-            const float mind2 = __int_as_float((int)(mnr[b] + fbits));
-            const float reach = (float)rad[i] + rmx;
-            if (mind2 < reach * reach * 1.0001f) flagged = 1;
+        float mind2 = mnf[b];
+        if (mnr[b] != 0xffffffffu) mind2 = fminf(mind2, __int_as_float((int)(mnr[b] + fbits)));
+        if (mind2 < INFINITY) {  // some other body exists
+            const float reach = ((float)rad[i] + rmx) * 1.00001f + slack;
+            if (mind2 < reach * reach * 1.0001f + floor2) {
+                flagged = 1;
+                const int k = atomicAdd(&cand.n, 1);
+                if (k < kEnsCand) cand.row[k] = i;
+            }
         }
         if (kick) {
             double4 v = vel[i];
@@ -248,8 +426,8 @@ __device__ __forceinline__ int ens_force_rows(int i0, int T, int nc, int npad, c
     return flagged;
 }
 
-// One launch = one KDK step (or the initial force) for every system.  IB bodies per thread (1 or 2;
-// with 2 each staged j pair feeds two bodies, halving the shared-memory reads per interaction).
+// One launch = one KDK step (or the initial force) for every system.  IB bodies per thread (1, 2 or 4;
+// each staged j pair feeds IB bodies, dividing the shared-memory reads per interaction by IB).
 template <int IB>
 __global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -262,6 +440,8 @@ __global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsA
     __shared__ float redr[32], redg[32];
     __shared__ int sh[8];
     __shared__ float rmax_s, floor_s;
+    __shared__ int xmax_bits;  // largest staged |coordinate| (non-negative float bits)
+    __shared__ EnsCand cand;   // rows the separation test flagged
     const int t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5, nw = (T + 31) >> 5;
     const double h = a.h, h2 = 0.5 * a.h;
     while (true) {
@@ -321,29 +501,51 @@ __global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsA
                 cen[0] = X / nc; cen[1] = Y / nc; cen[2] = Z / nc;
                 rmax_s = R;
                 floor_s = ens_r2_floor(Gm);
+                xmax_bits = 0;
+                cand.n = 0;
             }
             __syncthreads();
             const double mx = cen[0], my = cen[1], mz = cen[2];
             const float rmx = rmax_s, floor2 = floor_s;
             // stage the system: FP32 relative positions and G m (pad to an even count, far and massless)
             const int npad = (nc + 1) & ~1;
+            float xm = 0.f;
             for (int i = t; i < npad; i += T) {
                 if (i < nc) {
                     const double4 p = pos[i];
-                    sx[i] = (float)(p.x - mx); sy[i] = (float)(p.y - my); sz[i] = (float)(p.z - mz);
+                    const float X = (float)(p.x - mx), Y = (float)(p.y - my), Z = (float)(p.z - mz);
+                    sx[i] = X; sy[i] = Y; sz[i] = Z;
                     sm[i] = (float)(a.G * p.w);
+                    xm = fmaxf(xm, fmaxf(fabsf(X), fmaxf(fabsf(Y), fabsf(Z))));
                 } else {
                     sx[i] = 1e30f; sy[i] = 1e30f; sz[i] = 1e30f; sm[i] = 0.f;
                 }
             }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) xm = fmaxf(xm, __shfl_xor_sync(0xffffffffu, xm, o));
+            if (lane == 0) atomicMax(&xmax_bits, __float_as_int(xm));
             __syncthreads();
+            // Bound on the FP32 error of a staged separation: each staged coordinate is within
+            // 2^-24 |X| of its FP64 value, so a separation is off by at most sqrt(3) 2^-23 xmax
+            // (plus its own relative rounding, covered by the factor on the reach); 2^-21 xmax
+            // keeps a factor 2 of room.  Every pair the FP64 overlap test would merge is flagged.
+            const float slack = __int_as_float(xmax_bits) * 0x1p-21f;
+            // rows in passes of up to IB*T; a pass of c rows gives each of its first s threads (s the
+            // smallest multiple of 32 with IB*s >= c) the rows t, t + s, ...: threads hold IB valid
+            // rows except in the last warp, and whole warps past s sit the pass out
             int flagged = 0;
-            for (int i0 = t; i0 < nc; i0 += IB * T)
-                flagged |= ens_force_rows<IB>(i0, T, nc, npad, sx, sy, sz, sm, pos, vel, acc, rad, rmx, a.kdk && first,
-                                              h2, floor2);
+            for (int base = 0; base < nc; base += IB * T) {
+                const int c = min(IB * T, nc - base);
+                const int sw = ((c + IB - 1) / IB + 31) & ~31;
+                if (t < sw)
+                    flagged |= ens_force_rows<IB>(base + t, sw, nc, npad, sx, sy, sz, sm, pos, vel, acc, rad, rmx,
+                                                  slack, a.kdk && first, h2, floor2, cand);
+            }
             flagged = __syncthreads_or(flagged);
             if (!first || !flagged || !a.merge) break;
-            const int nn = ens_merge_scan(nc, pos, vel, acc, rad, a.rest + b0, a.ids + b0, sh);
+            const int nn = cand.n <= kEnsCand
+                               ? ens_merge_scan_cand(nc, pos, vel, acc, rad, a.rest + b0, a.ids + b0, cand, sh)
+                               : ens_merge_scan(nc, 0, false, pos, vel, acc, rad, a.rest + b0, a.ids + b0, sh);
             if (nn == nc) break;
             if (t == 0) {
                 a.cnt[s] = nn;
@@ -354,6 +556,14 @@ __global__ void __launch_bounds__(IB == 1 ? 512 : 256) ensemble_step_kernel(EnsA
         }
         __syncthreads();
     }
+}
+
+// The kernel for ib bodies per thread (1, 2 or 4).
+template <typename F>
+void with_ens_kernel(int ib, F &&f) {
+    if (ib == 4) f(ensemble_step_kernel<4>);
+    else if (ib == 2) f(ensemble_step_kernel<2>);
+    else f(ensemble_step_kernel<1>);
 }
 
 int ens_stride(int max_n) { return std::max(2, (max_n + 1) & ~1); }
@@ -379,17 +589,11 @@ static int ens_launch(gtd_ensemble *e, int kdk) {
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e->device);
     int per_sm = 1;
-    if (e->ib == 2)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_step_kernel<2>, e->threads, smem);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_step_kernel<1>, e->threads, smem);
+    with_ens_kernel(e->ib, [&](auto k) { cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, e->threads, smem); });
     if (per_sm < 1) per_sm = 1;
     const int grid = (int)std::min<int64_t>((int64_t)dev_sms * per_sm, std::max<int64_t>(e->n_sys, 1));
     GTD_CUDA(cudaMemsetAsync(e->work, 0, sizeof(unsigned), e->stream));
-    if (e->ib == 2)
-        ensemble_step_kernel<2><<<grid, e->threads, smem, e->stream>>>(a);
-    else
-        ensemble_step_kernel<1><<<grid, e->threads, smem, e->stream>>>(a);
+    with_ens_kernel(e->ib, [&](auto k) { k<<<grid, e->threads, smem, e->stream>>>(a); });
     GTD_CHECK_LAUNCH();
     e->launches += 1;
     return GTD_OK;
@@ -461,10 +665,13 @@ int gtd_ensemble_create(gtd_ensemble **out, int device) {
     GTD_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     GTD_CUDA(cudaEventCreate(&e->ev0));
     GTD_CUDA(cudaEventCreate(&e->ev1));
-    GTD_CUDA(cudaFuncSetAttribute(ensemble_step_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  ens_smem_bytes(kEnsMaxN)));
-    GTD_CUDA(cudaFuncSetAttribute(ensemble_step_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  ens_smem_bytes(kEnsMaxN)));
+    for (int ib : {1, 2, 4}) {
+        cudaError_t c = cudaSuccess;
+        with_ens_kernel(ib, [&](auto k) {
+            c = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, ens_smem_bytes(kEnsMaxN));
+        });
+        GTD_CUDA(c);
+    }
     *out = e;
     return GTD_OK;
 }
@@ -623,16 +830,17 @@ int gtd_ensemble_set_threads(gtd_ensemble *e, int threads) {
     if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
     if (threads != 64 && threads != 128 && threads != 256 && threads != 512)
         return fail(GTD_ERR_INVALID_ARGUMENT, "threads must be 64, 128, 256 or 512");
-    if (e->ib == 2 && threads > 256) e->ib = 1;
+    if (e->ib > 1 && threads > 256) e->ib = 1;
     e->threads = threads;
     return GTD_OK;
 }
 
 int gtd_ensemble_set_bodies_per_thread(gtd_ensemble *e, int bodies) {
     if (!e) return fail(GTD_ERR_INVALID_ARGUMENT, "ensemble is NULL");
-    if (bodies != 1 && bodies != 2) return fail(GTD_ERR_INVALID_ARGUMENT, "bodies per thread must be 1 or 2");
-    if (bodies == 2 && e->threads > 256)
-        return fail(GTD_ERR_INVALID_ARGUMENT, "2 bodies per thread need a CTA of at most 256 threads");
+    if (bodies != 1 && bodies != 2 && bodies != 4)
+        return fail(GTD_ERR_INVALID_ARGUMENT, "bodies per thread must be 1, 2 or 4");
+    if (bodies > 1 && e->threads > 256)
+        return fail(GTD_ERR_INVALID_ARGUMENT, "%d bodies per thread need a CTA of at most 256 threads", bodies);
     e->ib = bodies;
     return GTD_OK;
 }
@@ -684,7 +892,7 @@ int gtd_ensemble_autotune(gtd_ensemble *e, int *best_threads, double *best_ms) {
     int rc = save(false);
     const bool was_begun = e->begun;
     const int orig_threads = e->threads, orig_ib = e->ib;
-    const int cands[][2] = {{128, 1}, {256, 1}, {512, 1}, {128, 2}, {256, 2}};
+    const int cands[][2] = {{128, 1}, {256, 1}, {512, 1}, {128, 2}, {256, 2}, {128, 4}, {256, 4}};
     constexpr int kCands = sizeof(cands) / sizeof(cands[0]);
     // Each timing runs kTuneSteps consecutive steps from the saved state, so a candidate is judged on
     // steady stepping rather than on one launch.  The candidates take turns (round robin) so that a

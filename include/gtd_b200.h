@@ -113,8 +113,10 @@ GTD_API int gtd_system_survivors(gtd_system *sys, int64_t *upload_index);
 /* ---- trajectory frames (memFreq) -------------------------------------------------------------
  * Replaces the recording of gtd::system<..., memFreq, ...> (body trajectories gregbod.hpp:304-320,
  * per-body and total energies gregsys.hpp:219-227, 343-363, 439-476, 608-630).  With every != 0,
- * each direct-summation evolve records a frame at its start and after every every-th step (after
- * that step's collision pass); a frame holds, per body in download order, x, y, z, vx, vy, vz,
+ * each direct-summation evolve (gtd_system_evolve, gtd_system_evolve_begin/_steps with host
+ * callbacks, gtd_system_evolve_callbacks with device callbacks) records a frame at its start and
+ * after every every-th step (after that step's for_all_bods and collision pass, before
+ * for_each_bod: FUNC_TEMPL_SELECT, gregsys.hpp:16-106); a frame holds, per body in download order, x, y, z, vx, vy, vz,
  * ke = 0.5 m |v| |v| and pe = 0.5 sum_{j != i} -G m_i m_j / r_ij, computed on the device in FP64.
  * Each evolve starts a new recording; Barnes-Hut evolves record nothing (as the reference).  Which
  * of these values the reference keeps depends on the method and collision mode; the C++ and Python
@@ -354,8 +356,9 @@ GTD_API int gtd_ensemble_counts(gtd_ensemble *ens, int64_t *counts, uint64_t *me
 GTD_API int gtd_ensemble_download(gtd_ensemble *ens, double *m, double *r, double *rest, double *x3, double *v3,
                                   double *a3);
 /* CTA size of the step kernel (64, 128, 256 or 512) and bodies per thread in its force loop (1, or
- * 2 with at most 256 threads), or let the autotuner time (128|256|512, 1) and (128|256, 2) on the
- * current state (restored afterwards) and keep the fastest; gtd_ensemble_config reads the choice. */
+ * 2 or 4 with at most 256 threads), or let the autotuner time (128|256|512, 1), (128|256, 2) and
+ * (128|256, 4) on the current state (restored afterwards) and keep the fastest; gtd_ensemble_config
+ * reads the choice. */
 GTD_API int gtd_ensemble_set_threads(gtd_ensemble *ens, int threads);
 GTD_API int gtd_ensemble_set_bodies_per_thread(gtd_ensemble *ens, int bodies);
 GTD_API int gtd_ensemble_config(const gtd_ensemble *ens, int *threads, int *bodies_per_thread);

@@ -62,6 +62,30 @@ def test_merges_vs_oracle(gpu, oracle):
         assert np.abs(p_gpu - p_orc).max() <= 1e-6 * (mo[:, None] * np.abs(vo)).sum()
 
 
+@pytest.mark.parametrize("n,r_ball,fac", [(1500, 3.0, 30.0), (400, 1.0, 20.0), (600, 0.5, 30.0), (300, 0.2, 10.0)])
+def test_dense_merges_vs_oracle(gpu, oracle, n, r_ball, fac):
+    """Systems with many overlaps at upload and after each step.  The first two flag fewer than 256
+    rows (203 and 101 at upload), so the scan runs on the candidate list, with merged bodies
+    meeting new partners; the last two flag more (597, 267) and take the full scan.  Either way
+    the merges are the reference's: the same survivors and masses, positions within 1e-10."""
+    off, m, r, x, v = ensemble(1, 5, n_min=n, n_max=n, r_ball=r_ball * AU)
+    r = r * fac
+    rest = np.random.default_rng(4).uniform(0, 1, n)
+    e = Ensemble(off, m, x, v, r, rest, merge=True, dt=DT)
+    e.evolve(3)
+    st = e.state()
+    counts, merges, _ = e.counts()
+    rows = np.concatenate([m[:, None], r[:, None], rest[:, None], x, v, np.zeros((n, 3))], 1)
+    rows = oracle.merge_overlapping(rows)
+    mo, ro, xo, vo = oracle_run(oracle, rows[:, 0].copy(), rows[:, 1].copy(), rows[:, 2].copy(), rows[:, 3:6].copy(),
+                                rows[:, 6:9].copy(), 3, True)
+    assert merges == n - len(mo) and merges > 0
+    assert counts[0] == len(mo)
+    np.testing.assert_allclose(st[0]["m"], mo, rtol=1e-15)
+    np.testing.assert_allclose(st[0]["r"], ro, rtol=1e-15)  # cbrt: the device's and the host's may differ by an ulp
+    assert np.abs(st[0]["x"] - xo).max() / np.abs(xo).max() < 1e-10
+
+
 def test_graph_replay_equals_single_launches(gpu):
     off, m, r, x, v = ensemble(40, 73, n_min=3, n_max=400)
     a = Ensemble(off, m, x, v, r, merge=True, dt=DT)
@@ -92,12 +116,14 @@ def test_autotune_restores_state(gpu):
     assert all(np.array_equal(sa[s]["x"], sb[s]["x"]) for s in range(64))
 
 
-def test_two_bodies_per_thread_is_bit_identical(gpu):
-    """The force loop with 2 bodies per thread performs, per body, the same operations in the same
-    order as with 1: the trajectories (merges included) are bit-identical."""
+def test_bodies_per_thread_is_bit_identical(gpu):
+    """The force loop with 2 or 4 bodies per thread performs, per body, the same operations in the
+    same order as with 1 (the rows of a pass are spread over the threads differently, and the
+    separation minimum is exact in every form): the trajectories (merges included) are
+    bit-identical."""
     off, m, r, x, v = ensemble(48, 75, n_min=3, n_max=1500)
     runs = []
-    for threads, ib in ((256, 1), (256, 2), (128, 2)):
+    for threads, ib in ((256, 1), (64, 1), (256, 2), (128, 2), (128, 4), (256, 4)):
         e = Ensemble(off, m, x, v, r, merge=True, dt=DT)
         e.set_threads(threads)
         e.set_bodies_per_thread(ib)
@@ -110,8 +136,11 @@ def test_two_bodies_per_thread_is_bit_identical(gpu):
             assert np.array_equal(st[s]["x"], runs[0][0][s]["x"]) and np.array_equal(st[s]["v"], runs[0][0][s]["v"])
     e = Ensemble(off, m, x, v, r, merge=True, dt=DT)
     e.set_threads(512)
+    for ib in (2, 4):
+        with pytest.raises(ValueError):
+            e.set_bodies_per_thread(ib)
     with pytest.raises(ValueError):
-        e.set_bodies_per_thread(2)
+        e.set_bodies_per_thread(3)
 
 
 def test_capacity_limit(gpu):
