@@ -521,9 +521,10 @@ class System:
         return a, cnt
 
     def set_bh_walk_variant(self, variant: int) -> None:
-        """Node-record layout of the float-tree walk (-1 default, 0 separate arrays, 1 interleaved
-        32-byte records); both take the same interactions in the same order."""
-        if variant < -1 or variant > 1:
+        """Float-tree walk (-1 default = 2, 0 per-lane walk with separate node arrays, 1 per-lane
+        walk with interleaved 32-byte records, 2 list walk); all take the same interactions per
+        body, 0 and 1 in the same order, 2 summed in another order."""
+        if variant < -1 or variant > 2:
             raise ValueError(f"walk variant {variant} out of range")
         self._walk_variant = int(variant)
 

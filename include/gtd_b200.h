@@ -293,10 +293,11 @@ GTD_API int gtd_measure_fma_peak(int device, int precision, double *flops_per_s)
 GTD_API int gtd_bh_build(gtd_system *sys, int tree_float);
 /* Tree geometry for evolve(leapfrog_kdk | barnes_hut): 1 = T=float (the default), 0 = T=double. */
 GTD_API int gtd_bh_set_tree_float(gtd_system *sys, int tree_float);
-/* Node-record layout of the float-tree walk that replaces the cell_iterator loop
- * (greg8tree.hpp:702-833): -1 = default (1), 0 = position/mass and links in separate arrays, 1 =
- * both halves of a node in one 32-byte sector.  Both give the same interaction lists and bits; the
- * next gtd_bh_build applies it. */
+/* Float-tree walk that replaces the cell_iterator loop (greg8tree.hpp:702-833): -1 = default (2),
+ * 0 = per-lane walk with position/mass and links in separate arrays, 1 = per-lane walk with both
+ * halves of a node in one 32-byte sector (0 and 1 give the same interaction lists and bits), 2 =
+ * list walk: the same interaction list per body, classified for a warp's 32 bodies at once and
+ * summed in another order.  The next gtd_bh_build applies it. */
 GTD_API int gtd_bh_set_walk_variant(gtd_system *sys, int variant);
 GTD_API int gtd_bh_tree_size(gtd_system *sys, int64_t *n_nodes, int64_t *n_leaves, double *box6);
 /* Copies the tree out (any pointer may be NULL): sorted codes and slot->body permutation [n],

@@ -83,7 +83,7 @@ def test_fp64_walk_vs_reference_golden(gpu, golden, oracle):
     assert np.array_equal(cnt, ocnt)
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 @pytest.mark.parametrize("n,theta", [(5000, 0.5), (30000, 0.5), (30000, 1.0), (3000, 0.0)])
 def test_fp32_walk_vs_host_rebuild(gpu, oracle, n, theta, variant):
     m, x, _ = plummer(n, 30 + n)
@@ -114,7 +114,47 @@ def test_walk_record_layouts_bit_identical(gpu):
         assert np.array_equal(out[0][1], o[1])
         assert np.array_equal(out[0][0], o[0])
     with pytest.raises(ValueError):
-        System(m, x, np.zeros_like(x), units_format=UNITS_G6674).set_bh_walk_variant(2)
+        System(m, x, np.zeros_like(x), units_format=UNITS_G6674).set_bh_walk_variant(3)
+
+
+@pytest.mark.parametrize("n,theta,eps", [(1, 0.5, 0.0), (2, 0.5, 0.0), (33, 0.5, 0.0), (20001, 0.5, 0.0),
+                                         (20001, 0.7, 1e9), (4099, 1.5, 0.0), (4099, 0.2, 0.0)])
+def test_list_walk_same_interactions(gpu, oracle, n, theta, eps):
+    """The list walk (variant 2) against the per-lane walk (variant 1) and the oracle: every
+    body's interaction count equal, accelerations equal up to the order of the FP32 sum.  Odd
+    sizes leave a partial last warp; softening changes only the terms; bodies 7 and 8 share a
+    depth-21 cell (a bucket leaf of two bodies, 1e5 m apart at 1 AU scale)."""
+    if n == 1:
+        m, x = np.array([1e30]), np.zeros((1, 3))
+    else:
+        m, x, _ = plummer(n, 90 + n)
+    if n > 8:
+        x[8] = x[7] + np.array([1e5, 0.0, 0.0])
+    out = []
+    for variant in (1, 2):
+        s = System(m, x, np.zeros_like(x), units_format=UNITS_G6674)
+        s.set_bh_opening_angle(theta)
+        if eps:
+            s.set_softening(eps)
+        s.set_bh_walk_variant(variant)
+        if n == 1:
+            with pytest.raises(InvalidBodyPlacement):
+                s.bh_accelerations(tree_float=True)
+            return
+        out.append(s.bh_accelerations(tree_float=True))
+    (a1, c1), (a2, c2) = out
+    assert np.array_equal(c1, c2)
+    if n > 8:
+        t = s.bh_tree()
+        assert (t["count"][t["is_leaf"] == 1] > 1).any()  # the bucket leaf is there
+    rel = np.linalg.norm(a2 - a1, axis=1) / np.linalg.norm(a1, axis=1)
+    assert np.sqrt((rel ** 2).mean()) < 1e-5 and rel.max() < 1e-3  # the FP32 bar of the walk vs the oracle
+    t = oracle.bh_tree(x, m, 1)
+    try:
+        ao, ocnt = oracle.bh_acc(t, x, m, 1, theta, eps, G)
+    finally:
+        oracle.bh_free(t)
+    assert np.array_equal(c2, ocnt)
 
 
 def test_theta_zero_is_direct_sum(gpu, oracle):
