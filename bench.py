@@ -41,7 +41,7 @@ FLOPS_PER_INTERACTION = 20
 # (--metrics dram__bytes_read.sum,dram__bytes_write.sum, one launch at N = 262144): (N, variant) ->
 # (read, write).  The positions (N x 32 B = 8.39 MB) are read about once; the writes are the work
 # units' FP64 partial sums (units x 3 x 8 B per i-body), of which part stays in L2.
-NCU_FORCE_TRAFFIC = {(262144, 2): (12063744, 179496448), (262144, 8): (11524096, 177701888)}
+NCU_FORCE_TRAFFIC = {(262144, 2): (12255232, 178242304), (262144, 8): (9481216, 176747264)}
 
 
 def parse_args():
