@@ -889,7 +889,11 @@ int launch_integrate(const ForcePlan &p, const double *partials, int epi, const 
     if (p.n == 0) return GTD_OK;
     IntArgs a{p.n, p.tiles, p.total, p.grid, p.bi, epi, partials, st, p.segs};
     const int threads = 256;
-    if (p.slots > 4 * p.rows)  // a row's force is spread over more than ~4 slots
+    // A row's force spread over more than ~4 slots, with too few bodies for a thread each to keep
+    // the loads in flight: a warp per body.  From 2^17 bodies the thread-per-body form has the
+    // parallelism, and its loads of 32 neighbouring bodies' slots are coalesced where the warp form
+    // reads one 8-byte value per sector (0.196 ms per step at N = 262144 with 37 slots per row).
+    if (p.slots > 4 * p.rows && p.n < ((int64_t)1 << 17))
         integrate_warp_kernel<<<(unsigned)((p.n * 32 + threads - 1) / threads), threads, 0, s>>>(a);
     else
         integrate_kernel<<<(unsigned)((p.n + threads - 1) / threads), threads, 0, s>>>(a);
