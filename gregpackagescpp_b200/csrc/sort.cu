@@ -109,11 +109,13 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const unsigned
     hist[(size_t)threadIdx.x * blocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Stable scatter.  A block takes its chunk in two halves of kHalf keys.  For each half it counts the
-// digits, ranks every key stably inside its digit (rounds of 256 keys in index order; within a round
-// by lane (match_any) and warp), places the keys digit-sorted in shared memory, and then writes them
-// out in that order: keys of one digit go to consecutive addresses, so the stores fill whole sectors
-// instead of one 8-byte store per key.
+// Stable scatter.  A block takes its chunk in two halves of kHalf keys.  In a half, warp w owns the
+// contiguous keys w*256 .. w*256+255 (eight rounds of 32, in index order) and ranks them stably
+// inside its own digit counters (match_any per round, warp-synchronous: no block barrier); one block
+// scan over the 256 digits then turns the per-warp counts into offsets, the keys are placed
+// digit-sorted in shared memory and written out in that order: keys of one digit go to consecutive
+// addresses, so the stores fill whole sectors instead of one 8-byte store per key.  Seven block
+// barriers per half (the earlier block-wide ranking rounds took 34).
 constexpr int kHalfItems = kSortItems / 2;
 constexpr int kHalf = kSortThreads * kHalfItems;
 
@@ -123,10 +125,11 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsig
                                                                      int32_t *vals_out, int64_t n, int shift,
                                                                      const uint32_t *offsets, int blocks) {
     constexpr int kWarps = kSortThreads / 32;
+    static_assert(kHalf == kWarps * 32 * kHalfItems, "a warp owns kHalfItems rounds of 32 keys");
     __shared__ unsigned long long sk[kHalf];
     __shared__ int32_t sv[kHalf];
-    __shared__ uint32_t wcnt[kWarps][256];
-    __shared__ uint32_t cnt[256], pre[256], run_local[256], run_global[256], wsum[kWarps];
+    __shared__ uint32_t wcnt[kWarps][256];  // per-warp digit counts, then per-warp digit offsets
+    __shared__ uint32_t pre[256], run_global[256], wsum[kWarps];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const unsigned lt = (1u << lane) - 1u;
     run_global[t] = offsets[(size_t)t * blocks + blockIdx.x];
@@ -135,12 +138,12 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsig
         const int64_t hbase = base + (int64_t)h * kHalf;
         unsigned long long key[kHalfItems];
         int32_t val[kHalfItems];
-        uint32_t dig[kHalfItems];
-        cnt[t] = 0;
-        __syncthreads();
+        uint32_t dig[kHalfItems], wr[kHalfItems];
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) wcnt[w][t] = 0;
 #pragma unroll
         for (int k = 0; k < kHalfItems; ++k) {
-            const int64_t i = hbase + (int64_t)k * kSortThreads + t;
+            const int64_t i = hbase + (int64_t)warp * (32 * kHalfItems) + k * 32 + lane;
             key[k] = 0;
             val[k] = 0;
             dig[k] = 256;  // absent keys get a digit no key has
@@ -148,12 +151,26 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsig
                 key[k] = keys_in[i];
                 val[k] = vals_in[i];
                 dig[k] = (uint32_t)((key[k] >> shift) & 0xffu);
-                atomicAdd(&cnt[dig[k]], 1u);
             }
         }
         __syncthreads();
-        // exclusive scan of the half's digit counts, one digit per thread
-        const uint32_t c = cnt[t];
+        // stable rank inside the warp: rounds in index order, lanes in index order within a round
+#pragma unroll
+        for (int k = 0; k < kHalfItems; ++k) {
+            const uint32_t d = dig[k];
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const unsigned rank = __popc(peers & lt);
+            const uint32_t before = d < 256 ? wcnt[warp][d] : 0u;
+            __syncwarp();
+            if (d < 256 && rank == 0) wcnt[warp][d] = before + __popc(peers);
+            __syncwarp();
+            wr[k] = before + rank;
+        }
+        __syncthreads();
+        // digit totals of the half and their exclusive scan, one digit per thread
+        uint32_t c = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) c += wcnt[w][t];
         uint32_t incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -164,34 +181,29 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsig
         __syncthreads();
         uint32_t wofs = 0;
         for (int w = 0; w < warp; ++w) wofs += wsum[w];
-        pre[t] = wofs + incl - c;
-        run_local[t] = wofs + incl - c;
+        const uint32_t start = wofs + incl - c;
+        pre[t] = start;
+        // per-warp offsets of digit t inside the half: warps in order
+        uint32_t run = start;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t cw = wcnt[w][t];
+            wcnt[w][t] = run;
+            run += cw;
+        }
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < kHalfItems; ++k) {
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) wcnt[w][t] = 0;
-            __syncthreads();
             const uint32_t d = dig[k];
-            const unsigned peers = __match_any_sync(0xffffffffu, d);
-            const unsigned rank = __popc(peers & lt);
-            if (d < 256 && rank == 0) wcnt[warp][d] = __popc(peers);
-            __syncthreads();
             if (d < 256) {
-                uint32_t pos = run_local[d] + rank;
-                for (int w = 0; w < warp; ++w) pos += wcnt[w][d];
+                const uint32_t pos = wcnt[warp][d] + wr[k];
                 if (pos < (uint32_t)kHalf) {
                     sk[pos] = key[k];
                     sv[pos] = val[k];
                 }
             }
-            __syncthreads();
-            uint32_t tot = 0;
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) tot += wcnt[w][t];
-            run_local[t] += tot;
-            __syncthreads();
         }
+        __syncthreads();
         const int64_t rem = n - hbase;
         const int hcount = rem <= 0 ? 0 : (rem < kHalf ? (int)rem : kHalf);
 #pragma unroll
