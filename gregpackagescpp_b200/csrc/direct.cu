@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(kThreads) force_f64_kernel(ForceKArgs a) {
 
 // -------------------------------------------------------------------------------------------
 // Mixed precision.  Each j-tile is staged in shared memory as FP32 coordinates relative to the
-// row's centre c (the FP64 mean position of the row's bodies, which the Morton reordering keeps
+// row's centre c (the FP64 mean position of the row's bodies, which the Hilbert reordering keeps
 // compact), with G m_j in FP32.  Pair arithmetic runs two j-bodies per instruction on the packed
 // FP32x2 pipe (add/mul/fma .f32x2) with one MUFU rsqrt per pair; each i keeps FP32 partial sums
 // for FOLD j-bodies, then folds them into FP64 Kahan-compensated accumulators.  Tiles that

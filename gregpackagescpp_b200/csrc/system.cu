@@ -305,7 +305,7 @@ int output_rows(gtd_system *s, std::vector<int64_t> &row) {
     return GTD_OK;
 }
 
-// The mixed kernel centres each row's FP32 frame on the row; Morton-ordered bodies keep rows
+// The mixed kernel centres each row's FP32 frame on the row; Hilbert-ordered bodies keep rows
 // compact, so the mixed path reorders at the start of an evolve and every reorder_interval steps.
 static int maybe_reorder(gtd_system *s, bool force) {
     // collisions scan the bodies in upload order (as the reference scans its vector): no reordering
