@@ -78,3 +78,27 @@ def test_noalloc_rejects_host_memory(gpu):
     rc = L.gtd_direct_accelerations_noalloc(64, host_pm4.ctypes.data, G, _lib.PREC_F64, acc3.data_ptr(), None)
     assert rc == _lib.ERR_INVALID_ARGUMENT
     assert b"device" in L.gtd_last_error()
+
+
+@pytest.mark.parametrize("precision", [_lib.PREC_F64, _lib.PREC_MIXED])
+def test_noalloc_call_is_capturable(gpu, precision):
+    """What the entry point exists for: once a first call has looked up the scratch address, a call
+    allocates nothing and does not synchronise, so it can be captured in a CUDA graph (a cudaMalloc
+    or a synchronisation inside the capture would make it fail).  The replay gives the eager call's
+    result bit for bit."""
+    import torch
+    n = 4000
+    m, x, _ = plummer(n, 94)
+    pm4 = torch.tensor(np.concatenate([x, m[:, None]], 1), dtype=torch.float64, device="cuda:0")
+    eager = torch.empty((n, 3), dtype=torch.float64, device="cuda:0")
+    _lib.check(_noalloc(pm4, eager, precision))
+    torch.cuda.synchronize()
+    out = torch.full((n, 3), float("nan"), dtype=torch.float64, device="cuda:0")
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, capture_error_mode="thread_local"):
+        rc = _noalloc(pm4, out, precision)
+    assert rc == 0, _lib.load().gtd_last_error()
+    assert torch.isnan(out).all()  # captured, not run
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(out, eager)
