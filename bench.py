@@ -764,11 +764,59 @@ def cfg_ensemble(args, local, peak32=None, peak64=None, hbm=None):
             line["reference_cpu"] = {"pair_interactions_per_s_per_core": ref_ips,
                                      "ensemble_steps_per_s_per_core_est": ref_ips / (inter / (len(off) - 1)),
                                      "sample": "24 random systems, evolve(leapfrog_kdk) 4 steps, collisions off"}
+            line["reference_cpu"]["all_cores"] = ensemble_reference_all_cores(off, m, r, x, v, inter)
     except Exception as exc:
         line["reference_cpu"] = {"unavailable": str(exc)}
     if args.ens_check_systems > 0:
         line["vs_oracle"] = ensemble_oracle_check(off, m, r, x, v, e.config(), local, args.ens_check_systems)
     return line
+
+
+_ENS_REF = None
+
+
+def _ens_ref_worker(task):
+    """One system of the reference's ensemble timing, in a worker process (each process holds its
+    own copy of the reference's global body-ID set, so the workers do not contend on its mutex)."""
+    global _ENS_REF
+    if _ENS_REF is None:
+        from oracle.oracle import RefOracle
+        _ENS_REF = RefOracle()
+    if task is None:
+        return 0.0
+    m, r, x, v, steps = task
+    n = len(m)
+    xo, vo, _, _ = _ENS_REF.evolve(16, m, x, v, 600.0, steps, "M66743:66740,D1:1,T1:1", r=r, coll=0)
+    _ENS_REF.check_overlap_merge(m, r, np.ones(n), xo, vo)
+    return float(steps) * n * (n - 1)
+
+
+def ensemble_reference_all_cores(off, m, r, x, v, inter, n_sample=128, steps=4, seed=3):
+    """The reference's ensemble pattern on every host core, one process per core (bdsim.cpp:82-113
+    runs one gtd::system per std::thread; the reference's bodies take their IDs from one global
+    mutex-guarded set, so its threads serialise on system construction, and separate processes
+    measure the evolve instead): n_sample seeded systems, each evolve(leapfrog_kdk) for `steps`
+    steps in one call (one initial force sweep besides the steps' own, and the system's
+    construction) followed by its check_overlap merge scan.  The sample's pair work over the pool's
+    wall time, scaled by the whole ensemble's pair work per step, estimates the reference's
+    ensemble steps/s (system-steps/s) on this host."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    rng = np.random.default_rng(seed)
+    pick = [int(s) for s in rng.choice(len(off) - 1, n_sample, replace=False) if off[s + 1] - off[s] >= 2]
+    tasks = [(m[off[s]:off[s + 1]].copy(), r[off[s]:off[s + 1]].copy(), x[off[s]:off[s + 1]].copy(),
+              v[off[s]:off[s + 1]].copy(), steps) for s in pick]
+    procs = os.cpu_count() or 1
+    with cf.ProcessPoolExecutor(procs, mp_context=mp.get_context("spawn")) as ex:
+        list(ex.map(_ens_ref_worker, [None] * procs))  # start the workers and load the library, untimed
+        t0 = time.perf_counter()
+        work = sum(ex.map(_ens_ref_worker, tasks))
+        wall = time.perf_counter() - t0
+    rate = work / wall
+    return {"pair_interactions_per_s": rate, "ensemble_steps_per_s_est": rate / (inter / (len(off) - 1)),
+            "processes": procs, "wall_s": wall,
+            "sample": f"{len(pick)} seeded systems, evolve(leapfrog_kdk) {steps} steps in one call + check_overlap, "
+                      "one system per process at a time"}
 
 
 def ensemble_oracle_check(off, m, r, x, v, config, local, n_check, steps=20, seed=11):
