@@ -819,9 +819,10 @@ def ensemble_reference_all_cores(off, m, r, x, v, inter, n_sample=128, steps=4, 
                       "one system per process at a time"}
 
 
-def ensemble_oracle_check(off, m, r, x, v, config, local, n_check, steps=20, seed=11):
-    """The checker beside the ensemble line (untimed): the same ICs, 20 KDK steps with merges in one
-    batch on the GPU (the timed configuration), and n_check seeded systems re-run one by one on the
+def ensemble_oracle_check(off, m, r, x, v, config, local, n_check, steps=60, seed=11):
+    """The checker beside the ensemble line (untimed): the same ICs, 60 KDK steps with merges in one
+    batch on the GPU (the timed configuration), and n_check seeded systems plus up to four systems
+    in which the GPU merged bodies re-run one by one on the
     oracle (the reference's KDK, then its check_overlap merge scan after each step).  Survivors and
     masses must match exactly; positions and velocities are reported relative to each system's
     largest value (the FP32 pair forces carry the mixed bar of 1e-6 relative acceleration)."""
@@ -835,7 +836,10 @@ def ensemble_oracle_check(off, m, r, x, v, config, local, n_check, steps=20, see
     e.evolve(steps)
     st = e.state()
     counts, merges, _ = e.counts()
-    pick = np.random.default_rng(seed).choice(len(off) - 1, n_check, replace=False)
+    pick = [int(s) for s in np.random.default_rng(seed).choice(len(off) - 1, n_check, replace=False)]
+    # and the systems in which merges happened (up to 4), so that merges are compared too
+    merged = [int(s) for s in np.nonzero(counts < np.diff(off))[0] if int(s) not in pick]
+    pick += merged[:4]
     t0 = time.perf_counter()
     worst_x = worst_v = 0.0
     same_survivors = same_mass = True
@@ -856,7 +860,8 @@ def ensemble_oracle_check(off, m, r, x, v, config, local, n_check, steps=20, see
         same_mass &= bool(np.array_equal(st[s]["m"], rows[:, 0]))
         worst_x = max(worst_x, float(np.abs(st[s]["x"] - rows[:, 3:6]).max() / np.abs(rows[:, 3:6]).max()))
         worst_v = max(worst_v, float(np.abs(st[s]["v"] - rows[:, 6:9]).max() / np.abs(rows[:, 6:9]).max()))
-    return {"systems": int(n_check), "steps": steps, "bodies": int(sum(off[s + 1] - off[s] for s in pick)),
+    return {"systems": len(pick), "systems_with_merges": len(merged[:4]), "steps": steps,
+            "bodies": int(sum(off[s + 1] - off[s] for s in pick)),
             "same_survivors": same_survivors, "same_masses": same_mass, "merges_gpu": gpu_merges,
             "merges_oracle": oracle_merges, "merges_all_systems_gpu": int(merges),
             "x_rel_max": worst_x, "v_rel_max": worst_v, "oracle_s": time.perf_counter() - t0}
