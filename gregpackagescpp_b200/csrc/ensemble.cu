@@ -6,16 +6,16 @@
 // std::thread (bdsim.cpp:82-113) - with FP64 state and FP32 pair forces.
 //
 // Work decomposition: one CTA owns one system at a time.  Systems are handed out largest first
-// from an atomic work counter (longest-processing-time order), so the 680x spread in per-system
-// work (N = 3 .. 2048) balances across the persistent grid.  A system's bodies are staged once per
+// from an atomic work counter (longest-processing-time order), so the spread in per-system work
+// (N = 3 .. 2048: 4.7e5x in pairs) balances across the persistent grid.  A system's bodies are staged once per
 // step in shared memory as FP32 coordinates relative to the system's mean position, with G m and
 // the radius; the rows are spread over the CTA in passes of IB rows per thread (IB = 1, 2 or 4),
 // and each thread sums its rows' forces two j-bodies per packed FP32x2 instruction, folding every
 // 64 j-bodies into FP64.  Alongside the force it keeps the smallest separation to any other body (a
 // 3-input float minimum; the one fold holding the row's own body excludes the self pair by its bit
 // pattern); a body closer to another than its radius plus the system's largest radius, plus a
-// bound on the FP32 staging error, flags the system, and only flagged systems run the exact FP64
-// merge scan.
+// bound on the FP32 staging error, flags the row; only systems with flagged rows run the exact FP64
+// merge scan, over those rows.
 #include <cuda_runtime.h>
 
 #include <algorithm>
