@@ -239,11 +239,13 @@ int gtd_adjoint_create(gtd_adjoint **out, int device, int64_t n, uint64_t steps,
     A->every = std::min<uint64_t>(checkpoint_every, steps);
     A->G = G;
     A->h = dt;
-    A->fplan = make_plan(n, GTD_PREC_F64, device, 0);
-    // the VJP kernel runs one i-body per thread: a plan with 256-body rows
+    A->fplan = make_plan(n, GTD_PREC_F64, device, tuned_variant(device, GTD_PREC_F64, n));
+    // the VJP kernel runs one i-body per thread against 256-body j-tiles: a plan with 256-body rows
+    // and tiles
     A->vplan = A->fplan;
     A->vplan.bi = kVT;
     A->vplan.rows = (n + kVT - 1) / kVT;
+    A->vplan.tiles = (n + kVT - 1) / kVT;
     A->vplan.total = A->vplan.rows * A->vplan.tiles;
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

@@ -540,10 +540,13 @@ int variant_count(int precision) { return precision == GTD_PREC_MIXED ? kNumMixe
 // Variant for a handle nobody tuned.  From N ~ 32768 up the mixed kernel is fastest with 4 i-bodies
 // per thread at 1 CTA/SM (<4,128,1,regs,U4>, variant 8: 27.4 ms against 29.1 ms for variant 0 at
 // N = 262144 on B200); below that the 2-per-thread variants keep more CTAs busy.  Small FP64
-// systems take the 32-wide work units so that every SM has work.
+// systems take the 32-wide work units so that every SM has work; up to N = 32768 one i-body per
+// thread (0.37 against 0.41 ms per force at N = 16384), above that four (4.50 against 4.64 ms at
+// N = 65536).
 int default_variant(int precision, int64_t n) {
     if (precision == GTD_PREC_MIXED) return n >= 32768 ? 8 : 0;
-    return n <= 4096 ? 4 : 0;  // FP64: 32-wide units up to N = 4096 (at least 512 units on 148 SMs)
+    if (n <= 4096) return 4;  // FP64: 32-wide units up to N = 4096 (at least 512 units on 148 SMs)
+    return n <= 32768 ? 1 : 2;
 }
 
 namespace {
