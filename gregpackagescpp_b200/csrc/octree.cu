@@ -621,9 +621,9 @@ __global__ void __launch_bounds__(kTT, sizeof(T) == 4 ? 6 : 1) walk_kernel(int64
 // every lane, and only the nodes in between take the per-lane test (one broadcast per node).
 // Leaves are accepted by every lane but their own body.  Accepted (node, lanes) pairs go to an
 // interaction list; a refused node's children go back on the stack as one sibling chain with the
-// lanes that refused it.  Evaluation: every lane runs down the list (one broadcast shared-memory
-// read per entry) and keeps the terms its mask bit selects, with walk_kernel's arithmetic per term;
-// only the order of the sum differs.
+// lanes that refused it.  Evaluation: every lane runs down the list (broadcast shared-memory reads,
+// one per component for two entries) and keeps the terms its mask bit selects, with walk_kernel's
+// arithmetic per term; only the order of the sum differs.
 // Resident warps hide the traversal's dependent loads: 4 warps per CTA with 6.25 KB of shared
 // memory each and at most 64 registers give 8 CTAs (32 warps) per SM (14.3 ms per walk at
 // N = 4194304, against 15.2 ms with a 512-entry stack at 24 warps per SM).
