@@ -29,6 +29,7 @@
 #include <cstring>
 
 #include "gtd_internal.cuh"
+#include "gtd_math.cuh"
 #include "gtd_sort.cuh"
 #include "gtd_system.cuh"
 
@@ -505,8 +506,16 @@ struct V4<double> {
     using type = double4;
 };
 
-__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
-__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+// 1/sqrt(r2) of a walk term.  FP32: the MUFU approximation with subnormal inputs flushed (a
+// separation whose square is below 2^-126 does not occur in a tree of distinct bodies; the
+// non-flushing form spends extra instructions per term on that range).  FP64: the MUFU seed and its
+// binomial correction (inv_r).
+__device__ __forceinline__ float rsqrt_t(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ double rsqrt_t(double x) { return inv_r(x); }
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ float mul_t(float a, float b) { return __fmul_rn(a, b); }
@@ -625,7 +634,7 @@ __global__ void __launch_bounds__(kTT, sizeof(T) == 4 ? 6 : 1) walk_kernel(int64
 // one per component for two entries) and keeps the terms its mask bit selects, with walk_kernel's
 // arithmetic per term; only the order of the sum differs.
 // Resident warps hide the traversal's dependent loads: 4 warps per CTA with 6.25 KB of shared
-// memory each and at most 64 registers give 8 CTAs (32 warps) per SM (14.3 ms per walk at
+// memory each and at most 64 registers give 8 CTAs (32 warps) per SM (13.5 ms per walk at
 // N = 4194304, against 15.2 ms with a 512-entry stack at 24 warps per SM).
 constexpr int kLwWarps = 4;      // warps per CTA
 constexpr int kLwStack = 320;    // stack entries per warp (a walk of 2M bodies peaks near 220)
@@ -674,7 +683,7 @@ __device__ __forceinline__ void lw_eval(const LwWarp &W, int len, unsigned lane,
         float2 r2 = __fmul2_rn(dx, dx);
         r2 = __ffma2_rn(dy, dy, r2);
         r2 = __ffma2_rn(dz, dz, r2);
-        const float2 inv = make_float2(rsqrtf(SOFT ? r2.x + eps2 : r2.x), rsqrtf(SOFT ? r2.y + eps2 : r2.y));
+        const float2 inv = make_float2(rsqrt_t(SOFT ? r2.x + eps2 : r2.x), rsqrt_t(SOFT ? r2.y + eps2 : r2.y));
         float2 sc = __fmul2_rn(__fmul2_rn(__fmul2_rn(M, inv), inv), inv);
         sc.x = b0 ? sc.x : 0.f;
         sc.y = b1 ? sc.y : 0.f;
@@ -700,7 +709,7 @@ __device__ __forceinline__ void lw_eval(const LwWarp &W, int len, unsigned lane,
         const unsigned bit = (W.lm[e] >> lane) & 1u;
         const float dx = __fsub_rn(X, p.x), dy = __fsub_rn(Y, p.y), dz = __fsub_rn(Z, p.z);
         const float r2 = lw_r2(dx, dy, dz);
-        const float inv = rsqrtf(SOFT ? r2 + eps2 : r2);
+        const float inv = rsqrt_t(SOFT ? r2 + eps2 : r2);
         float sc = __fmul_rn(__fmul_rn(__fmul_rn(M, inv), inv), inv);
         sc = bit ? sc : 0.f;
         fx.x = __fmaf_rn(sc, dx, fx.x);
@@ -950,7 +959,7 @@ using namespace gtd;
 static unsigned blocks_for(int64_t n, int t = kTT) { return (unsigned)((n + t - 1) / t); }
 
 // Float walk: 0 = walk_kernel with A and B in separate arrays, 1 = walk_kernel with interleaved
-// records, 2 = list_walk_kernel (interleaved records; the default: 15.3 ms against 22.6 ms for 1 at
+// records, 2 = list_walk_kernel (interleaved records; the default: 13.5 ms against 21.0 ms for 1 at
 // N = 4194304, theta = 0.5).  Double trees take walk_kernel.
 constexpr int kDefaultWalkVariant = 2;
 constexpr int kNumWalkVariants = 3;
