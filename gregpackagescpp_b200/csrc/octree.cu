@@ -630,11 +630,11 @@ __global__ void __launch_bounds__(kTT, sizeof(T) == 4 ? 6 : 1) walk_kernel(int64
 // every lane, and only the nodes in between take the per-lane test (one broadcast per node).
 // Leaves are accepted by every lane but their own body.  Accepted (node, lanes) pairs go to an
 // interaction list; a refused node's children go back on the stack as one sibling chain with the
-// lanes that refused it.  Evaluation: every lane runs down the list (broadcast shared-memory reads,
-// one per component for two entries) and keeps the terms its mask bit selects, with walk_kernel's
-// arithmetic per term; only the order of the sum differs.
+// lanes that refused it.  Evaluation: every lane runs down the list (three broadcast shared-memory
+// reads per two entries, stored as interleaved pairs) and keeps the terms its mask bit selects, with
+// walk_kernel's arithmetic per term; only the order of the sum differs.
 // Resident warps hide the traversal's dependent loads: 4 warps per CTA with 6.25 KB of shared
-// memory each and at most 64 registers give 8 CTAs (32 warps) per SM (13.5 ms per walk at
+// memory each and at most 64 registers give 8 CTAs (32 warps) per SM (13.1 ms per walk at
 // N = 4194304, against 15.2 ms with a 512-entry stack at 24 warps per SM).
 constexpr int kLwWarps = 4;      // warps per CTA
 constexpr int kLwStack = 320;    // stack entries per warp (a walk of 2M bodies peaks near 220)
@@ -644,11 +644,24 @@ constexpr int kLwList = 128;     // list entries per warp before an evaluation p
 struct LwWarp {
     int st[kLwStack], en[kLwStack];  // sibling chain: nodes st, skip[st], ... below en
     unsigned mk[kLwStack];           // lanes still walking below the chain's parent
-    // accepted node: centre of mass and G M (or a bucket leaf's body), one array per component so
-    // that entries e and e+1 load as one float2 per component
-    float lx[kLwList], ly[kLwList], lz[kLwList], lw[kLwList];
+    // accepted node: centre of mass and G M (or a bucket leaf's body), stored by pairs of entries:
+    // pxy[q] = (x, x', y, y') and pzw[q] = (z, z', w, w') of entries 2q and 2q + 1, so that the
+    // evaluation reads two entries with two float4 loads whose halves are its FP32x2 operands
+    float4 pxy[kLwList / 2], pzw[kLwList / 2];
     unsigned lm[kLwList];            // lanes that take it
 };
+static_assert(kLwList % 2 == 0 && (3 * kLwStack * sizeof(int)) % 16 == 0, "float4 pairs of list entries");
+
+// writes list entry `at`
+__device__ __forceinline__ void lw_put(LwWarp &W, int at, float x, float y, float z, float w, unsigned m) {
+    float *a = reinterpret_cast<float *>(&W.pxy[at >> 1]) + (at & 1);
+    float *b = reinterpret_cast<float *>(&W.pzw[at >> 1]) + (at & 1);
+    a[0] = x;
+    a[2] = y;
+    b[0] = z;
+    b[2] = w;
+    W.lm[at] = m;
+}
 constexpr size_t kLwSmem = sizeof(LwWarp) * kLwWarps;
 
 __device__ __forceinline__ float lw_r2(float dx, float dy, float dz) {
@@ -671,14 +684,14 @@ __device__ __forceinline__ void lw_eval(const LwWarp &W, int len, unsigned lane,
                                         float &ay, float &az, uint32_t &cnt) {
     const float2 npx = make_float2(-p.x, -p.x), npy = make_float2(-p.y, -p.y), npz = make_float2(-p.z, -p.z);
     const float2 zero = make_float2(0.f, 0.f);
+    const unsigned lbit = 1u << lane;
     float2 fx = zero, fy = zero, fz = zero, gx = zero, gy = zero, gz = zero;
-    auto pair = [&](int e, float2 &ox, float2 &oy, float2 &oz) {
-        const float2 X = *reinterpret_cast<const float2 *>(&W.lx[e]);
-        const float2 Y = *reinterpret_cast<const float2 *>(&W.ly[e]);
-        const float2 Z = *reinterpret_cast<const float2 *>(&W.lz[e]);
-        const float2 M = *reinterpret_cast<const float2 *>(&W.lw[e]);
+    auto pair = [&](int e, float2 &ox, float2 &oy, float2 &oz) {  // entries e, e + 1 (e even)
+        const float4 P = W.pxy[e >> 1], Q = W.pzw[e >> 1];
+        const float2 X = make_float2(P.x, P.y), Y = make_float2(P.z, P.w);
+        const float2 Z = make_float2(Q.x, Q.y), M = make_float2(Q.z, Q.w);
         const uint2 mk = *reinterpret_cast<const uint2 *>(&W.lm[e]);
-        const unsigned b0 = (mk.x >> lane) & 1u, b1 = (mk.y >> lane) & 1u;
+        const bool b0 = (mk.x & lbit) != 0u, b1 = (mk.y & lbit) != 0u;
         const float2 dx = __fadd2_rn(X, npx), dy = __fadd2_rn(Y, npy), dz = __fadd2_rn(Z, npz);
         float2 r2 = __fmul2_rn(dx, dx);
         r2 = __ffma2_rn(dy, dy, r2);
@@ -690,7 +703,7 @@ __device__ __forceinline__ void lw_eval(const LwWarp &W, int len, unsigned lane,
         ox = __ffma2_rn(sc, dx, ox);
         oy = __ffma2_rn(sc, dy, oy);
         oz = __ffma2_rn(sc, dz, oz);
-        if constexpr (COUNT) cnt += b0 + b1;
+        if constexpr (COUNT) cnt += (b0 ? 1u : 0u) + (b1 ? 1u : 0u);
     };
     int e = 0;
     for (; e + 3 < len; e += 4) {  // two independent pairs per step
@@ -704,9 +717,10 @@ __device__ __forceinline__ void lw_eval(const LwWarp &W, int len, unsigned lane,
     fx = __fadd2_rn(fx, gx);
     fy = __fadd2_rn(fy, gy);
     fz = __fadd2_rn(fz, gz);
-    if (e < len) {
-        const float X = W.lx[e], Y = W.ly[e], Z = W.lz[e], M = W.lw[e];
-        const unsigned bit = (W.lm[e] >> lane) & 1u;
+    if (e < len) {  // e even: the first half of its pair
+        const float4 P = W.pxy[e >> 1], Q = W.pzw[e >> 1];
+        const float X = P.x, Y = P.z, Z = Q.x, M = Q.z;
+        const bool bit = (W.lm[e] & lbit) != 0u;
         const float dx = __fsub_rn(X, p.x), dy = __fsub_rn(Y, p.y), dz = __fsub_rn(Z, p.z);
         const float r2 = lw_r2(dx, dy, dz);
         const float inv = rsqrt_t(SOFT ? r2 + eps2 : r2);
@@ -715,7 +729,7 @@ __device__ __forceinline__ void lw_eval(const LwWarp &W, int len, unsigned lane,
         fx.x = __fmaf_rn(sc, dx, fx.x);
         fy.x = __fmaf_rn(sc, dy, fy.x);
         fz.x = __fmaf_rn(sc, dz, fz.x);
-        if constexpr (COUNT) cnt += bit;
+        if constexpr (COUNT) cnt += bit ? 1u : 0u;
     }
     ax += fx.x + fx.y;
     ay += fy.x + fy.y;
@@ -820,11 +834,10 @@ __global__ void __launch_bounds__(kLwWarps * 32, 8) list_walk_kernel(int64_t n, 
             mm &= mm - 1;
             const float cx = __shfl_sync(0xffffffffu, A.x, j), cy = __shfl_sync(0xffffffffu, A.y, j);
             const float cz = __shfl_sync(0xffffffffu, A.z, j), cw = __shfl_sync(0xffffffffu, w2, j);
-            const unsigned cm = __shfl_sync(0xffffffffu, mk, j);
             const float dx = __fsub_rn(cx, p.x), dy = __fsub_rn(cy, p.y), dz = __fsub_rn(cz, p.z);
-            const bool ok = ((cm >> lane) & 1u) && cw < __fmul_rn(th2, lw_r2(dx, dy, dz));
-            const unsigned a = __ballot_sync(0xffffffffu, ok);
-            if ((int)lane == j) acc = a;
+            // every lane tests; lane j keeps the answers of the lanes in its node's mask
+            const unsigned a = __ballot_sync(0xffffffffu, cw < __fmul_rn(th2, lw_r2(dx, dy, dz)));
+            if ((int)lane == j) acc = a & mk;
         }
         unsigned em = 0;
         if (leaf && count == 1) {
@@ -837,14 +850,7 @@ __global__ void __launch_bounds__(kLwWarps * 32, 8) list_walk_kernel(int64_t n, 
         }
         const bool app = em != 0u;
         const unsigned ab = __ballot_sync(0xffffffffu, app);
-        if (app) {
-            const int at = len + __popc(ab & lt);
-            W.lx[at] = A.x;
-            W.ly[at] = A.y;
-            W.lz[at] = A.z;
-            W.lw[at] = A.w;
-            W.lm[at] = em;
-        }
+        if (app) lw_put(W, len + __popc(ab & lt), A.x, A.y, A.z, A.w, em);
         len += __popc(ab);
         const bool rem = have && B.x < en;
         const unsigned rb = __ballot_sync(0xffffffffu, rem);
@@ -885,13 +891,8 @@ __global__ void __launch_bounds__(kLwWarps * 32, 8) list_walk_kernel(int64_t n, 
                 const bool ap = q0 + (int)lane < c && m1 != 0u;
                 const unsigned b2 = __ballot_sync(0xffffffffu, ap);
                 if (ap) {
-                    const int at = len + __popc(b2 & lt);
                     const float4 Q = bodies[q];
-                    W.lx[at] = Q.x;
-                    W.ly[at] = Q.y;
-                    W.lz[at] = Q.z;
-                    W.lw[at] = Q.w;
-                    W.lm[at] = m1;
+                    lw_put(W, len + __popc(b2 & lt), Q.x, Q.y, Q.z, Q.w, m1);
                 }
                 len += __popc(b2);
             }
@@ -959,7 +960,7 @@ using namespace gtd;
 static unsigned blocks_for(int64_t n, int t = kTT) { return (unsigned)((n + t - 1) / t); }
 
 // Float walk: 0 = walk_kernel with A and B in separate arrays, 1 = walk_kernel with interleaved
-// records, 2 = list_walk_kernel (interleaved records; the default: 13.5 ms against 21.0 ms for 1 at
+// records, 2 = list_walk_kernel (interleaved records; the default: 13.1 ms against 21.0 ms for 1 at
 // N = 4194304, theta = 0.5).  Double trees take walk_kernel.
 constexpr int kDefaultWalkVariant = 2;
 constexpr int kNumWalkVariants = 3;
