@@ -37,6 +37,38 @@ struct VjpArgs {
 
 constexpr int kVT = 256;
 
+// One staged j-tile against body k.  The J^T w sum is kept as two parts, sum u / r^3 (j*) and
+// sum (d . u) d / r^5 (k*), combined as j - 3 k by the caller, so that the factor 3 costs no
+// operation per pair; with the |r|^-1 correction that is 34 FP64 operations per pair.  kGuard: the
+// tile holds k itself or padding bodies (r2 = 0 or a zero mass), whose terms are selected away; every
+// other tile runs without the compare.
+template <bool kGuard>
+__device__ __forceinline__ void vjp_tile(const double4 *__restrict__ tx, const double4 *__restrict__ tw,
+                                         const double4 &xk, const double4 &wk, double &jx, double &jy, double &jz,
+                                         double &kx, double &ky, double &kz, double &mu) {
+#pragma unroll 2
+    for (int jj = 0; jj < kVT; ++jj) {
+        const double4 xj = tx[jj], wj = tw[jj];
+        const double dx = xj.x - xk.x, dy = xj.y - xk.y, dz = xj.z - xk.z;
+        const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+        double inv = inv_r(r2);
+        if (kGuard) inv = r2 > 0.0 ? inv : 0.0;  // j == k and padding contribute nothing
+        const double inv2 = inv * inv, inv3 = inv2 * inv, inv5 = inv3 * inv2;
+        const double ux = xk.w * wj.x - xj.w * wk.x;
+        const double uy = xk.w * wj.y - xj.w * wk.y;
+        const double uz = xk.w * wj.z - xj.w * wk.z;
+        const double c5 = fma(dz, uz, fma(dy, uy, dx * ux)) * inv5;
+        jx = fma(inv3, ux, jx);
+        jy = fma(inv3, uy, jy);
+        jz = fma(inv3, uz, jz);
+        kx = fma(c5, dx, kx);
+        ky = fma(c5, dy, ky);
+        kz = fma(c5, dz, kz);
+        const double wd = fma(wj.z, dz, fma(wj.y, dy, wj.x * dx));
+        mu = fma(-wd, inv3, mu);
+    }
+}
+
 // Partial VJP sums over j-tiles; same (row, tile) stream-K split as the force kernel, I = 1.
 __global__ void __launch_bounds__(kVT) vjp_kernel(VjpArgs a) {
     __shared__ double4 tx[kVT];
@@ -55,36 +87,24 @@ __global__ void __launch_bounds__(kVT) vjp_kernel(VjpArgs a) {
             xk = a.x[k];
             wk = a.w[k];
         }
-        double jx = 0, jy = 0, jz = 0, mu = 0;
+        double jx = 0, jy = 0, jz = 0, kx = 0, ky = 0, kz = 0, mu = 0;
         for (int64_t jt = jt0; jt < jt1; ++jt) {
             const int64_t j = jt * kVT + t;
             __syncthreads();
             tx[t] = j < a.n ? a.x[j] : make_double4(0, 0, 0, 0);
             tw[t] = j < a.n ? a.w[j] : make_double4(0, 0, 0, 0);
             __syncthreads();
-#pragma unroll 2
-            for (int jj = 0; jj < kVT; ++jj) {
-                const double4 xj = tx[jj], wj = tw[jj];
-                const double dx = xj.x - xk.x, dy = xj.y - xk.y, dz = xj.z - xk.z;
-                const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-                const double inv = r2 > 0.0 ? inv_r(r2) : 0.0;  // j == k and padding contribute nothing
-                const double inv2 = inv * inv, inv3 = inv2 * inv;
-                const double ux = xk.w * wj.x - xj.w * wk.x;
-                const double uy = xk.w * wj.y - xj.w * wk.y;
-                const double uz = xk.w * wj.z - xj.w * wk.z;
-                const double du = fma(dz, uz, fma(dy, uy, dx * ux));
-                const double c5 = 3.0 * du * inv3 * inv2;
-                jx = fma(inv3, ux, fma(-c5, dx, jx));
-                jy = fma(inv3, uy, fma(-c5, dy, jy));
-                jz = fma(inv3, uz, fma(-c5, dz, jz));
-                const double wd = fma(wj.z, dz, fma(wj.y, dy, wj.x * dx));
-                mu = fma(-wd, inv3, mu);
-            }
+            // rows and tiles are both kVT bodies wide (bi == kVT): tile r holds the row's own bodies
+            const bool guard = jt == r || (jt + 1) * kVT > a.n;
+            if (guard)
+                vjp_tile<true>(tx, tw, xk, wk, jx, jy, jz, kx, ky, kz, mu);
+            else
+                vjp_tile<false>(tx, tw, xk, wk, jx, jy, jz, kx, ky, kz, mu);
         }
         double *slot = a.part + (size_t)(blockIdx.x + r) * 4 * a.bi;
-        slot[t] = jx;
-        slot[a.bi + t] = jy;
-        slot[2 * a.bi + t] = jz;
+        slot[t] = fma(-3.0, kx, jx);
+        slot[a.bi + t] = fma(-3.0, ky, jy);
+        slot[2 * a.bi + t] = fma(-3.0, kz, jz);
         slot[3 * a.bi + t] = mu;
         s = row_end;
     }

@@ -9,8 +9,9 @@
 namespace gtd {
 
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;                      // keys per thread per block chunk
-constexpr int kChunk = kSortThreads * kSortItems;   // keys per block
+constexpr int kHalfItems = 8;                        // keys per thread per chunk
+constexpr int kHalf = kSortThreads * kHalfItems;     // keys per chunk (a block takes a run of chunks)
+constexpr int kScatterBlocksPerSm = 4;               // the scatter's launch bound (at most 64 registers)
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -95,35 +96,31 @@ int exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *s
 }
 
 // ---- radix sort ----------------------------------------------------------------------------
+// Block b of a pass owns the keys [b * per_block, (b + 1) * per_block), per_block a whole number of
+// kHalf-key chunks: the grid is one wave of the scatter kernel, whatever n is (radix_grid).
 __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const unsigned long long *keys, int64_t n,
-                                                                  int shift, uint32_t *hist, int blocks) {
+                                                                  int shift, uint32_t *hist, int blocks,
+                                                                  int64_t per_block) {
     __shared__ uint32_t h[256];
     h[threadIdx.x] = 0;
     __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * kChunk;
-    for (int k = 0; k < kSortItems; ++k) {
-        const int64_t i = base + (int64_t)k * kSortThreads + threadIdx.x;
-        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xffu], 1u);
-    }
+    const int64_t base = (int64_t)blockIdx.x * per_block;
+    const int64_t end = min(base + per_block, n);
+    for (int64_t i = base + threadIdx.x; i < end; i += kSortThreads) atomicAdd(&h[(keys[i] >> shift) & 0xffu], 1u);
     __syncthreads();
     hist[(size_t)threadIdx.x * blocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Stable scatter.  A block takes its chunk in two halves of kHalf keys.  In a half, warp w owns the
+// Stable scatter.  A block takes its keys in chunks of kHalf.  In a chunk, warp w owns the
 // contiguous keys w*256 .. w*256+255 (eight rounds of 32, in index order) and ranks them stably
 // inside its own digit counters (match_any per round, warp-synchronous: no block barrier); one block
 // scan over the 256 digits then turns the per-warp counts into offsets, the keys are placed
 // digit-sorted in shared memory and written out in that order: keys of one digit go to consecutive
 // addresses, so the stores fill whole sectors instead of one 8-byte store per key.  Seven block
-// barriers per half (the earlier block-wide ranking rounds took 34).
-constexpr int kHalfItems = kSortItems / 2;
-constexpr int kHalf = kSortThreads * kHalfItems;
-
-__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsigned long long *keys_in,
-                                                                     const int32_t *vals_in,
-                                                                     unsigned long long *keys_out,
-                                                                     int32_t *vals_out, int64_t n, int shift,
-                                                                     const uint32_t *offsets, int blocks) {
+// barriers per chunk (the earlier block-wide ranking rounds took 34).
+__global__ void __launch_bounds__(kSortThreads, kScatterBlocksPerSm) radix_scatter_kernel(
+    const unsigned long long *keys_in, const int32_t *vals_in, unsigned long long *keys_out, int32_t *vals_out,
+    int64_t n, int shift, const uint32_t *offsets, int blocks, int64_t per_block) {
     constexpr int kWarps = kSortThreads / 32;
     static_assert(kHalf == kWarps * 32 * kHalfItems, "a warp owns kHalfItems rounds of 32 keys");
     __shared__ unsigned long long sk[kHalf];
@@ -133,9 +130,9 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsig
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const unsigned lt = (1u << lane) - 1u;
     run_global[t] = offsets[(size_t)t * blocks + blockIdx.x];
-    const int64_t base = (int64_t)blockIdx.x * kChunk;
-    for (int h = 0; h < 2; ++h) {
-        const int64_t hbase = base + (int64_t)h * kHalf;
+    const int64_t base = (int64_t)blockIdx.x * per_block;
+    const int64_t end = min(base + per_block, n);
+    for (int64_t hbase = base; hbase < end; hbase += kHalf) {
         unsigned long long key[kHalfItems];
         int32_t val[kHalfItems];
         uint32_t dig[kHalfItems], wr[kHalfItems];
@@ -147,7 +144,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsig
             key[k] = 0;
             val[k] = 0;
             dig[k] = 256;  // absent keys get a digit no key has
-            if (i < n) {
+            if (i < end) {
                 key[k] = keys_in[i];
                 val[k] = vals_in[i];
                 dig[k] = (uint32_t)((key[k] >> shift) & 0xffu);
@@ -204,8 +201,8 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsig
             }
         }
         __syncthreads();
-        const int64_t rem = n - hbase;
-        const int hcount = rem <= 0 ? 0 : (rem < kHalf ? (int)rem : kHalf);
+        const int64_t rem = end - hbase;
+        const int hcount = rem < kHalf ? (int)rem : kHalf;
 #pragma unroll
         for (int k = 0; k < kHalfItems; ++k) {
             const int i = k * kSortThreads + t;
@@ -225,8 +222,37 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const unsig
     }
 }
 
+// The scatter's resident blocks per SM on the current device (its launch bound or less).
+static int scatter_blocks_per_sm() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+    int *c = dev < 64 ? &cached[dev] : nullptr;
+    if (c && *c > 0) return *c;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, radix_scatter_kernel, kSortThreads, 0) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    if (c) *c = per_sm;
+    return per_sm;
+}
+
+// Grid of a pass: blocks of a whole number of chunks each, as few chunks per block as one wave of
+// the scatter kernel allows (a second, partial wave would cost as much as the first).
+static void radix_grid(int64_t n, int *blocks, int64_t *per_block) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+    const int64_t slots = (int64_t)sms * scatter_blocks_per_sm();
+    const int64_t chunks = (n + kHalf - 1) / kHalf;
+    const int64_t cpb = (chunks + slots - 1) / slots;
+    *per_block = cpb * kHalf;
+    *blocks = (int)((chunks + cpb - 1) / cpb);
+}
+
+// Sized for one block per chunk, the most any device's grid takes.
 size_t radix_scratch_words(int64_t n) {
-    const int64_t blocks = (n + kChunk - 1) / kChunk;
+    const int64_t blocks = (n + kHalf - 1) / kHalf;
     const int64_t h = 256 * blocks;
     return (size_t)h + scan_scratch_words(h);
 }
@@ -236,18 +262,20 @@ size_t radix_scratch_words(int64_t n) {
 int radix_sort_u64(unsigned long long *keys, int32_t *vals, unsigned long long *keys_alt, int32_t *vals_alt,
                    int64_t n, int bits, uint32_t *scratch, cudaStream_t s, uint64_t *launches) {
     if (n <= 1) return GTD_OK;
-    const int blocks = (int)((n + kChunk - 1) / kChunk);
+    int blocks = 1;
+    int64_t per_block = kHalf;
+    radix_grid(n, &blocks, &per_block);
     uint32_t *hist = scratch;
     uint32_t *scan_scratch = scratch + (size_t)256 * blocks;
     unsigned long long *ka = keys, *kb = keys_alt;
     int32_t *va = vals, *vb = vals_alt;
     int passes = 0;
     for (int shift = 0; shift < bits; shift += 8, ++passes) {
-        radix_hist_kernel<<<blocks, kSortThreads, 0, s>>>(ka, n, shift, hist, blocks);
+        radix_hist_kernel<<<blocks, kSortThreads, 0, s>>>(ka, n, shift, hist, blocks, per_block);
         GTD_CHECK_LAUNCH();
         int rc = exclusive_scan_u32(hist, hist, (int64_t)256 * blocks, scan_scratch, s, launches);
         if (rc) return rc;
-        radix_scatter_kernel<<<blocks, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist, blocks);
+        radix_scatter_kernel<<<blocks, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist, blocks, per_block);
         GTD_CHECK_LAUNCH();
         if (launches) *launches += 2;
         unsigned long long *tk = ka; ka = kb; kb = tk;
