@@ -13,12 +13,14 @@
 //     (dL/dm)_k += sum_j G (w_j . (x_k - x_j)) / r^3.
 // Memory: sqrt(T)-step checkpointing.  The forward keeps (x, v_{k-1/2}, a) every C steps; the
 // reverse sweep recomputes one segment of positions at a time from its checkpoint, then runs the
-// segment's VJPs backwards.  Both the force and the VJP use the stream-K FP64 decomposition of
-// direct.cu (every SM gets the same number of pair tiles whatever N is).
+// segment's VJPs backwards.  The force uses the stream-K FP64 decomposition of direct.cu; the VJP
+// takes each unordered pair once (vjp_sym_kernel: the J^T w term is antisymmetric in the pair),
+// or, where that kernel's partial sums would not fit, every ordered pair (vjp_kernel).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "gtd_internal.cuh"
@@ -107,6 +109,208 @@ __global__ void __launch_bounds__(kVT) vjp_kernel(VjpArgs a) {
         slot[2 * a.bi + t] = fma(-3.0, kz, jz);
         slot[3 * a.bi + t] = mu;
         s = row_end;
+    }
+}
+
+// ---- symmetric VJP ---------------------------------------------------------------------------
+// The J^T w term of a pair is antisymmetric: with d = x_j - x_k and u = m_k w_j - m_j w_k, body k
+// receives T = u / r^3 - 3 d (d . u) / r^5 and body j receives -T.  So each unordered pair of
+// 256-body blocks (r < c) is evaluated once, 45 FP64 operations per pair for both bodies' J^T w and
+// mass terms (two ordered pairs cost 68 in vjp_kernel); a diagonal block (r == r) sums its ordered
+// pairs for its own rows only.  Work: items (r, c), c >= r, in row-major order, each cut into 8
+// units of 32 columns; CTA g takes the contiguous units [g U / grid, (g + 1) U / grid), so a CTA
+// touches consecutive items and every CTA has the same number of units.
+//   Rows: summed in registers over the units of an item, written to slot g + item (unique per
+//   (CTA, item), as in the stream-K split of the force kernel).
+//   Columns: inside a unit a warp's lane l pairs its row with column (l + s) mod 32 at step s and
+//   carries that column's running sum, passed on to lane l - 1 after each step by one shuffle, so
+//   lane l ends holding column l; the 8 warps' sums are added in warp order and written per unit.
+// Every sum is taken in a fixed order: the results are bit-reproducible.
+constexpr int kSymChunks = kVT / 32;  // units per item
+
+struct SymArgs {
+    int64_t n;
+    int nb;          // 256-body blocks
+    int64_t items;   // nb (nb + 1) / 2
+    int64_t units;   // items * kSymChunks
+    int grid;
+    const int2 *item_rc;  // item -> (r, c)
+    const double4 *x;     // positions + mass
+    const double4 *w;     // c_k * lambda_v
+    double *rowpart;      // (grid + items) slots of 4 x kVT doubles
+    double *colpart;      // units slots of 4 x 32 doubles
+};
+
+// The pair terms of body k against body j (d = x_j - x_k): T (for k; -T for j) and the two mass
+// terms, mk_term for k's mass sum and mj_term for j's.
+template <bool kGuard>
+__device__ __forceinline__ void sym_pair(const double4 &xk, const double4 &wk, const double4 &xj, const double4 &wj,
+                                         double &tx, double &ty, double &tz, double &mk_term, double &mj_term) {
+    const double dx = xj.x - xk.x, dy = xj.y - xk.y, dz = xj.z - xk.z;
+    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+    double inv = inv_r(r2);
+    if (kGuard) inv = r2 > 0.0 ? inv : 0.0;  // the self pair and padding contribute nothing
+    const double inv2 = inv * inv, inv3 = inv2 * inv, inv5 = inv3 * inv2;
+    const double ux = xk.w * wj.x - xj.w * wk.x;
+    const double uy = xk.w * wj.y - xj.w * wk.y;
+    const double uz = xk.w * wj.z - xj.w * wk.z;
+    const double c5 = 3.0 * (fma(dz, uz, fma(dy, uy, dx * ux)) * inv5);
+    tx = fma(inv3, ux, -c5 * dx);
+    ty = fma(inv3, uy, -c5 * dy);
+    tz = fma(inv3, uz, -c5 * dz);
+    mk_term = -fma(wj.z, dz, fma(wj.y, dy, wj.x * dx)) * inv3;
+    mj_term = fma(wk.z, dz, fma(wk.y, dy, wk.x * dx)) * inv3;
+}
+
+__global__ void __launch_bounds__(kVT, 2) vjp_sym_kernel(SymArgs a) {
+    // the column block, one array per component: a warp reads 32 different bodies per step (lane l
+    // the body (l + s) mod 32), which as 8-byte words fall in distinct banks
+    __shared__ double cxx[kVT], cxy[kVT], cxz[kVT], cxm[kVT], cwx[kVT], cwy[kVT], cwz[kVT];
+    __shared__ double red[kVT / 32][4][32];
+    auto col_x = [&](int i) { return make_double4(cxx[i], cxy[i], cxz[i], cxm[i]); };
+    auto col_w = [&](int i) { return make_double4(cwx[i], cwy[i], cwz[i], 0.0); };
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int64_t u0 = (int64_t)blockIdx.x * a.units / a.grid;
+    const int64_t u1 = (int64_t)(blockIdx.x + 1) * a.units / a.grid;
+    int64_t cur = -1;
+    int r = 0, c = 0;
+    double4 xk = make_double4(0, 0, 0, 0), wk = xk;
+    double rx = 0, ry = 0, rz = 0, rm = 0;
+    auto flush_rows = [&]() {
+        double *slot = a.rowpart + (size_t)(blockIdx.x + cur) * 4 * kVT;
+        slot[t] = rx;
+        slot[kVT + t] = ry;
+        slot[2 * kVT + t] = rz;
+        slot[3 * kVT + t] = rm;
+        rx = ry = rz = rm = 0;
+    };
+    for (int64_t u = u0; u < u1; ++u) {
+        const int64_t q = u / kSymChunks;
+        const int chunk = (int)(u - q * kSymChunks);
+        if (q != cur) {
+            if (cur >= 0) flush_rows();
+            cur = q;
+            const int2 rc = a.item_rc[q];
+            r = rc.x;
+            c = rc.y;
+            const int64_t k = (int64_t)r * kVT + t;
+            xk = k < a.n ? a.x[k] : make_double4(0, 0, 0, 0);
+            wk = k < a.n ? a.w[k] : make_double4(0, 0, 0, 0);
+            const int64_t j = (int64_t)c * kVT + t;
+            const double4 qx = j < a.n ? a.x[j] : make_double4(0, 0, 0, 0);
+            const double4 qw = j < a.n ? a.w[j] : make_double4(0, 0, 0, 0);
+            __syncthreads();  // the previous item's columns are no longer read
+            cxx[t] = qx.x;
+            cxy[t] = qx.y;
+            cxz[t] = qx.z;
+            cxm[t] = qx.w;
+            cwx[t] = qw.x;
+            cwy[t] = qw.y;
+            cwz[t] = qw.z;
+            __syncthreads();
+        }
+        const int jb = chunk * 32;
+        if (r == c) {
+            // diagonal block: the row's ordered pairs with this chunk's columns, self pair excluded
+            for (int i = 0; i < 32; ++i) {
+                double tx, ty, tz, mk, mj;
+                sym_pair<true>(xk, wk, col_x(jb + i), col_w(jb + i), tx, ty, tz, mk, mj);
+                rx += tx;
+                ry += ty;
+                rz += tz;
+                rm += mk;
+            }
+        } else {
+            double cx = 0, cy = 0, cz = 0, cm = 0;  // running sums of column (lane + s) mod 32
+            const bool guard = (int64_t)(c + 1) * kVT > a.n;  // padding columns in the last block
+            auto step = [&](auto gd, int s) {
+                const int i = jb + ((lane + s) & 31);
+                double tx, ty, tz, mk, mj;
+                sym_pair<decltype(gd)::value>(xk, wk, col_x(i), col_w(i), tx, ty, tz, mk, mj);
+                rx += tx;
+                ry += ty;
+                rz += tz;
+                rm += mk;
+                cx -= tx;
+                cy -= ty;
+                cz -= tz;
+                cm += mj;
+                const int from = (lane + 1) & 31;
+                cx = __shfl_sync(0xffffffffu, cx, from);
+                cy = __shfl_sync(0xffffffffu, cy, from);
+                cz = __shfl_sync(0xffffffffu, cz, from);
+                cm = __shfl_sync(0xffffffffu, cm, from);
+            };
+            if (guard) {
+                for (int s2 = 0; s2 < 32; ++s2) step(std::true_type{}, s2);
+            } else {
+#pragma unroll 2
+                for (int s2 = 0; s2 < 32; ++s2) step(std::false_type{}, s2);
+            }
+            // after 32 steps and 32 passes lane l holds column l's sum over this warp's rows
+            red[warp][0][lane] = cx;
+            red[warp][1][lane] = cy;
+            red[warp][2][lane] = cz;
+            red[warp][3][lane] = cm;
+            __syncthreads();
+            if (t < 128) {
+                const int comp = t >> 5;
+                double sum = 0;
+#pragma unroll
+                for (int w2 = 0; w2 < kVT / 32; ++w2) sum += red[w2][comp][lane];
+                a.colpart[((size_t)u * 4 + comp) * 32 + lane] = sum;
+            }
+            __syncthreads();
+        }
+    }
+    if (cur >= 0) flush_rows();
+}
+
+// The combine of vjp_sym_kernel's sums for body i of block b (fixed order: its row slots over the
+// items (b, c), c = b .. nb-1, then its column sums over the items (r, b), r < b), then the same
+// update as vjp_combine_kernel.
+__global__ void vjp_sym_combine_kernel(SymArgs a, double G, double4 *lx, double4 *lv, double *mu, double h,
+                                       int drift) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int b = (int)(i / kVT);
+    const int t = (int)(i - (int64_t)b * kVT);
+    const int nb = a.nb;
+    double jx = 0, jy = 0, jz = 0, m = 0;
+    const int64_t qb = (int64_t)b * nb - (int64_t)b * (b - 1) / 2;  // item (b, b)
+    for (int c = b; c < nb; ++c) {
+        const int64_t q = qb + (c - b);
+        const int64_t g0 = ((q * kSymChunks + 1) * (int64_t)a.grid - 1) / a.units;
+        const int64_t g1 = ((q * kSymChunks + kSymChunks) * (int64_t)a.grid - 1) / a.units;
+        for (int64_t g = g0; g <= g1; ++g) {
+            const double *slot = a.rowpart + (size_t)(g + q) * 4 * kVT;
+            jx += slot[t];
+            jy += slot[kVT + t];
+            jz += slot[2 * kVT + t];
+            m += slot[3 * kVT + t];
+        }
+    }
+    const int chunk = t >> 5, lane = t & 31;
+    for (int r = 0; r < b; ++r) {
+        const int64_t q = (int64_t)r * nb - (int64_t)r * (r - 1) / 2 + (b - r);
+        const double *cp = a.colpart + (size_t)(q * kSymChunks + chunk) * 4 * 32;
+        jx += cp[lane];
+        jy += cp[32 + lane];
+        jz += cp[64 + lane];
+        m += cp[96 + lane];
+    }
+    double4 x = lx[i];
+    x.x = fma(G, jx, x.x);
+    x.y = fma(G, jy, x.y);
+    x.z = fma(G, jz, x.z);
+    lx[i] = x;
+    mu[i] = fma(G, m, mu[i]);
+    if (drift) {
+        double4 v = lv[i];
+        v.x = fma(h, x.x, v.x);
+        v.y = fma(h, x.y, v.y);
+        v.z = fma(h, x.z, v.z);
+        lv[i] = v;
     }
 }
 
@@ -210,6 +414,11 @@ struct gtd_adjoint {
     double4 *seg = nullptr;                                // positions of one segment [(every+1) * n]
     double4 *lx = nullptr, *lv = nullptr, *w = nullptr;
     double *mu = nullptr;
+    // symmetric VJP (vjp_sym_kernel) when its partial sums fit kSymMaxBytes, else vjp_kernel
+    bool sym = false;
+    SymArgs sa{};
+    int2 *item_rc = nullptr;
+    double *rowpart = nullptr, *colpart = nullptr;
     bool have_forward = false;
     uint64_t launches = 0;
 };
@@ -230,7 +439,22 @@ static int adj_force(gtd_adjoint *A, const double4 *x, cudaStream_t st) {
     return rc;
 }
 
+// The symmetric VJP keeps 8 KB of row sums per (CTA, item) and 8 KB of column sums per item:
+// 38 MB at N = 16384; above this size (N ~ 90000) the ordered-pair kernel runs instead.
+constexpr size_t kSymMaxBytes = (size_t)1 << 30;
+
 static int adj_vjp(gtd_adjoint *A, const double4 *x, bool drift, cudaStream_t st) {
+    if (A->sym) {
+        SymArgs a = A->sa;
+        a.x = x;
+        a.w = A->w;
+        vjp_sym_kernel<<<a.grid, kVT, 0, st>>>(a);
+        GTD_CHECK_LAUNCH();
+        vjp_sym_combine_kernel<<<g1(A->n), 256, 0, st>>>(a, A->G, A->lx, A->lv, A->mu, A->h, drift ? 1 : 0);
+        GTD_CHECK_LAUNCH();
+        A->launches += 2;
+        return GTD_OK;
+    }
     const ForcePlan &p = A->vplan;
     VjpArgs va{p.n, p.rows, p.tiles, p.total, p.grid, p.bi, x, A->w, A->G, A->vpart};
     vjp_kernel<<<p.grid, kVT, 0, st>>>(va);
@@ -273,9 +497,41 @@ int gtd_adjoint_create(gtd_adjoint **out, int device, int64_t n, uint64_t steps,
     A->vplan.grid = (int)std::min<int64_t>((int64_t)sms * std::max(per_sm, 1), A->vplan.total);
     A->vplan.slots = A->vplan.grid + A->vplan.rows;
     A->ncheck = (int64_t)((steps + A->every - 1) / A->every) + 1;
+    {
+        const int nb = (int)((n + kVT - 1) / kVT);
+        const int64_t items = (int64_t)nb * (nb + 1) / 2;
+        const int64_t units = items * kSymChunks;
+        int sym_per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sym_per_sm, vjp_sym_kernel, kVT, 0);
+        const int64_t grid = std::min<int64_t>((int64_t)sms * std::max(sym_per_sm, 1), units);
+        const size_t bytes = ((size_t)(grid + items) + (size_t)units / kSymChunks) * 4 * kVT * sizeof(double);
+        if (bytes <= kSymMaxBytes) {
+            A->sym = true;
+            A->sa.n = n;
+            A->sa.nb = nb;
+            A->sa.items = items;
+            A->sa.units = units;
+            A->sa.grid = (int)grid;
+        }
+    }
     const size_t b4 = sizeof(double4) * (size_t)n;
     cudaError_t e = cudaSuccess;
     auto M = [&](void **p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
+    if (A->sym) {
+        M((void **)&A->item_rc, sizeof(int2) * (size_t)A->sa.items);
+        M((void **)&A->rowpart, (size_t)(A->sa.grid + A->sa.items) * 4 * kVT * sizeof(double));
+        M((void **)&A->colpart, (size_t)A->sa.units * 4 * 32 * sizeof(double));
+        if (e == cudaSuccess) {
+            std::vector<int2> rc;
+            rc.reserve((size_t)A->sa.items);
+            for (int r = 0; r < A->sa.nb; ++r)
+                for (int c = r; c < A->sa.nb; ++c) rc.push_back(make_int2(r, c));
+            e = cudaMemcpy(A->item_rc, rc.data(), sizeof(int2) * rc.size(), cudaMemcpyHostToDevice);
+        }
+        A->sa.item_rc = A->item_rc;
+        A->sa.rowpart = A->rowpart;
+        A->sa.colpart = A->colpart;
+    }
     M((void **)&A->fpart, partial_bytes(A->fplan));
     M((void **)&A->vpart, (size_t)A->vplan.slots * 4 * A->vplan.bi * sizeof(double));
     M((void **)&A->x, b4);
@@ -301,6 +557,7 @@ int gtd_adjoint_destroy(gtd_adjoint *A) {
     cudaSetDevice(A->device);
     cudaFree(A->fpart); cudaFree(A->vpart); cudaFree(A->x); cudaFree(A->v); cudaFree(A->a); cudaFree(A->ck);
     cudaFree(A->seg); cudaFree(A->lx); cudaFree(A->lv); cudaFree(A->w); cudaFree(A->mu);
+    cudaFree(A->item_rc); cudaFree(A->rowpart); cudaFree(A->colpart);
     delete A;
     return GTD_OK;
 }

@@ -39,14 +39,16 @@ def setup(n, seed):
     return t(m), t(x), t(v)
 
 
-def test_adjoint_vs_unrolled_torch_forward(gpu):
+# 48 bodies: one 256-body block (the symmetric VJP's diagonal form only); 700: three blocks, the
+# last one padded, so the off-diagonal blocks' pairs are taken once for both of their bodies.
+@pytest.mark.parametrize("n,steps", [(48, 40), (700, 12)])
+def test_adjoint_vs_unrolled_torch_forward(gpu, n, steps):
     import torch
 
     from gregpackagescpp_b200.adjoint import leapfrog_final_state
-    m, x, v = setup(48, 81)
+    m, x, v = setup(n, 81)
     target = x + 0.01 * AU * torch.randn(x.shape, dtype=torch.float64, device=x.device,
                                          generator=torch.Generator(device="cuda").manual_seed(5))
-    steps = 40
     xa, va, ma = x.clone().requires_grad_(), v.clone().requires_grad_(), m.clone().requires_grad_()
     xT, vT = leapfrog_final_state(xa, va, ma, G, DT, steps, checkpoint_every=7)
     loss = ((xT - target) ** 2).sum(-1).mean()
@@ -99,11 +101,12 @@ def test_adjoint_vs_central_differences(gpu):
     assert checks == 18
 
 
-def test_checkpoint_interval_invariance(gpu):
+@pytest.mark.parametrize("n", [64, 600])
+def test_checkpoint_interval_invariance(gpu, n):
     import torch
 
     from gregpackagescpp_b200.adjoint import leapfrog_final_state
-    m, x, v = setup(64, 83)
+    m, x, v = setup(n, 83)
     target = x * 1.0001
     grads = []
     for every in (1, 5, 13, 50):
