@@ -162,11 +162,17 @@ __device__ __forceinline__ void sym_pair(const double4 &xk, const double4 &wk, c
     mj_term = fma(wk.z, dz, fma(wk.y, dy, wk.x * dx)) * inv3;
 }
 
-__global__ void __launch_bounds__(kVT, 2) vjp_sym_kernel(SymArgs a) {
+// Two rows per thread (k and k + 128 of the row block): each rotated column read and each shuffle
+// of the column sums serves two pairs.
+constexpr int kSymRows = 2;
+constexpr int kSymThreads = kVT / kSymRows;
+static_assert(kSymThreads >= 128 && kSymThreads % 32 == 0, "the column reduction uses 128 threads");
+
+__global__ void __launch_bounds__(kSymThreads, 3) vjp_sym_kernel(SymArgs a) {
     // the column block, one array per component: a warp reads 32 different bodies per step (lane l
     // the body (l + s) mod 32), which as 8-byte words fall in distinct banks
     __shared__ double cxx[kVT], cxy[kVT], cxz[kVT], cxm[kVT], cwx[kVT], cwy[kVT], cwz[kVT];
-    __shared__ double red[kVT / 32][4][32];
+    __shared__ double red[kSymThreads / 32][4][32];
     auto col_x = [&](int i) { return make_double4(cxx[i], cxy[i], cxz[i], cxm[i]); };
     auto col_w = [&](int i) { return make_double4(cwx[i], cwy[i], cwz[i], 0.0); };
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -174,67 +180,92 @@ __global__ void __launch_bounds__(kVT, 2) vjp_sym_kernel(SymArgs a) {
     const int64_t u1 = (int64_t)(blockIdx.x + 1) * a.units / a.grid;
     int64_t cur = -1;
     int r = 0, c = 0;
-    double4 xk = make_double4(0, 0, 0, 0), wk = xk;
-    double rx = 0, ry = 0, rz = 0, rm = 0;
+    double4 xk[kSymRows], wk[kSymRows];
+    double rx[kSymRows], ry[kSymRows], rz[kSymRows], rm[kSymRows];
+#pragma unroll
+    for (int q = 0; q < kSymRows; ++q) {
+        xk[q] = wk[q] = make_double4(0, 0, 0, 0);
+        rx[q] = ry[q] = rz[q] = rm[q] = 0;
+    }
     auto flush_rows = [&]() {
         double *slot = a.rowpart + (size_t)(blockIdx.x + cur) * 4 * kVT;
-        slot[t] = rx;
-        slot[kVT + t] = ry;
-        slot[2 * kVT + t] = rz;
-        slot[3 * kVT + t] = rm;
-        rx = ry = rz = rm = 0;
+#pragma unroll
+        for (int q = 0; q < kSymRows; ++q) {
+            const int l = t + q * kSymThreads;
+            slot[l] = rx[q];
+            slot[kVT + l] = ry[q];
+            slot[2 * kVT + l] = rz[q];
+            slot[3 * kVT + l] = rm[q];
+            rx[q] = ry[q] = rz[q] = rm[q] = 0;
+        }
     };
     for (int64_t u = u0; u < u1; ++u) {
-        const int64_t q = u / kSymChunks;
-        const int chunk = (int)(u - q * kSymChunks);
-        if (q != cur) {
+        const int64_t it = u / kSymChunks;
+        const int chunk = (int)(u - it * kSymChunks);
+        if (it != cur) {
             if (cur >= 0) flush_rows();
-            cur = q;
-            const int2 rc = a.item_rc[q];
+            cur = it;
+            const int2 rc = a.item_rc[it];
             r = rc.x;
             c = rc.y;
-            const int64_t k = (int64_t)r * kVT + t;
-            xk = k < a.n ? a.x[k] : make_double4(0, 0, 0, 0);
-            wk = k < a.n ? a.w[k] : make_double4(0, 0, 0, 0);
-            const int64_t j = (int64_t)c * kVT + t;
-            const double4 qx = j < a.n ? a.x[j] : make_double4(0, 0, 0, 0);
-            const double4 qw = j < a.n ? a.w[j] : make_double4(0, 0, 0, 0);
+            double4 qx[kSymRows], qw[kSymRows];
+#pragma unroll
+            for (int q = 0; q < kSymRows; ++q) {
+                const int64_t k = (int64_t)r * kVT + t + q * kSymThreads;
+                xk[q] = k < a.n ? a.x[k] : make_double4(0, 0, 0, 0);
+                wk[q] = k < a.n ? a.w[k] : make_double4(0, 0, 0, 0);
+                const int64_t j = (int64_t)c * kVT + t + q * kSymThreads;
+                qx[q] = j < a.n ? a.x[j] : make_double4(0, 0, 0, 0);
+                qw[q] = j < a.n ? a.w[j] : make_double4(0, 0, 0, 0);
+            }
             __syncthreads();  // the previous item's columns are no longer read
-            cxx[t] = qx.x;
-            cxy[t] = qx.y;
-            cxz[t] = qx.z;
-            cxm[t] = qx.w;
-            cwx[t] = qw.x;
-            cwy[t] = qw.y;
-            cwz[t] = qw.z;
+#pragma unroll
+            for (int q = 0; q < kSymRows; ++q) {
+                const int l = t + q * kSymThreads;
+                cxx[l] = qx[q].x;
+                cxy[l] = qx[q].y;
+                cxz[l] = qx[q].z;
+                cxm[l] = qx[q].w;
+                cwx[l] = qw[q].x;
+                cwy[l] = qw[q].y;
+                cwz[l] = qw[q].z;
+            }
             __syncthreads();
         }
         const int jb = chunk * 32;
         if (r == c) {
-            // diagonal block: the row's ordered pairs with this chunk's columns, self pair excluded
+            // diagonal block: the rows' ordered pairs with this chunk's columns, self pairs excluded
             for (int i = 0; i < 32; ++i) {
-                double tx, ty, tz, mk, mj;
-                sym_pair<true>(xk, wk, col_x(jb + i), col_w(jb + i), tx, ty, tz, mk, mj);
-                rx += tx;
-                ry += ty;
-                rz += tz;
-                rm += mk;
+                const double4 xj = col_x(jb + i), wj = col_w(jb + i);
+#pragma unroll
+                for (int q = 0; q < kSymRows; ++q) {
+                    double tx, ty, tz, mk, mj;
+                    sym_pair<true>(xk[q], wk[q], xj, wj, tx, ty, tz, mk, mj);
+                    rx[q] += tx;
+                    ry[q] += ty;
+                    rz[q] += tz;
+                    rm[q] += mk;
+                }
             }
         } else {
             double cx = 0, cy = 0, cz = 0, cm = 0;  // running sums of column (lane + s) mod 32
             const bool guard = (int64_t)(c + 1) * kVT > a.n;  // padding columns in the last block
             auto step = [&](auto gd, int s) {
                 const int i = jb + ((lane + s) & 31);
-                double tx, ty, tz, mk, mj;
-                sym_pair<decltype(gd)::value>(xk, wk, col_x(i), col_w(i), tx, ty, tz, mk, mj);
-                rx += tx;
-                ry += ty;
-                rz += tz;
-                rm += mk;
-                cx -= tx;
-                cy -= ty;
-                cz -= tz;
-                cm += mj;
+                const double4 xj = col_x(i), wj = col_w(i);
+#pragma unroll
+                for (int q = 0; q < kSymRows; ++q) {
+                    double tx, ty, tz, mk, mj;
+                    sym_pair<decltype(gd)::value>(xk[q], wk[q], xj, wj, tx, ty, tz, mk, mj);
+                    rx[q] += tx;
+                    ry[q] += ty;
+                    rz[q] += tz;
+                    rm[q] += mk;
+                    cx -= tx;
+                    cy -= ty;
+                    cz -= tz;
+                    cm += mj;
+                }
                 const int from = (lane + 1) & 31;
                 cx = __shfl_sync(0xffffffffu, cx, from);
                 cy = __shfl_sync(0xffffffffu, cy, from);
@@ -257,7 +288,7 @@ __global__ void __launch_bounds__(kVT, 2) vjp_sym_kernel(SymArgs a) {
                 const int comp = t >> 5;
                 double sum = 0;
 #pragma unroll
-                for (int w2 = 0; w2 < kVT / 32; ++w2) sum += red[w2][comp][lane];
+                for (int w2 = 0; w2 < kSymThreads / 32; ++w2) sum += red[w2][comp][lane];
                 a.colpart[((size_t)u * 4 + comp) * 32 + lane] = sum;
             }
             __syncthreads();
@@ -448,7 +479,7 @@ static int adj_vjp(gtd_adjoint *A, const double4 *x, bool drift, cudaStream_t st
         SymArgs a = A->sa;
         a.x = x;
         a.w = A->w;
-        vjp_sym_kernel<<<a.grid, kVT, 0, st>>>(a);
+        vjp_sym_kernel<<<a.grid, kSymThreads, 0, st>>>(a);
         GTD_CHECK_LAUNCH();
         vjp_sym_combine_kernel<<<g1(A->n), 256, 0, st>>>(a, A->G, A->lx, A->lv, A->mu, A->h, drift ? 1 : 0);
         GTD_CHECK_LAUNCH();
@@ -502,7 +533,7 @@ int gtd_adjoint_create(gtd_adjoint **out, int device, int64_t n, uint64_t steps,
         const int64_t items = (int64_t)nb * (nb + 1) / 2;
         const int64_t units = items * kSymChunks;
         int sym_per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sym_per_sm, vjp_sym_kernel, kVT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sym_per_sm, vjp_sym_kernel, kSymThreads, 0);
         const int64_t grid = std::min<int64_t>((int64_t)sms * std::max(sym_per_sm, 1), units);
         const size_t bytes = ((size_t)(grid + items) + (size_t)units / kSymChunks) * 4 * kVT * sizeof(double);
         if (bytes <= kSymMaxBytes) {
