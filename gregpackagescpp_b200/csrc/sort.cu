@@ -3,6 +3,8 @@
 // for the spatial reordering of the direct-sum bodies.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "gtd_internal.cuh"
 #include "gtd_sort.cuh"
 
@@ -222,18 +224,22 @@ __global__ void __launch_bounds__(kSortThreads, kScatterBlocksPerSm) radix_scatt
     }
 }
 
-// The scatter's resident blocks per SM on the current device (its launch bound or less).
+// The scatter's resident blocks per SM on the current device (its launch bound or less), looked up
+// once per device; handles on different host threads may sort at the same time.
 static int scatter_blocks_per_sm() {
-    static int cached[64] = {0};
+    static std::atomic<int> cached[64];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
-    int *c = dev < 64 ? &cached[dev] : nullptr;
-    if (c && *c > 0) return *c;
+    std::atomic<int> *c = dev < 64 ? &cached[dev] : nullptr;
+    if (c) {
+        const int v = c->load(std::memory_order_relaxed);
+        if (v > 0) return v;
+    }
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, radix_scatter_kernel, kSortThreads, 0) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
-    if (c) *c = per_sm;
+    if (c) c->store(per_sm, std::memory_order_relaxed);
     return per_sm;
 }
 
