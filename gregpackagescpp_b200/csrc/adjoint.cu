@@ -115,16 +115,17 @@ __global__ void __launch_bounds__(kVT) vjp_kernel(VjpArgs a) {
 // ---- symmetric VJP ---------------------------------------------------------------------------
 // The J^T w term of a pair is antisymmetric: with d = x_j - x_k and u = m_k w_j - m_j w_k, body k
 // receives T = u / r^3 - 3 d (d . u) / r^5 and body j receives -T.  So each unordered pair of
-// 256-body blocks (r < c) is evaluated once, 45 FP64 operations per pair for both bodies' J^T w and
-// mass terms (two ordered pairs cost 68 in vjp_kernel); a diagonal block (r == r) sums its ordered
-// pairs for its own rows only.  Work: items (r, c), c >= r, in row-major order, each cut into 8
-// units of 32 columns; CTA g takes the contiguous units [g U / grid, (g + 1) U / grid), so a CTA
-// touches consecutive items and every CTA has the same number of units.
+// 256-body blocks (r < c) is evaluated once, 47 FP64 operations per pair for both bodies' J^T w
+// and mass terms and their sums (two ordered pairs cost 68 in vjp_kernel); a diagonal block
+// (r == c) sums its ordered pairs for its own rows only.  Work: items (r, c), c >= r, in row-major
+// order, each cut into 8 units of 32 columns; CTA g takes the contiguous units
+// [g U / grid, (g + 1) U / grid), so a CTA touches consecutive items and every CTA has the same
+// number of units.
 //   Rows: summed in registers over the units of an item, written to slot g + item (unique per
 //   (CTA, item), as in the stream-K split of the force kernel).
-//   Columns: inside a unit a warp's lane l pairs its row with column (l + s) mod 32 at step s and
+//   Columns: inside a unit a warp's lane l pairs its rows with column (l + s) mod 32 at step s and
 //   carries that column's running sum, passed on to lane l - 1 after each step by one shuffle, so
-//   lane l ends holding column l; the 8 warps' sums are added in warp order and written per unit.
+//   lane l ends holding column l; the warps' sums are added in warp order and written per unit.
 // Every sum is taken in a fixed order: the results are bit-reproducible.
 constexpr int kSymChunks = kVT / 32;  // units per item
 
