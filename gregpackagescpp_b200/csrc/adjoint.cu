@@ -471,8 +471,9 @@ static int adj_force(gtd_adjoint *A, const double4 *x, cudaStream_t st) {
     return rc;
 }
 
-// The symmetric VJP keeps 8 KB of row sums per (CTA, item) and 8 KB of column sums per item:
-// 38 MB at N = 16384; above this size (N ~ 90000) the ordered-pair kernel runs instead.
+// The symmetric VJP keeps 8 KB of row sums per slot (one slot per item and one per CTA) and 8 KB of
+// column sums per item: 37 MB at N = 16384; above this size (N ~ 90000) the ordered-pair kernel
+// runs instead.
 constexpr size_t kSymMaxBytes = (size_t)1 << 30;
 
 static int adj_vjp(gtd_adjoint *A, const double4 *x, bool drift, cudaStream_t st) {
